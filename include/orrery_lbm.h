@@ -1,0 +1,226 @@
+/*
+ * orrery_lbm.h - C ABI of the B200 lattice Boltzmann solvers (D3Q19 and D2Q9).
+ *
+ * This is the drop-in boundary for Orrery's LBM hot path.  Every entry point
+ * below replaces one member of the reference's solver seam
+ *   class Lbm3DSolver          src/aero/lbm3d/include/orrery/aero/lbm3d/lbm3d.h:196-232
+ *   make_gpu_solver (3D)       src/aero/lbm3d/include/orrery/aero/lbm3d/lbm3d.h:246-247
+ *   class Lbm2DSolver          src/aero/lbm/include/orrery/aero/lbm/lbm2d.h:173-202
+ *   make_gpu_solver (2D)       src/aero/lbm/include/orrery/aero/lbm/lbm2d.h:211-212
+ * and is cited at its declaration.  The signatures carry plain C types only:
+ * host pointers, sizes and opaque handles.
+ *
+ * Conventions
+ *   - Every call returns an orr_status; 0 is success.  The text of the last
+ *     failure is available from orr_lbm3d_last_error(handle) (per handle) or
+ *     orr_last_error() (per thread; also set by failed create calls).  Error
+ *     texts follow the reference's wording (lbm3d_common.cpp:74-155,
+ *     lbm3d_gpu.cpp:94-149) so callers that match on them keep working.
+ *   - Nothing throws across this boundary.  Creation refuses a configuration
+ *     before allocating anything on the device (lbm3d_gpu.cpp:488-513).
+ *   - Node (x, y, z) has the linear index x + nx (y + ny z); populations are
+ *     reported structure-of-arrays, f[i * cells + cell], in the reference's
+ *     D3Q19 / D2Q9 direction order (d3q19.h:15-36, d2q9.h:12-23), unshifted.
+ *   - The library copies every caller array it is given; callers keep
+ *     ownership.  A handle owns one CUDA stream and is not thread-safe.
+ */
+#ifndef ORRERY_LBM_H
+#define ORRERY_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ORR_API __attribute__((visibility("default")))
+#else
+#define ORR_API
+#endif
+
+typedef int32_t orr_status;
+enum {
+    ORR_OK = 0,
+    ORR_ERR_INVALID = 1,   /* configuration, mask or argument refused */
+    ORR_ERR_MEMORY = 2,    /* device memory refused or exhausted */
+    ORR_ERR_CUDA = 3,      /* a CUDA call failed */
+    ORR_ERR_STATE = 4,     /* call not valid in the handle's state */
+    ORR_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+    ORR_ERR_DIVERGED = 6,  /* non-finite coefficients detected */
+    ORR_ERR_NO_DEVICE = 7  /* no CUDA device of compute capability 10.0 */
+};
+
+/* Wall kinds of the y and z sides (WallKind, lbm2d.h:51). */
+enum { ORR_WALL_PERIODIC = 0, ORR_WALL_SLIP = 1, ORR_WALL_NO_SLIP = 2 };
+/* x boundary (XBoundary, lbm2d.h:43). */
+enum { ORR_X_PERIODIC = 0, ORR_X_INFLOW_OUTFLOW = 1 };
+/* Outlet treatment (Outlet, lbm2d.h:50). */
+enum { ORR_OUTLET_CONVECTIVE = 0, ORR_OUTLET_EXTRAPOLATION = 1 };
+/* Solid wall treatment (SolidWall, lbm3d.h:81). */
+enum { ORR_SOLID_HALFWAY = 0, ORR_SOLID_INTERPOLATED = 1 };
+/* Population storage on the device.  All forms collide in binary32 except
+ * F64, which computes in binary64 throughout (the FP64 device oracle).
+ * F32 holds f - w; F16 holds (f - w) scaled by 2^15 (FP16S); BF16 holds f - w. */
+enum { ORR_STORAGE_F32 = 0, ORR_STORAGE_F16 = 1, ORR_STORAGE_BF16 = 2, ORR_STORAGE_F64 = 3 };
+
+/* Wall (lbm2d.h:53-56). velocity_x is the tangential speed of a no-slip wall. */
+typedef struct orr_wall {
+    int32_t kind;
+    int32_t pad_;
+    double velocity_x;
+} orr_wall;
+
+/* Lbm3DConfig (lbm3d.h:83-103), field for field; Smagorinsky and Sponge
+ * (lbm2d.h:60-63, lbm3d.h:61-66) are flattened. */
+typedef struct orr_lbm3d_config {
+    uint64_t nx, ny, nz;
+    double tau;
+    int32_t x_boundary;
+    int32_t outlet;
+    orr_wall y_low, y_high, z_low, z_high;
+    double inlet_ux, inlet_uy, inlet_uz;
+    double body_force_x, body_force_y, body_force_z;
+    int32_t smagorinsky_enabled;
+    int32_t solid_wall;
+    double smagorinsky_constant;
+    double sponge_strength;
+    uint64_t sponge_inlet, sponge_outlet, sponge_sides;
+} orr_lbm3d_config;
+
+/* Lbm2DConfig (lbm2d.h:65-78). */
+typedef struct orr_lbm2d_config {
+    uint64_t nx, ny;
+    double tau;
+    int32_t x_boundary;
+    int32_t outlet;
+    orr_wall bottom, top;
+    double inlet_ux, inlet_uy;
+    double body_force_x, body_force_y;
+    int32_t smagorinsky_enabled;
+    int32_t pad_;
+    double smagorinsky_constant;
+} orr_lbm2d_config;
+
+/* Options of the device solver that have no counterpart in Lbm3DConfig. */
+typedef struct orr_solver_options {
+    int32_t storage;          /* ORR_STORAGE_* */
+    int32_t allow_high_mach;  /* 1: skip the lattice Mach guard (opt-in; off by default) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t block_x;          /* threads per block of the step kernel; 0 = tuned default */
+} orr_solver_options;
+
+typedef struct orr_lbm3d orr_lbm3d;
+typedef struct orr_lbm2d orr_lbm2d;
+
+/* ---- library ----------------------------------------------------------- */
+
+/* Text of the last failure on the calling thread ("" if none). */
+ORR_API const char* orr_last_error(void);
+/* Library version string. */
+ORR_API const char* orr_version(void);
+/* Number of CUDA devices the library can use (0 when none). */
+ORR_API orr_status orr_device_count(int32_t* count);
+
+/* ---- D3Q19 ------------------------------------------------------------- */
+
+/* validate() (lbm3d.h:113-114; lbm3d_common.cpp:74-161), plus the checks of
+ * make_gpu_solver (lbm3d_gpu.cpp:94-127, 492-500) for the chosen storage.
+ * `distance` may be NULL (a mask without distances).  Writes the reason into
+ * `message` (capacity `capacity`, always NUL-terminated) and returns
+ * ORR_ERR_INVALID when refused, ORR_OK otherwise.  No device is touched. */
+ORR_API orr_status orr_lbm3d_validate(const orr_lbm3d_config* config, const uint8_t* solid,
+                                      const double* distance, const orr_solver_options* options,
+                                      char* message, size_t capacity);
+
+/* make_gpu_solver (lbm3d.h:246-247; lbm3d_gpu.cpp:487-513): validates, counts
+ * the boundary tables, checks device memory and only then allocates; the
+ * state starts at uniform_inlet_state (lbm3d_common.cpp:262-270).
+ * `options` may be NULL (FP32 storage, Mach guard on, device 0). */
+ORR_API orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid,
+                                    const double* distance, const orr_solver_options* options,
+                                    orr_lbm3d** out);
+ORR_API void orr_lbm3d_destroy(orr_lbm3d* solver);
+ORR_API const char* orr_lbm3d_last_error(const orr_lbm3d* solver);
+
+/* Lbm3DSolver::initialize (lbm3d.h:211): equilibrium of the given fields at
+ * every fluid node (solids at rest), step count reset, inlet velocity back to
+ * the configuration's.  Each of rho, ux, uy, uz is an array of nx*ny*nz
+ * doubles; all four NULL gives uniform_inlet_state. */
+ORR_API orr_status orr_lbm3d_initialize(orr_lbm3d* solver, const double* rho, const double* ux,
+                                        const double* uy, const double* uz);
+/* Lbm3DSolver::step (lbm3d.h:212). */
+ORR_API orr_status orr_lbm3d_step(orr_lbm3d* solver, uint64_t count);
+/* Lbm3DSolver::steps (lbm3d.h:207). */
+ORR_API orr_status orr_lbm3d_steps(const orr_lbm3d* solver, uint64_t* steps);
+/* Lbm3DSolver::set_inlet_velocity / inlet_velocity (lbm3d.h:218-219;
+ * check_inlet_velocity, lbm3d_common.cpp:163-174). */
+ORR_API orr_status orr_lbm3d_set_inlet_velocity(orr_lbm3d* solver, const double velocity[3]);
+ORR_API orr_status orr_lbm3d_inlet_velocity(const orr_lbm3d* solver, double velocity[3]);
+/* Lbm3DSolver::force (lbm3d.h:227; lbm3d_gpu.cpp:407-436): force[0..2] and
+ * moment about the lattice origin [3..5], summed in binary64 on the device. */
+ORR_API orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]);
+/* Lbm3DSolver::macroscopic (lbm3d.h:221; lbm3d_gpu.cpp:357-392): density and
+ * velocity with the Guo half-force correction; solids report 1 and 0.  Any
+ * output pointer may be NULL. */
+ORR_API orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, double* uy,
+                                         double* uz);
+/* Lbm3DSolver::populations (lbm3d.h:222): 19 * cells doubles, unshifted. */
+ORR_API orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f);
+/* Lbm3DSolver::mass (lbm3d.h:229): sum of populations over fluid nodes,
+ * accumulated in binary64 on the device. */
+ORR_API orr_status orr_lbm3d_mass(orr_lbm3d* solver, double* mass);
+/* Lbm3DSolver::links (lbm3d.h:231; boundary_links, lbm3d_common.cpp:176-198),
+ * in the reference's scan order.  Query the count first. */
+ORR_API orr_status orr_lbm3d_link_count(const orr_lbm3d* solver, uint64_t* count);
+ORR_API orr_status orr_lbm3d_links(const orr_lbm3d* solver, uint32_t* cell, uint32_t* direction,
+                                   double* q);
+/* gpu_memory_bytes(config, links, wall_slots) (lbm3d.h:188-189) for this
+ * library's layout and the chosen storage: what create() checks against the
+ * free device memory.  Empty result (ORR_ERR_INVALID) when it overflows. */
+ORR_API orr_status orr_lbm3d_memory_bytes(const orr_lbm3d_config* config, uint64_t links,
+                                          uint64_t boundary_nodes, int32_t storage,
+                                          uint64_t* bytes);
+/* Number of boundary (non-bulk fluid) nodes the step kernel handles on its
+ * general path, and of fluid nodes. */
+ORR_API orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* fluid,
+                                         uint64_t* boundary);
+/* The cudaStream_t the handle launches on (for event timing by the caller). */
+ORR_API orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream);
+/* Kernels launched by this handle since creation (step, force, moments, ...). */
+ORR_API orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches);
+
+/* ---- D2Q9 -------------------------------------------------------------- */
+
+/* validate (lbm2d.h:85-86; lbm2d_common.cpp:31-77) plus the binary32 checks
+ * of the 2D make_gpu_solver (lbm2d.h:205-212). */
+ORR_API orr_status orr_lbm2d_validate(const orr_lbm2d_config* config, const uint8_t* solid,
+                                      const orr_solver_options* options, char* message,
+                                      size_t capacity);
+/* make_gpu_solver (lbm2d.h:211-212). */
+ORR_API orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid,
+                                    const orr_solver_options* options, orr_lbm2d** out);
+ORR_API void orr_lbm2d_destroy(orr_lbm2d* solver);
+ORR_API const char* orr_lbm2d_last_error(const orr_lbm2d* solver);
+/* Lbm2DSolver::initialize (lbm2d.h:187); rho, ux, uy arrays of nx*ny doubles
+ * or all NULL for uniform_inlet_state. */
+ORR_API orr_status orr_lbm2d_initialize(orr_lbm2d* solver, const double* rho, const double* ux,
+                                        const double* uy);
+ORR_API orr_status orr_lbm2d_step(orr_lbm2d* solver, uint64_t count);
+ORR_API orr_status orr_lbm2d_steps(const orr_lbm2d* solver, uint64_t* steps);
+/* Lbm2DSolver::force (lbm2d.h:196): x, y and the z moment about the origin. */
+ORR_API orr_status orr_lbm2d_force(orr_lbm2d* solver, double force_moment[3]);
+ORR_API orr_status orr_lbm2d_macroscopic(orr_lbm2d* solver, double* rho, double* ux, double* uy);
+ORR_API orr_status orr_lbm2d_populations(orr_lbm2d* solver, double* f);
+ORR_API orr_status orr_lbm2d_mass(orr_lbm2d* solver, double* mass);
+ORR_API orr_status orr_lbm2d_link_count(const orr_lbm2d* solver, uint64_t* count);
+ORR_API orr_status orr_lbm2d_links(const orr_lbm2d* solver, uint32_t* cell, uint32_t* direction);
+ORR_API orr_status orr_lbm2d_stream(const orr_lbm2d* solver, void** stream);
+ORR_API orr_status orr_lbm2d_launch_count(const orr_lbm2d* solver, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORRERY_LBM_H */

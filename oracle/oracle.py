@@ -1,0 +1,444 @@
+"""Python access to the two CPU oracles of the LBM path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+benchmark's CPU-baseline leg, never by the product package.
+
+``Restated3D`` / ``Restated2D``  the plain-C binary64 restatement
+                                  (oracle/lbm_oracle.c, always buildable).
+``Reference3D`` / ``Reference2D`` Orrery's own CpuLbm3D / CpuLbm2D compiled
+                                  from the reference sources (oracle/_ref);
+                                  present only where that build ran.
+Both expose the same methods, shaped like the reference's Lbm3DSolver
+(src/aero/lbm3d/include/orrery/aero/lbm3d/lbm3d.h:196-232).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from orrery_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATED_SO = os.path.join(HERE, "_build", "liblbm_oracle.so")
+REFERENCE_SO = os.path.join(HERE, "_ref", "libref_lbm.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_vp = ctypes.c_void_p
+
+_restated = None
+_reference = None
+
+
+def build(reference: str | None = None) -> None:
+    """Builds the restatement, and the reference library when the reference tree exists."""
+    env = dict(os.environ)
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True, env=env)
+    ref = reference or os.environ.get("ORR_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src", "aero", "lbm3d")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True, env=env)
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def restated_lib():
+    global _restated
+    if _restated is None:
+        if not os.path.exists(RESTATED_SO):
+            build()
+        lib = ctypes.CDLL(RESTATED_SO)
+        lib.lo3_create.restype = _vp
+        lib.lo3_create.argtypes = [ctypes.POINTER(abi.CLbm3DConfig), _u8p, _dp]
+        lib.lo3_destroy.argtypes = [_vp]
+        lib.lo3_initialize.argtypes = [_vp, _dp, _dp, _dp, _dp]
+        lib.lo3_step.argtypes = [_vp, ctypes.c_uint64]
+        lib.lo3_set_inlet.argtypes = [_vp, _dp]
+        lib.lo3_populations.argtypes = [_vp, _dp]
+        lib.lo3_force.argtypes = [_vp, _dp]
+        lib.lo3_macroscopic.argtypes = [_vp, _dp, _dp, _dp, _dp]
+        lib.lo3_mass.argtypes = [_vp]
+        lib.lo3_mass.restype = ctypes.c_double
+        lib.lo3_link_count.argtypes = [_vp]
+        lib.lo3_link_count.restype = ctypes.c_uint64
+        lib.lo3_links.argtypes = [_vp, _u32p, _u32p, _dp]
+        lib.lo3_boundary_count.argtypes = [_vp]
+        lib.lo3_boundary_count.restype = ctypes.c_uint64
+        lib.lo2_create.restype = _vp
+        lib.lo2_create.argtypes = [ctypes.POINTER(abi.CLbm2DConfig), _u8p]
+        lib.lo2_destroy.argtypes = [_vp]
+        lib.lo2_initialize.argtypes = [_vp, _dp, _dp, _dp]
+        lib.lo2_step.argtypes = [_vp, ctypes.c_uint64]
+        lib.lo2_populations.argtypes = [_vp, _dp]
+        lib.lo2_force.argtypes = [_vp, _dp]
+        lib.lo2_macroscopic.argtypes = [_vp, _dp, _dp, _dp]
+        lib.lo2_mass.argtypes = [_vp]
+        lib.lo2_mass.restype = ctypes.c_double
+        lib.lo2_link_count.argtypes = [_vp]
+        lib.lo2_link_count.restype = ctypes.c_uint64
+        lib.lo2_links.argtypes = [_vp, _u32p, _u32p]
+        lib.lo_set_threads.argtypes = [ctypes.c_int]
+        lib.lo_threads.restype = ctypes.c_int
+        _restated = lib
+    return _restated
+
+
+def reference_available() -> bool:
+    return os.path.exists(REFERENCE_SO)
+
+
+def reference_lib():
+    global _reference
+    if _reference is None:
+        if not reference_available():
+            raise FileNotFoundError(f"reference oracle not built: {REFERENCE_SO}")
+        lib = ctypes.CDLL(REFERENCE_SO)
+        c3 = ctypes.POINTER(abi.CLbm3DConfig)
+        c2 = ctypes.POINTER(abi.CLbm2DConfig)
+        lib.ref_set_threads.argtypes = [ctypes.c_int]
+        lib.ref_threads.restype = ctypes.c_int
+        lib.ref3d_validate.argtypes = [c3, _u8p, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref3d_create.restype = _vp
+        lib.ref3d_create.argtypes = [c3, _u8p, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref3d_destroy.argtypes = [_vp]
+        lib.ref3d_initialize.argtypes = [_vp, _dp, _dp, _dp, _dp]
+        lib.ref3d_step.argtypes = [_vp, ctypes.c_uint64]
+        lib.ref3d_set_inlet.argtypes = [_vp, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref3d_populations.argtypes = [_vp, _dp]
+        lib.ref3d_force.argtypes = [_vp, _dp]
+        lib.ref3d_macroscopic.argtypes = [_vp, _dp, _dp, _dp, _dp]
+        lib.ref3d_mass.argtypes = [_vp, _dp]
+        lib.ref3d_link_count.argtypes = [_vp]
+        lib.ref3d_link_count.restype = ctypes.c_uint64
+        lib.ref3d_links.argtypes = [_vp, _u32p, _u32p, _dp]
+        lib.ref3d_steps.argtypes = [_vp]
+        lib.ref3d_steps.restype = ctypes.c_uint64
+        lib.ref3d_sphere_mask.argtypes = [ctypes.c_uint64] * 3 + [_dp, ctypes.c_double, _u8p, _dp]
+        lib.ref3d_box_mask.argtypes = [ctypes.c_uint64] * 3 + [_dp, _dp, _u8p, _dp]
+        lib.ref3d_memory.argtypes = [c3, ctypes.c_uint64, ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64)]
+        lib.ref2d_validate.argtypes = [c2, _u8p, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref2d_create.restype = _vp
+        lib.ref2d_create.argtypes = [c2, _u8p, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref2d_destroy.argtypes = [_vp]
+        lib.ref2d_initialize.argtypes = [_vp, _dp, _dp, _dp]
+        lib.ref2d_step.argtypes = [_vp, ctypes.c_uint64]
+        lib.ref2d_populations.argtypes = [_vp, _dp]
+        lib.ref2d_force.argtypes = [_vp, _dp]
+        lib.ref2d_macroscopic.argtypes = [_vp, _dp, _dp, _dp]
+        lib.ref2d_mass.argtypes = [_vp, _dp]
+        lib.ref2d_circle_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, _u8p]
+        _reference = lib
+    return _reference
+
+
+class _Base3D:
+    q = 19
+
+    def __init__(self, config, solid, distance=None):
+        self.config = config
+        self.cells = config.cells
+        self.solid = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
+        self.distance = None if distance is None else np.ascontiguousarray(distance, dtype=np.float64).reshape(-1)
+        self._c = config.to_c()
+
+    def macroscopic(self):
+        out = [np.empty(self.cells) for _ in range(4)]
+        self._macroscopic(*out)
+        return out
+
+    def populations(self):
+        f = np.empty(self.q * self.cells)
+        self._populations(f)
+        return f
+
+    def force(self):
+        out = np.empty(6)
+        self._force(out)
+        return out
+
+
+class Restated3D(_Base3D):
+    """The C restatement (lo3_*)."""
+
+    def __init__(self, config, solid, distance=None):
+        super().__init__(config, solid, distance)
+        self._lib = restated_lib()
+        self._h = self._lib.lo3_create(ctypes.byref(self._c), _ptr(self.solid, _u8p),
+                                       _ptr(self.distance, _dp))
+
+    def close(self):
+        if self._h:
+            self._lib.lo3_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def initialize(self, rho=None, ux=None, uy=None, uz=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (rho, ux, uy, uz)]
+        self._lib.lo3_initialize(self._h, *[_ptr(a, _dp) for a in arrs])
+
+    def step(self, n):
+        self._lib.lo3_step(self._h, int(n))
+
+    def set_inlet_velocity(self, u):
+        v = np.asarray(u, dtype=np.float64)
+        self._lib.lo3_set_inlet(self._h, _ptr(v, _dp))
+
+    def _macroscopic(self, *out):
+        self._lib.lo3_macroscopic(self._h, *[_ptr(a, _dp) for a in out])
+
+    def _populations(self, f):
+        self._lib.lo3_populations(self._h, _ptr(f, _dp))
+
+    def _force(self, out):
+        self._lib.lo3_force(self._h, _ptr(out, _dp))
+
+    def mass(self):
+        return self._lib.lo3_mass(self._h)
+
+    def links(self):
+        n = self._lib.lo3_link_count(self._h)
+        cell = np.empty(n, np.uint32)
+        d = np.empty(n, np.uint32)
+        q = np.empty(n)
+        self._lib.lo3_links(self._h, _ptr(cell, _u32p), _ptr(d, _u32p), _ptr(q, _dp))
+        return cell, d, q
+
+    def boundary_count(self):
+        return self._lib.lo3_boundary_count(self._h)
+
+
+class Reference3D(_Base3D):
+    """Orrery's CpuLbm3D, built from the reference sources (ref3d_*)."""
+
+    def __init__(self, config, solid, distance=None):
+        super().__init__(config, solid, distance)
+        self._lib = reference_lib()
+        msg = ctypes.create_string_buffer(1024)
+        self._h = self._lib.ref3d_create(ctypes.byref(self._c), _ptr(self.solid, _u8p),
+                                         _ptr(self.distance, _dp), msg, 1024)
+        if not self._h:
+            raise ValueError(msg.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ref3d_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def initialize(self, rho=None, ux=None, uy=None, uz=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (rho, ux, uy, uz)]
+        if self._lib.ref3d_initialize(self._h, *[_ptr(a, _dp) for a in arrs]) != 0:
+            raise RuntimeError("reference initialize failed")
+
+    def step(self, n):
+        if self._lib.ref3d_step(self._h, int(n)) != 0:
+            raise RuntimeError("reference step failed")
+
+    def set_inlet_velocity(self, u):
+        v = np.asarray(u, dtype=np.float64)
+        msg = ctypes.create_string_buffer(1024)
+        if self._lib.ref3d_set_inlet(self._h, _ptr(v, _dp), msg, 1024) != 0:
+            raise ValueError(msg.value.decode())
+
+    def _macroscopic(self, *out):
+        self._lib.ref3d_macroscopic(self._h, *[_ptr(a, _dp) for a in out])
+
+    def _populations(self, f):
+        self._lib.ref3d_populations(self._h, _ptr(f, _dp))
+
+    def _force(self, out):
+        self._lib.ref3d_force(self._h, _ptr(out, _dp))
+
+    def mass(self):
+        out = ctypes.c_double()
+        self._lib.ref3d_mass(self._h, ctypes.byref(out))
+        return out.value
+
+    def links(self):
+        n = self._lib.ref3d_link_count(self._h)
+        cell = np.empty(n, np.uint32)
+        d = np.empty(n, np.uint32)
+        q = np.empty(n)
+        self._lib.ref3d_links(self._h, _ptr(cell, _u32p), _ptr(d, _u32p), _ptr(q, _dp))
+        return cell, d, q
+
+
+def reference_validate3d(config, solid, distance=None):
+    """The reference's validate() message ('' when accepted)."""
+    lib = reference_lib()
+    c = config.to_c()
+    s = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
+    d = None if distance is None else np.ascontiguousarray(distance, dtype=np.float64).reshape(-1)
+    msg = ctypes.create_string_buffer(1024)
+    lib.ref3d_validate(ctypes.byref(c), _ptr(s, _u8p), _ptr(d, _dp), msg, 1024)
+    return msg.value.decode()
+
+
+def reference_sphere_mask(nx, ny, nz, centre, radius):
+    lib = reference_lib()
+    n = nx * ny * nz
+    solid = np.empty(n, np.uint8)
+    dist = np.empty(n)
+    c = np.asarray(centre, dtype=np.float64)
+    lib.ref3d_sphere_mask(nx, ny, nz, _ptr(c, _dp), float(radius), _ptr(solid, _u8p), _ptr(dist, _dp))
+    return solid, dist
+
+
+def reference_box_mask(nx, ny, nz, lo, hi):
+    lib = reference_lib()
+    n = nx * ny * nz
+    solid = np.empty(n, np.uint8)
+    dist = np.empty(n)
+    a = np.asarray(lo, dtype=np.float64)
+    b = np.asarray(hi, dtype=np.float64)
+    lib.ref3d_box_mask(nx, ny, nz, _ptr(a, _dp), _ptr(b, _dp), _ptr(solid, _u8p), _ptr(dist, _dp))
+    return solid, dist
+
+
+def reference_memory3d(config, links, wall_slots):
+    lib = reference_lib()
+    c = config.to_c()
+    a, b, cpu = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    if lib.ref3d_memory(ctypes.byref(c), links, wall_slots, ctypes.byref(a), ctypes.byref(b),
+                        ctypes.byref(cpu)) != 0:
+        return None
+    return a.value, b.value, cpu.value
+
+
+class _Base2D:
+    q = 9
+
+    def __init__(self, config, solid):
+        self.config = config
+        self.cells = config.cells
+        self.solid = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
+        self._c = config.to_c()
+
+    def macroscopic(self):
+        out = [np.empty(self.cells) for _ in range(3)]
+        self._macroscopic(*out)
+        return out
+
+    def populations(self):
+        f = np.empty(self.q * self.cells)
+        self._populations(f)
+        return f
+
+    def force(self):
+        out = np.empty(3)
+        self._force(out)
+        return out
+
+
+class Restated2D(_Base2D):
+    def __init__(self, config, solid):
+        super().__init__(config, solid)
+        self._lib = restated_lib()
+        self._h = self._lib.lo2_create(ctypes.byref(self._c), _ptr(self.solid, _u8p))
+
+    def close(self):
+        if self._h:
+            self._lib.lo2_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def initialize(self, rho=None, ux=None, uy=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (rho, ux, uy)]
+        self._lib.lo2_initialize(self._h, *[_ptr(a, _dp) for a in arrs])
+
+    def step(self, n):
+        self._lib.lo2_step(self._h, int(n))
+
+    def _macroscopic(self, *out):
+        self._lib.lo2_macroscopic(self._h, *[_ptr(a, _dp) for a in out])
+
+    def _populations(self, f):
+        self._lib.lo2_populations(self._h, _ptr(f, _dp))
+
+    def _force(self, out):
+        self._lib.lo2_force(self._h, _ptr(out, _dp))
+
+    def mass(self):
+        return self._lib.lo2_mass(self._h)
+
+    def links(self):
+        n = self._lib.lo2_link_count(self._h)
+        cell = np.empty(n, np.uint32)
+        d = np.empty(n, np.uint32)
+        self._lib.lo2_links(self._h, _ptr(cell, _u32p), _ptr(d, _u32p))
+        return cell, d
+
+
+class Reference2D(_Base2D):
+    def __init__(self, config, solid):
+        super().__init__(config, solid)
+        self._lib = reference_lib()
+        msg = ctypes.create_string_buffer(1024)
+        self._h = self._lib.ref2d_create(ctypes.byref(self._c), _ptr(self.solid, _u8p), msg, 1024)
+        if not self._h:
+            raise ValueError(msg.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ref2d_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def initialize(self, rho=None, ux=None, uy=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (rho, ux, uy)]
+        self._lib.ref2d_initialize(self._h, *[_ptr(a, _dp) for a in arrs])
+
+    def step(self, n):
+        self._lib.ref2d_step(self._h, int(n))
+
+    def _macroscopic(self, *out):
+        self._lib.ref2d_macroscopic(self._h, *[_ptr(a, _dp) for a in out])
+
+    def _populations(self, f):
+        self._lib.ref2d_populations(self._h, _ptr(f, _dp))
+
+    def _force(self, out):
+        self._lib.ref2d_force(self._h, _ptr(out, _dp))
+
+    def mass(self):
+        out = ctypes.c_double()
+        self._lib.ref2d_mass(self._h, ctypes.byref(out))
+        return out.value
+
+
+def reference_validate2d(config, solid):
+    lib = reference_lib()
+    c = config.to_c()
+    s = np.ascontiguousarray(solid, dtype=np.uint8).reshape(-1)
+    msg = ctypes.create_string_buffer(1024)
+    lib.ref2d_validate(ctypes.byref(c), _ptr(s, _u8p), msg, 1024)
+    return msg.value.decode()
+
+
+def reference_circle_mask(nx, ny, cx, cy, radius):
+    lib = reference_lib()
+    solid = np.empty(nx * ny, np.uint8)
+    lib.ref2d_circle_mask(nx, ny, float(cx), float(cy), float(radius), _ptr(solid, _u8p))
+    return solid
+
+
+def set_threads(n: int) -> None:
+    restated_lib().lo_set_threads(int(n))
+    if reference_available():
+        reference_lib().ref_set_threads(int(n))

@@ -1,0 +1,67 @@
+"""ctypes mirror of include/orrery_lbm.h: the C structs and enums of the ABI.
+
+Plain data definitions only; loading the native library lives in
+``orrery_b200._native``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+# Status codes.
+ORR_OK = 0
+ORR_ERR_INVALID = 1
+ORR_ERR_MEMORY = 2
+ORR_ERR_CUDA = 3
+ORR_ERR_STATE = 4
+ORR_ERR_TIMEOUT = 5
+ORR_ERR_DIVERGED = 6
+ORR_ERR_NO_DEVICE = 7
+
+# Wall kinds, x boundary, outlet, solid wall, storage.
+ORR_WALL_PERIODIC, ORR_WALL_SLIP, ORR_WALL_NO_SLIP = 0, 1, 2
+ORR_X_PERIODIC, ORR_X_INFLOW_OUTFLOW = 0, 1
+ORR_OUTLET_CONVECTIVE, ORR_OUTLET_EXTRAPOLATION = 0, 1
+ORR_SOLID_HALFWAY, ORR_SOLID_INTERPOLATED = 0, 1
+ORR_STORAGE_F32, ORR_STORAGE_F16, ORR_STORAGE_BF16, ORR_STORAGE_F64 = 0, 1, 2, 3
+
+STORAGE_NAMES = {"f32": ORR_STORAGE_F32, "f16": ORR_STORAGE_F16, "bf16": ORR_STORAGE_BF16,
+                 "f64": ORR_STORAGE_F64}
+
+
+class CWall(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("pad_", ctypes.c_int32), ("velocity_x", ctypes.c_double)]
+
+
+class CLbm3DConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_uint64), ("ny", ctypes.c_uint64), ("nz", ctypes.c_uint64),
+        ("tau", ctypes.c_double),
+        ("x_boundary", ctypes.c_int32), ("outlet", ctypes.c_int32),
+        ("y_low", CWall), ("y_high", CWall), ("z_low", CWall), ("z_high", CWall),
+        ("inlet_ux", ctypes.c_double), ("inlet_uy", ctypes.c_double), ("inlet_uz", ctypes.c_double),
+        ("body_force_x", ctypes.c_double), ("body_force_y", ctypes.c_double),
+        ("body_force_z", ctypes.c_double),
+        ("smagorinsky_enabled", ctypes.c_int32), ("solid_wall", ctypes.c_int32),
+        ("smagorinsky_constant", ctypes.c_double),
+        ("sponge_strength", ctypes.c_double),
+        ("sponge_inlet", ctypes.c_uint64), ("sponge_outlet", ctypes.c_uint64),
+        ("sponge_sides", ctypes.c_uint64),
+    ]
+
+
+class CLbm2DConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_uint64), ("ny", ctypes.c_uint64),
+        ("tau", ctypes.c_double),
+        ("x_boundary", ctypes.c_int32), ("outlet", ctypes.c_int32),
+        ("bottom", CWall), ("top", CWall),
+        ("inlet_ux", ctypes.c_double), ("inlet_uy", ctypes.c_double),
+        ("body_force_x", ctypes.c_double), ("body_force_y", ctypes.c_double),
+        ("smagorinsky_enabled", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("smagorinsky_constant", ctypes.c_double),
+    ]
+
+
+class CSolverOptions(ctypes.Structure):
+    _fields_ = [("storage", ctypes.c_int32), ("allow_high_mach", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("block_x", ctypes.c_int32)]
