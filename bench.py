@@ -1,0 +1,304 @@
+"""Benchmark of the D3Q19 hot path: MLUPS and the fraction of the HBM roofline.
+
+Workload: the 256 x 128 x 128 sphere channel (D 32 at (64, 64, 64), u 0.05,
+Re 200, Smagorinsky C 0.1, zero-gradient outflow, free-slip sides), binary32
+shifted populations, seeded +-1e-3 velocity noise.  A step is one fused
+collide-stream step over the whole lattice; MLUPS counts every node
+(steps * nx * ny * nz / s / 1e6).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {cuda,reference}]
+
+N > 1 runs under torchrun as N independent replicas (one lattice per GPU, no
+collective on the data path); the reported value is the whole-job MLUPS over
+the slowest rank's device time.  ``--impl reference`` times the reference's own
+CPU solver (compiled from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_UPDATE = {"f32": 152, "f16": 76, "bf16": 76, "f64": 304}  # 2 * 19 * sizeof(storage)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dram_traffic(workload: str, storage: str):
+    """Per-launch DRAM bytes of the bulk kernel from the committed ncu summary
+    of this workload (profiles/*.txt line 'traffic_bytes_per_step <storage> <B>')."""
+    path = os.path.join(ROOT, "profiles", f"bulk3d_{workload}.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_step" and parts[1] == storage:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"orr_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.remove(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_mlups(workload, seconds: float, threads: int | None = None, use_reference=True):
+    """Times a CPU solver of the path on the host cores on a bounded sample of
+    the workload: the reference's own CpuLbm3D when built (oracle/_ref), else
+    the C restatement.  Returns (mlups, cores, kind, sample-description, steps)."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    if use_reference and O.reference_available():
+        O.reference_lib().ref_set_threads(threads)
+        solver = O.Reference3D(workload.config, workload.mask.solid, workload.mask.distance)
+        kind = "reference"
+    else:
+        O.restated_lib().lo_set_threads(threads)
+        solver = O.Restated3D(workload.config, workload.mask.solid, workload.mask.distance)
+        kind = "port"
+    solver.initialize(workload.rho, workload.ux, workload.uy, workload.uz)
+    solver.step(1)  # warm-up
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        solver.step(1)
+        steps += 1
+        elapsed = time.perf_counter() - t0
+        if elapsed >= seconds or steps >= 1000:
+            break
+    mlups = steps * workload.cells / elapsed / 1e6
+    sample = (f"{steps} steps of the full {workload.config.nx}x{workload.config.ny}x{workload.config.nz} "
+              f"lattice after 1 warm-up step, {elapsed:.1f} s wall, {threads} threads")
+    solver.close()
+    return mlups, threads, kind, sample, steps
+
+
+def run_reference_arm(args, rank: int):
+    from orrery_b200 import workloads as W
+    if rank != 0:
+        return 0
+    w = W.sphere3d(seed=1)
+    budget = float(os.environ.get("ORR_REFERENCE_SECONDS", "60"))
+    per_step_budget = max(budget / max(args.steps + args.warmup, 1), 0.5)
+    mlups, cores, kind, sample, steps = cpu_reference_mlups(w, per_step_budget * args.steps)
+    line = {
+        "impl": "reference", "metric": "D3Q19 MLUPS", "value": mlups, "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "storage": "f64 (reference CPU solver)", "seed": 1},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=1000)
+    args = ap.parse_args(argv)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    else:
+        torch.cuda.set_device(0)
+
+    from orrery_b200 import solver as S
+    from orrery_b200 import workloads as W
+
+    w = W.sphere3d(seed=1 + rank)
+    solver = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank,
+                               block_x=args.block)
+    solver.initialize(w.rho, w.ux, w.uy, w.uz)
+    stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local_rank))
+    solver.step(max(args.warmup, 3))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank) if rank == 0 else None
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    launches_before = solver.launch_count()
+    barrier()
+    if clocks:
+        clocks.start()
+    start.record(stream)
+    solver.step(args.steps)
+    stop.record(stream)
+    stop.synchronize()
+    barrier()
+    clock_info = clocks.stop() if clocks else None
+    launches = solver.launch_count() - launches_before
+    ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    mlups_rank = w.cells * args.steps / (ms * 1e-3) / 1e6
+    mlups = mlups_rank * world
+
+    # Force sanity and the coefficient at the end of the timed run.
+    f = solver.force()
+    coeff = W.coefficients3d(f.force, f.moment, w.config.inlet_ux, w.reference_area, w.reference_length)
+
+    # Roofline of the step (bulk + boundary kernels): algorithmic bytes per
+    # step over the device time of a step.
+    bytes_per_step = BYTES_PER_UPDATE[args.storage] * w.cells
+    achieved_gbs = bytes_per_step / (ms_per_step * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = dram_traffic(w.name, args.storage)
+    solver.close()
+
+    # End to end through the C ABI with host buffers: create from the host
+    # mask, initialise from host fields, step with the force read back every
+    # 10 steps (the reference adapter's sampling), read the moments back.
+    e2e = None
+    if rank == 0 or world > 1:
+        import numpy as np
+        barrier()
+        t0 = time.perf_counter()
+        s2 = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank, block_x=args.block)
+        s2.initialize(w.rho, w.ux, w.uy, w.uz)
+        samples = 0
+        for _ in range(args.e2e_steps // 10):
+            s2.step(10)
+            s2.force()
+            samples += 1
+        fields = s2.macroscopic()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        k = samples * 10
+        h2d = w.cells * (1 + 4 * 8) + 8 * 3  # mask, four initial fields, inlet velocity
+        d2h = samples * 48 + 4 * 8 * w.cells
+        e2e = {"value": w.cells * k * world / e2e_s / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d / k, "d2h_bytes_per_step": d2h / k,
+               "steps": k, "seconds": e2e_s,
+               "note": "one whole solve per rank: create (plan + upload), initialise from host fields, "
+                       "steps with the force read back every 10 steps, moments read back"}
+        del fields
+        s2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        secs = float(os.environ.get("ORR_CPU_BASELINE_SECONDS", "15"))
+        mlups_cpu, cores, kind, sample, _ = cpu_reference_mlups(w, secs)
+        cpu = {"value": mlups_cpu, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "D3Q19 MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "f32", "f16": "f16-storage/f32-math", "bf16": "bf16-storage/f32-math",
+                      "f64": "f64"}[args.storage],
+            "data": "synthetic",
+            "config": {"workload": w.name, "nodes": w.cells, "storage": args.storage,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": f"inputs larger than L2: {w.cells * 19 * {'f32': 4, 'f16': 2, 'bf16': 2, 'f64': 8}[args.storage] / 1e6:.0f} MB per population buffer",
+                       "seed": 1},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_gbs / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_node": BYTES_PER_UPDATE[args.storage]},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "cd": coeff["cd"], "cl": coeff["cl"],
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -182,6 +182,15 @@ ORR_API orr_status orr_lbm3d_links(const orr_lbm3d* solver, uint32_t* cell, uint
 ORR_API orr_status orr_lbm3d_memory_bytes(const orr_lbm3d_config* config, uint64_t links,
                                           uint64_t boundary_nodes, int32_t storage,
                                           uint64_t* bytes);
+/* Host-only planning of an accepted configuration, no device involved:
+ * boundary_links (lbm3d.h:124-125; lbm3d_common.cpp:176-198) with their wall
+ * fractions (link_fraction, lbm3d_internal.h:132-179), and the node counts.
+ * Pass NULL arrays to query the counts; then arrays of `links` entries.
+ * Any count pointer may be NULL. */
+ORR_API orr_status orr_lbm3d_plan(const orr_lbm3d_config* config, const uint8_t* solid,
+                                  const double* distance, uint64_t* links, uint64_t* fluid,
+                                  uint64_t* boundary_nodes, uint32_t* cell, uint32_t* direction,
+                                  double* q);
 /* Number of boundary (non-bulk fluid) nodes the step kernel handles on its
  * general path, and of fluid nodes. */
 ORR_API orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* fluid,

@@ -1,0 +1,112 @@
+"""Loads the native library and declares the C ABI of include/orrery_lbm.h.
+
+The library is the only implementation of the solvers: there is no Python or
+CPU fallback.  If it is missing it is built in-tree (nvcc is part of the
+toolchain); if that fails, importing the solvers raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from . import abi
+
+_LOCK = threading.Lock()
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_vp = ctypes.c_void_p
+_st = ctypes.c_int32
+_c3 = ctypes.POINTER(abi.CLbm3DConfig)
+_c2 = ctypes.POINTER(abi.CLbm2DConfig)
+_opt = ctypes.POINTER(abi.CSolverOptions)
+
+# Every entry point of include/orrery_lbm.h: name -> (restype, argtypes).
+SIGNATURES = {
+    "orr_last_error": (ctypes.c_char_p, []),
+    "orr_version": (ctypes.c_char_p, []),
+    "orr_device_count": (_st, [_i32p]),
+    "orr_lbm3d_validate": (_st, [_c3, _u8p, _dp, _opt, ctypes.c_char_p, ctypes.c_size_t]),
+    "orr_lbm3d_create": (_st, [_c3, _u8p, _dp, _opt, ctypes.POINTER(_vp)]),
+    "orr_lbm3d_destroy": (None, [_vp]),
+    "orr_lbm3d_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_lbm3d_initialize": (_st, [_vp, _dp, _dp, _dp, _dp]),
+    "orr_lbm3d_step": (_st, [_vp, ctypes.c_uint64]),
+    "orr_lbm3d_steps": (_st, [_vp, _u64p]),
+    "orr_lbm3d_set_inlet_velocity": (_st, [_vp, _dp]),
+    "orr_lbm3d_inlet_velocity": (_st, [_vp, _dp]),
+    "orr_lbm3d_force": (_st, [_vp, _dp]),
+    "orr_lbm3d_macroscopic": (_st, [_vp, _dp, _dp, _dp, _dp]),
+    "orr_lbm3d_populations": (_st, [_vp, _dp]),
+    "orr_lbm3d_mass": (_st, [_vp, _dp]),
+    "orr_lbm3d_link_count": (_st, [_vp, _u64p]),
+    "orr_lbm3d_links": (_st, [_vp, _u32p, _u32p, _dp]),
+    "orr_lbm3d_memory_bytes": (_st, [_c3, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32, _u64p]),
+    "orr_lbm3d_plan": (_st, [_c3, _u8p, _dp, _u64p, _u64p, _u64p, _u32p, _u32p, _dp]),
+    "orr_lbm3d_node_counts": (_st, [_vp, _u64p, _u64p]),
+    "orr_lbm3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
+    "orr_lbm3d_launch_count": (_st, [_vp, _u64p]),
+    "orr_lbm2d_validate": (_st, [_c2, _u8p, _opt, ctypes.c_char_p, ctypes.c_size_t]),
+    "orr_lbm2d_create": (_st, [_c2, _u8p, _opt, ctypes.POINTER(_vp)]),
+    "orr_lbm2d_destroy": (None, [_vp]),
+    "orr_lbm2d_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_lbm2d_initialize": (_st, [_vp, _dp, _dp, _dp]),
+    "orr_lbm2d_step": (_st, [_vp, ctypes.c_uint64]),
+    "orr_lbm2d_steps": (_st, [_vp, _u64p]),
+    "orr_lbm2d_force": (_st, [_vp, _dp]),
+    "orr_lbm2d_macroscopic": (_st, [_vp, _dp, _dp, _dp]),
+    "orr_lbm2d_populations": (_st, [_vp, _dp]),
+    "orr_lbm2d_mass": (_st, [_vp, _dp]),
+    "orr_lbm2d_link_count": (_st, [_vp, _u64p]),
+    "orr_lbm2d_links": (_st, [_vp, _u32p, _u32p]),
+    "orr_lbm2d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
+    "orr_lbm2d_launch_count": (_st, [_vp, _u64p]),
+}
+
+
+def library_path() -> str:
+    from . import build
+    return build.LIBRARY
+
+
+def lib():
+    """The loaded native library (built on first use when absent)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            path = library_path()
+            if not os.path.exists(path):
+                from . import build
+                build.build()
+            handle = ctypes.CDLL(path)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            _LIB = handle
+        return _LIB
+
+
+class LbmError(RuntimeError):
+    """A refused or failed call: ``status`` is the orr_status, the message the library's text."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def check(status: int, message_fn) -> None:
+    if status != abi.ORR_OK:
+        msg = message_fn()
+        if isinstance(msg, bytes):
+            msg = msg.decode(errors="replace")
+        raise LbmError(status, msg)
+
+
+def ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)

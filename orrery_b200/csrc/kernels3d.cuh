@@ -1,0 +1,753 @@
+// D3Q19 device kernels: the fused pull-stream + collide step, initialisation,
+// moments, binary64 momentum-exchange force and mass reductions.
+//
+// The step follows the reference's fused pull step
+//   CPU   CpuLbm3D::update_row + collide  (src/aero/lbm3d/lbm3d_cpu.cpp:32-100, 261-322)
+//   GPU   lbm_d3q19_step                  (src/render/shaders/lbm/lbm_d3q19_step.comp.glsl,
+//                                          lbm_d3q19_common.glsl:87-368)
+// with the boundary rules of resolve_source (src/aero/lbm3d/lbm3d_internal.h:57-130).
+// A step is two kernels over disjoint node sets, writing disjoint entries:
+//   boundary3d   one thread per entry of the compact list of boundary fluid
+//                nodes: the general gather (sides, inlet, outlet, walls,
+//                bounce-back);
+//   bulk3d       one thread per node of the interior rows y in [1, ny-2],
+//                z in [1, nz-2]; bulk nodes take 19 plain pulls, every other
+//                node returns at once.
+// So bulk warps never diverge into the boundary path and keep a small
+// register budget; the solver runs the two as parallel branches of the
+// step's CUDA graph, so the boundary list (a few percent of the nodes)
+// overlaps the bulk.
+//
+// Shifted storage forms collide in binary32 on f - w (the GLSL formulation);
+// the binary64 form stores f itself and evaluates every expression in the
+// reference CPU solver's order (this translation unit is compiled without
+// FMA contraction for it), which makes it the FP64 device oracle.
+#pragma once
+
+#include <cstdint>
+
+#include "lattice.h"
+#include "orrery_lbm.h"
+#include "storage.cuh"
+
+namespace orr {
+
+// Lattice geometry and launch partition (all integers; by value).
+struct Geom3D {
+    uint32_t nx, ny, nz;
+    uint32_t plane;           // nx * ny
+    uint64_t cells;           // nx * ny * nz
+    uint32_t tiles_x;         // bulk blocks per interior row
+    uint32_t boundary_nodes;  // entries of the boundary list
+    int32_t x_mode;           // ORR_X_PERIODIC / ORR_X_INFLOW_OUTFLOW
+    int32_t outlet_mode;      // ORR_OUTLET_*
+    int32_t y_lo, y_hi, z_lo, z_hi; // ORR_WALL_*
+    int32_t forced;           // a body force is set (Guo forcing)
+    int32_t sponge;           // absorbing layers active
+    uint32_t sponge_inlet, sponge_outlet, sponge_sides;
+};
+
+// Real parameters in the arithmetic type (binary32 parameters are the
+// binary32 roundings of the configuration, as a Float32Uniform delivers them,
+// src/aero/compute/include/orrery/aero/compute/compute_backend.h:19-23).
+template <class A> struct Phys3D {
+    A tau;
+    A smag_c;     // Smagorinsky constant C (binary64 form)
+    A smag_c2;    // C^2 (binary32 forms, as u_smagorinsky_c2)
+    A fx, fy, fz; // body force density
+    A wall_ux[4]; // y_lo, y_hi, z_lo, z_hi tangential wall speeds
+    A outlet_speed;
+    A sponge_strength;
+};
+
+// 18 sqrt(2) (src/aero/lbm3d/lbm3d_cpu.cpp:23-26).
+constexpr double kSmagFactor = 18.0 * 1.4142135623730951;
+
+// c components of a direction known only at run time (the force links), from
+// bit-packed tables.
+__device__ __forceinline__ void c_rt(int j, int& x, int& y, int& z) {
+    // bits 2j..2j+1 hold c + 1 for j = 0..18
+    constexpr uint64_t kX = [] {
+        uint64_t v = 0;
+        for (int i = 0; i < d3::Q; ++i) v |= static_cast<uint64_t>(d3::cx(i) + 1) << (2 * i);
+        return v;
+    }();
+    constexpr uint64_t kY = [] {
+        uint64_t v = 0;
+        for (int i = 0; i < d3::Q; ++i) v |= static_cast<uint64_t>(d3::cy(i) + 1) << (2 * i);
+        return v;
+    }();
+    constexpr uint64_t kZ = [] {
+        uint64_t v = 0;
+        for (int i = 0; i < d3::Q; ++i) v |= static_cast<uint64_t>(d3::cz(i) + 1) << (2 * i);
+        return v;
+    }();
+    x = static_cast<int>((kX >> (2 * j)) & 3ULL) - 1;
+    y = static_cast<int>((kY >> (2 * j)) & 3ULL) - 1;
+    z = static_cast<int>((kZ >> (2 * j)) & 3ULL) - 1;
+}
+
+__device__ __forceinline__ int opposite_rt(int j) {
+    return j == 0 ? 0 : ((j & 1) ? j + 1 : j - 1);
+}
+
+__device__ __forceinline__ double w_rt(int j) {
+    return j == 0 ? 1.0 / 3.0 : (j <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+
+// ---------------------------------------------------------------- collide --
+
+// BGK collision with Guo forcing and the optional Smagorinsky closure.
+// Shifted form: lbm3_collide (lbm_d3q19_common.glsl:261-326).
+// Unshifted binary64 form: collide (lbm3d_cpu.cpp:32-93), same operation order.
+template <class A, bool kShifted, bool kSmag>
+__device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int forced,
+                                         A& out_ux, A& out_uy, A& out_uz) {
+    if constexpr (kShifted) {
+        A drho = 0;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) drho += f[i];
+        const A jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
+        const A jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
+        const A jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
+        const A rho = A(1) + drho;
+        const A inv = A(1) / rho;
+        const A ux = (jx + A(0.5) * p.fx) * inv;
+        const A uy = (jy + A(0.5) * p.fy) * inv;
+        const A uz = (jz + A(0.5) * p.fz) * inv;
+        const A uu = ux * ux + uy * uy + uz * uz;
+        A tau = p.tau;
+        if constexpr (kSmag) {
+            // Pi_neq = sum c c (f - f_eq).  For the second-order D3Q19
+            // equilibrium sum c_a c_b f_eq = rho (c_s^2 delta_ab + u_a u_b)
+            // exactly, and sum c c w = c_s^2 delta, so on shifted values
+            // Pi_neq = sum c c f_s - drho c_s^2 delta - rho u u; f_eq is then
+            // formed on the fly in the relaxation below.
+            const A sxx = f[1] + f[2] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] + f[14];
+            const A syy = f[3] + f[4] + f[7] + f[8] + f[9] + f[10] + f[15] + f[16] + f[17] + f[18];
+            const A szz = f[5] + f[6] + f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+            const A sxy = f[7] + f[8] - f[9] - f[10];
+            const A sxz = f[11] + f[12] - f[13] - f[14];
+            const A syz = f[15] + f[16] - f[17] - f[18];
+            const A iso = drho * A(1.0 / 3.0);
+            const A pxx = sxx - iso - rho * ux * ux;
+            const A pyy = syy - iso - rho * uy * uy;
+            const A pzz = szz - iso - rho * uz * uz;
+            const A pxy = sxy - rho * ux * uy;
+            const A pxz = sxz - rho * ux * uz;
+            const A pyz = syz - rho * uy * uz;
+            const A strain =
+                sqrt(pxx * pxx + pyy * pyy + pzz * pzz + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+            tau = A(0.5) * (tau + sqrt(tau * tau + A(kSmagFactor) * p.smag_c2 * strain * inv));
+        }
+        const A omega = A(1) / tau;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
+            const A feq = A(d3::w(i)) * (drho + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu));
+            f[i] = f[i] - omega * (f[i] - feq);
+        }
+        if (forced) {
+            const A scale = A(1) - A(0.5) * omega;
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
+                const A cu = ex * ux + ey * uy + ez * uz;
+                f[i] += scale * A(d3::w(i)) *
+                        (A(3) * ((ex - ux) * p.fx + (ey - uy) * p.fy + (ez - uz) * p.fz) +
+                         A(9) * cu * (ex * p.fx + ey * p.fy + ez * p.fz));
+            }
+        }
+        out_ux = ux;
+        out_uy = uy;
+        out_uz = uz;
+    } else {
+        double rho = 0.0;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) rho += f[i];
+        const double jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
+        const double jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
+        const double jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
+        const double fx = p.fx, fy = p.fy, fz = p.fz;
+        const double ux = (jx + 0.5 * fx) / rho;
+        const double uy = (jy + 0.5 * fy) / rho;
+        const double uz = (jz + 0.5 * fz) / rho;
+        const double base = 1.0 - 1.5 * (ux * ux + uy * uy + uz * uz);
+        const double cu[d3::Q] = {0.0,     ux,       -ux,     uy,      -uy,     uz,       -uz,
+                                  ux + uy, -ux - uy, ux - uy, uy - ux, ux + uz, -ux - uz, ux - uz,
+                                  uz - ux, uy + uz,  -uy - uz, uy - uz, uz - uy};
+        double feq[d3::Q];
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            feq[i] = d3::w(i) * rho * (base + cu[i] * (3.0 + 4.5 * cu[i]));
+        }
+        double tau = p.tau;
+        if constexpr (kSmag) {
+            double pi[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                const double neq = f[i] - feq[i];
+                const double ex = d3::cx(i), ey = d3::cy(i), ez = d3::cz(i);
+                pi[0] += ex * ex * neq;
+                pi[1] += ey * ey * neq;
+                pi[2] += ez * ez * neq;
+                pi[3] += ex * ey * neq;
+                pi[4] += ex * ez * neq;
+                pi[5] += ey * ez * neq;
+            }
+            const double strain = sqrt(pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] +
+                                       2.0 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]));
+            const double c = p.smag_c;
+            tau = 0.5 * (tau + sqrt(tau * tau + kSmagFactor * c * c * strain / rho));
+        }
+        const double omega = 1.0 / tau;
+        const double scale = 1.0 - 0.5 * omega;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            double v = f[i] - omega * (f[i] - feq[i]);
+            if (forced) {
+                const double ex = d3::cx(i), ey = d3::cy(i), ez = d3::cz(i);
+                v += scale * d3::w(i) *
+                     (3.0 * ((ex - ux) * fx + (ey - uy) * fy + (ez - uz) * fz) +
+                      9.0 * cu[i] * (ex * fx + ey * fy + ez * fz));
+            }
+            f[i] = v;
+        }
+        out_ux = ux;
+        out_uy = uy;
+        out_uz = uz;
+    }
+}
+
+// Relaxation rate of the absorbing layers at (x, y, z)
+// (sponge_sigma, lbm3d_internal.h:255-281; lbm3_sponge, glsl:336-353).
+template <class A>
+__device__ __forceinline__ A sponge_rate3(const Geom3D& g, const Phys3D<A>& p, uint32_t x,
+                                          uint32_t y, uint32_t z) {
+    A best = 0;
+    const auto layer = [&best](uint32_t d, uint32_t t) {
+        if (d < t) {
+            const A r = A(t - d) / A(t);
+            const A v = r * r;
+            best = best < v ? v : best;
+        }
+    };
+    layer(x, g.sponge_inlet);
+    layer(g.nx - 1u - x, g.sponge_outlet);
+    if (g.y_lo != ORR_WALL_PERIODIC) {
+        layer(y, g.sponge_sides);
+        layer(g.ny - 1u - y, g.sponge_sides);
+    }
+    if (g.z_lo != ORR_WALL_PERIODIC) {
+        layer(z, g.sponge_sides);
+        layer(g.nz - 1u - z, g.sponge_sides);
+    }
+    return p.sponge_strength * best;
+}
+
+// Absorbing-layer relaxation towards f_eq(1, u_inlet)
+// (collide tail, lbm3d_cpu.cpp:94-99; lbm3_absorb, glsl:355-368).
+template <class A, bool kShifted>
+__device__ __forceinline__ void absorb3(A (&f)[d3::Q], A s, const A* inlet) {
+    const A ux = inlet[0], uy = inlet[1], uz = inlet[2];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
+        const A uu = ux * ux + uy * uy + uz * uz;
+        A target;
+        if constexpr (kShifted) {
+            target = A(d3::w(i)) * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu);
+        } else {
+            target = A(d3::w(i)) * A(1) * (A(1) + A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu);
+        }
+        f[i] -= s * (f[i] - target);
+    }
+}
+
+// Regularized Zou-He velocity inlet on the west face.
+// Shifted: lbm3_inlet_west (glsl:105-162).  Unshifted binary64:
+// velocity_inlet_west (lbm3d_internal.h:312-365), same operation order.
+template <class A, bool kShifted>
+__device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
+    const A ux = inlet[0], uy = inlet[1], uz = inlet[2];
+    A known = 0;
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        if (d3::cx(i) == 0) {
+            known += f[i];
+        } else if (d3::cx(i) < 0) {
+            known += A(2) * f[i];
+        }
+    }
+    A rho, drho;
+    if constexpr (kShifted) {
+        drho = (known + ux) / (A(1) - ux);
+        rho = A(1) + drho;
+    } else {
+        rho = known / (1.0 - ux);
+        drho = 0;
+    }
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        if (d3::cx(i) > 0) {
+            const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
+            f[i] = f[d3::opposite(i)] + A(6) * A(d3::w(i)) * rho * cu;
+        }
+    }
+    const A uu = ux * ux + uy * uy + uz * uz;
+    A feq[d3::Q];
+    A pi0 = 0, pi1 = 0, pi2 = 0, pi3 = 0, pi4 = 0, pi5 = 0;
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
+        const A cu = ex * ux + ey * uy + ez * uz;
+        if constexpr (kShifted) {
+            feq[i] = A(d3::w(i)) * (drho + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu));
+        } else {
+            feq[i] = A(d3::w(i)) * rho * (A(1) + A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu);
+        }
+        const A neq = f[i] - feq[i];
+        pi0 += ex * ex * neq;
+        pi1 += ey * ey * neq;
+        pi2 += ez * ez * neq;
+        pi3 += ex * ey * neq;
+        pi4 += ex * ez * neq;
+        pi5 += ey * ez * neq;
+    }
+    const A cs2 = A(1.0 / 3.0);
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
+        f[i] = feq[i] + A(4.5) * A(d3::w(i)) *
+                            ((ex * ex - cs2) * pi0 + (ey * ey - cs2) * pi1 + (ez * ez - cs2) * pi2 +
+                             A(2) * (ex * ey * pi3 + ex * ez * pi4 + ey * ez * pi5));
+    }
+}
+
+// ------------------------------------------------------------------- step --
+
+struct StepBuffers3D {
+    const uint8_t* cls;      // node classes
+    const uint32_t* bnode;   // boundary-node list (cells)
+    const int32_t* bslot;    // wall slot per boundary node, -1 none
+    const void* wall_q;      // 19 fractions per slot (arithmetic type)
+    void* hist;              // convective-outlet history (arithmetic type)
+    const void* inlet;       // imposed inlet velocity, 3 values (arithmetic type)
+};
+
+// The population `here` receives from the wall of its link i (reflected,
+// lbm3d_internal.h:181-197; lbm3_reflected, glsl:164-181).
+template <class S, int I>
+__device__ __forceinline__ typename Storage<S>::A reflected3(const S* __restrict__ src,
+                                                             uint64_t cells, uint64_t here,
+                                                             int64_t farther_off,
+                                                             typename Storage<S>::A q) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    constexpr int O = d3::opposite(I);
+    const A leaving = T::load(src + static_cast<uint64_t>(O) * cells + here);
+    if (q == A(0.5)) {
+        return leaving;
+    }
+    if (q < A(0.5)) {
+        const uint64_t farther = static_cast<uint64_t>(static_cast<int64_t>(here) + farther_off);
+        return A(2) * q * leaving + (A(1) - A(2) * q) * T::load(src + O * cells + farther);
+    }
+    return (leaving + (A(2) * q - A(1)) * T::load(src + static_cast<uint64_t>(I) * cells + here)) /
+           (A(2) * q);
+}
+
+// General gather of direction I at boundary node (x, y, z) (resolve_source,
+// lbm3d_internal.h:87-130, and the CPU's per-kind handling, lbm3d_cpu.cpp:281-312).
+template <class S, int I>
+__device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                            const S* __restrict__ src, const StepBuffers3D& b,
+                                            int32_t slot, int x, int y, int z, uint64_t here,
+                                            typename Storage<S>::A& wall_rho,
+                                            typename Storage<S>::A& out) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    constexpr int CX = d3::cx(I), CY = d3::cy(I), CZ = d3::cz(I);
+    constexpr int MY = d3::mirror_y(I);
+    constexpr int MZ = d3::mirror_z(I);
+    constexpr int MZY = d3::mirror_z(d3::mirror_y(I));
+    const uint64_t cells = g.cells;
+    int sx = x - CX, sy = y - CY, sz = z - CZ;
+    bool ymir = false, zmir = false;
+    int wall_side = -1;
+    if (CY != 0 && (sy < 0 || sy >= static_cast<int>(g.ny))) {
+        const int kind = sy < 0 ? g.y_lo : g.y_hi;
+        if (kind == ORR_WALL_PERIODIC) {
+            sy = sy < 0 ? static_cast<int>(g.ny) - 1 : 0;
+        } else if (kind == ORR_WALL_SLIP) {
+            sy = y;
+            ymir = true;
+        } else {
+            wall_side = sy < 0 ? 0 : 1;
+        }
+    }
+    if (wall_side < 0 && CZ != 0 && (sz < 0 || sz >= static_cast<int>(g.nz))) {
+        const int kind = sz < 0 ? g.z_lo : g.z_hi;
+        if (kind == ORR_WALL_PERIODIC) {
+            sz = sz < 0 ? static_cast<int>(g.nz) - 1 : 0;
+        } else if (kind == ORR_WALL_SLIP) {
+            sz = z;
+            zmir = true;
+        } else {
+            wall_side = sz < 0 ? 2 : 3;
+        }
+    }
+    if (wall_side >= 0) {
+        // No-slip domain wall: bounce-back plus the moving-wall term scaled
+        // by the node's own density at the previous step.
+        if (wall_rho < A(0)) {
+            A r = 0;
+#pragma unroll
+            for (int k = 0; k < d3::Q; ++k) r += T::load(src + static_cast<uint64_t>(k) * cells + here);
+            wall_rho = T::kShifted ? A(1) + r : r;
+        }
+        out = T::load(src + static_cast<uint64_t>(d3::opposite(I)) * cells + here) +
+              A(6) * A(d3::w(I)) * wall_rho * A(CX) * p.wall_ux[wall_side];
+        return;
+    }
+    const int dir = zmir ? (ymir ? MZY : MZ) : (ymir ? MY : I);
+    if (CX != 0 && (sx < 0 || sx >= static_cast<int>(g.nx))) {
+        if (g.x_mode == ORR_X_PERIODIC) {
+            sx = sx < 0 ? static_cast<int>(g.nx) - 1 : 0;
+        } else if (sx < 0) {
+            out = A(0); // reconstructed by the inlet
+            return;
+        } else {
+            // Outlet: the zero-gradient value, blended with the node's
+            // history by the convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).
+            const uint64_t face = (g.nx - 1u) + static_cast<uint64_t>(g.nx) *
+                                                    (static_cast<uint64_t>(sy) + static_cast<uint64_t>(g.ny) * sz);
+            const A up = T::load(src + static_cast<uint64_t>(dir) * cells + face);
+            if (g.outlet_mode == ORR_OUTLET_EXTRAPOLATION) {
+                out = up;
+            } else {
+                A* hist = static_cast<A*>(b.hist);
+                const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(I)) * g.ny * g.nz +
+                                   static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
+                const A u = p.outlet_speed;
+                const A v = (hist[k] + u * up) / (A(1) + u);
+                hist[k] = v;
+                out = v;
+            }
+            return;
+        }
+    }
+    const uint64_t source = static_cast<uint64_t>(sx) +
+                            static_cast<uint64_t>(g.nx) * (static_cast<uint64_t>(sy) +
+                                                           static_cast<uint64_t>(g.ny) * sz);
+    if (b.cls[source] == kSolid) {
+        const A q = slot >= 0 ? static_cast<const A*>(b.wall_q)[static_cast<uint64_t>(slot) * d3::Q + I]
+                              : A(0.5);
+        const int64_t farther_off = static_cast<int64_t>(CX) + static_cast<int64_t>(g.nx) * CY +
+                                    static_cast<int64_t>(g.plane) * CZ;
+        out = reflected3<S, I>(src, cells, here, farther_off, q);
+        return;
+    }
+    out = T::load(src + static_cast<uint64_t>(dir) * cells + source);
+}
+
+template <class S, int I>
+__device__ __forceinline__ void gather_all3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                            const S* __restrict__ src, const StepBuffers3D& b,
+                                            int32_t slot, int x, int y, int z, uint64_t here,
+                                            typename Storage<S>::A& wall_rho,
+                                            typename Storage<S>::A (&f)[d3::Q]) {
+    if constexpr (I < d3::Q) {
+        gather_one3<S, I>(g, p, src, b, slot, x, y, z, here, wall_rho, f[I]);
+        gather_all3<S, I + 1>(g, p, src, b, slot, x, y, z, here, wall_rho, f);
+    }
+}
+
+// Collision, absorbing layers and the 19 stores of one node.
+template <class S, bool kSmag>
+__device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                        const StepBuffers3D& b, typename Storage<S>::A (&f)[d3::Q],
+                                        uint32_t x, uint32_t y, uint32_t z, uint64_t here,
+                                        S* __restrict__ dst) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    A ux, uy, uz;
+    collide3<A, T::kShifted, kSmag>(f, p, g.forced, ux, uy, uz);
+    if (g.sponge) {
+        const A s = sponge_rate3<A>(g, p, x, y, z);
+        if (s > A(0)) {
+            absorb3<A, T::kShifted>(f, s, static_cast<const A*>(b.inlet));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        T::store(dst + static_cast<uint64_t>(i) * g.cells + here, f[i]);
+    }
+}
+
+// Bulk nodes: one thread per node of the interior rows y in [1, ny-2],
+// z in [1, nz-2]; block (tile, row) covers x in [tile * blockDim.x, ...).
+// Every source node is inside the lattice and fluid, so the gather is 19
+// plain pulls f_i(x) = f*_i(x - c_i) (lbm3d_cpu.cpp:272-276).
+template <class S, bool kSmag>
+__global__ void __launch_bounds__(256) bulk3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
+                                                     const S* __restrict__ src, S* __restrict__ dst,
+                                                     StepBuffers3D b) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint32_t row = blockIdx.x / g.tiles_x;
+    const uint32_t x = (blockIdx.x - row * g.tiles_x) * blockDim.x + threadIdx.x;
+    const uint32_t inner = g.ny - 2u;
+    const uint32_t y = 1u + row % inner;
+    const uint32_t z = 1u + row / inner;
+    if (x == 0 || x >= g.nx - 1u) {
+        return;
+    }
+    const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
+    if (b.cls[here] != kBulk) {
+        return;
+    }
+    const uint64_t cells = g.cells;
+    const int64_t nx = g.nx, plane = g.plane;
+    A f[d3::Q];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const int64_t off = d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i);
+        f[i] = T::load(src + static_cast<uint64_t>(i) * cells +
+                       static_cast<uint64_t>(static_cast<int64_t>(here) - off));
+    }
+    finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
+}
+
+// Boundary nodes: one thread per entry of the compact boundary-node list;
+// the general gather, then the inlet reconstruction on the west face.
+template <class S, bool kSmag>
+__global__ void __launch_bounds__(128) boundary3d_kernel(Geom3D g,
+                                                         Phys3D<typename Storage<S>::A> p,
+                                                         const S* __restrict__ src,
+                                                         S* __restrict__ dst, StepBuffers3D b) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.boundary_nodes) {
+        return;
+    }
+    const uint64_t here = b.bnode[k];
+    const uint32_t z = static_cast<uint32_t>(here / g.plane);
+    const uint32_t rest = static_cast<uint32_t>(here - static_cast<uint64_t>(z) * g.plane);
+    const uint32_t y = rest / g.nx;
+    const uint32_t x = rest - y * g.nx;
+    A f[d3::Q];
+    A wall_rho = A(-1);
+    gather_all3<S, 0>(g, p, src, b, b.bslot[k], static_cast<int>(x), static_cast<int>(y),
+                      static_cast<int>(z), here, wall_rho, f);
+    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0) {
+        inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
+    }
+    finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
+}
+
+// ------------------------------------------------------------ init / misc --
+
+// Equilibrium of (rho, u) at every node, solids at rest (initial_populations,
+// lbm3d_common.cpp:243-260); binary32 forms store f - w like the reference GPU
+// driver (lbm3d_gpu.cpp:298-305).  The field arrays may live in the other
+// population buffer (the solver stages them there), so they are read before
+// the node's own entries are written and never alias them.
+template <class S>
+__global__ void init3d_kernel(Geom3D g, const uint8_t* __restrict__ cls, const double* rho,
+                              const double* ux, const double* uy, const double* uz, double r0,
+                              double u0x, double u0y, double u0z, S* __restrict__ f0) {
+    using T = Storage<S>;
+    const uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= g.cells) {
+        return;
+    }
+    double r = 1.0, vx = 0.0, vy = 0.0, vz = 0.0;
+    if (cls[c] != kSolid) {
+        if (rho != nullptr) {
+            r = rho[c];
+            vx = ux[c];
+            vy = uy[c];
+            vz = uz[c];
+        } else {
+            r = r0;
+            vx = u0x;
+            vy = u0y;
+            vz = u0z;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const double cu = static_cast<double>(d3::cx(i)) * vx + static_cast<double>(d3::cy(i)) * vy +
+                          static_cast<double>(d3::cz(i)) * vz;
+        const double uu = vx * vx + vy * vy + vz * vz;
+        double feq = d3::w(i) * r * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * uu);
+        if (T::kShifted) {
+            feq -= d3::w(i);
+        }
+        f0[static_cast<uint64_t>(i) * g.cells + c] = T::encode(feq);
+    }
+}
+
+// Convective-outlet history from the populations entering the outlet face
+// (reset_outlet, lbm3d_cpu.cpp:225-237; lbm3d_gpu.cpp:311-323).
+template <class S>
+__global__ void history3d_kernel(Geom3D g, const S* __restrict__ f,
+                                 typename Storage<S>::A* __restrict__ hist) {
+    using T = Storage<S>;
+    const uint32_t face = g.ny * g.nz;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= face) {
+        return;
+    }
+    const uint32_t y = k % g.ny, z = k / g.ny;
+    const uint64_t cell = (g.nx - 1u) + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
+    constexpr int dirs[5] = {2, 8, 10, 12, 14};
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        hist[static_cast<uint64_t>(d3::outlet_slot(dirs[s])) * face + y + static_cast<uint64_t>(g.ny) * z] =
+            T::load(f + static_cast<uint64_t>(dirs[s]) * g.cells + cell);
+    }
+}
+
+// Moments of the stored post-collision populations: rho (rho - 1 for the
+// shifted forms) and the velocity with the Guo half-force correction; solids
+// report rest (lbm_d3q19_moments.comp.glsl; CpuLbm3D::macroscopic,
+// lbm3d_cpu.cpp:154-186).
+template <class S>
+__global__ void moments3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
+                                 const uint8_t* __restrict__ cls, const S* __restrict__ f,
+                                 typename Storage<S>::A* __restrict__ m) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= g.cells) {
+        return;
+    }
+    A r = T::kShifted ? A(0) : A(1), ux = 0, uy = 0, uz = 0;
+    if (cls[c] != kSolid) {
+        A v[d3::Q];
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) v[i] = T::load(f + static_cast<uint64_t>(i) * g.cells + c);
+        A s = 0;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) s += v[i];
+        const A jx = v[1] - v[2] + v[7] - v[8] + v[9] - v[10] + v[11] - v[12] + v[13] - v[14];
+        const A jy = v[3] - v[4] + v[7] - v[8] - v[9] + v[10] + v[15] - v[16] + v[17] - v[18];
+        const A jz = v[5] - v[6] + v[11] - v[12] - v[13] + v[14] + v[15] - v[16] - v[17] + v[18];
+        const A rho = T::kShifted ? A(1) + s : s;
+        r = s;
+        ux = (jx - A(0.5) * p.fx) / rho;
+        uy = (jy - A(0.5) * p.fy) / rho;
+        uz = (jz - A(0.5) * p.fz) / rho;
+    }
+    m[c] = r;
+    m[g.cells + c] = ux;
+    m[2 * g.cells + c] = uy;
+    m[3 * g.cells + c] = uz;
+}
+
+// Block-wide sum of N doubles per thread, then one atomicAdd per value per
+// block into `out`.
+template <int N>
+__device__ __forceinline__ void block_reduce_add(double (&v)[N], double* out) {
+    __shared__ double part[N][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) part[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            double s = lane < warps ? part[k][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) atomicAdd(out + k, s);
+        }
+    }
+}
+
+// Momentum exchange over the boundary links, summed in binary64: force
+// sum c_o (f*_o(x) + f_j(x, t+1)) and moment sum r x F at the wall point
+// x - q c_j (CpuLbm3D::force, lbm3d_cpu.cpp:192-203; add_link_force and
+// link_wall_point, lbm3d_common.cpp:213-241; lbm_d3q19_force.comp.glsl).
+template <class S>
+__global__ void force3d_kernel(Geom3D g, const S* __restrict__ f, const uint32_t* __restrict__ lcell,
+                               const uint32_t* __restrict__ ldir, const double* __restrict__ lq,
+                               uint64_t links, double* __restrict__ out) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < links;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t h = lcell[k];
+        const int j = static_cast<int>(ldir[k]);
+        const int o = opposite_rt(j);
+        const double q = lq[k];
+        int jx, jy, jz;
+        c_rt(j, jx, jy, jz);
+        const A leaving = T::load(f + static_cast<uint64_t>(o) * g.cells + h);
+        A back;
+        const A qa = static_cast<A>(q);
+        if (q == 0.5) {
+            back = leaving;
+        } else if (q < 0.5) {
+            const uint64_t farther = static_cast<uint64_t>(
+                static_cast<int64_t>(h) + jx + static_cast<int64_t>(g.nx) * jy +
+                static_cast<int64_t>(g.plane) * jz);
+            back = A(2) * qa * leaving + (A(1) - A(2) * qa) * T::load(f + static_cast<uint64_t>(o) * g.cells + farther);
+        } else {
+            back = (leaving + (A(2) * qa - A(1)) * T::load(f + static_cast<uint64_t>(j) * g.cells + h)) /
+                   (A(2) * qa);
+        }
+        double ex = static_cast<double>(leaving) + static_cast<double>(back);
+        if (T::kShifted) {
+            ex += 2.0 * w_rt(o);
+        }
+        // c_o = -c_j
+        const double fx = -jx * ex, fy = -jy * ex, fz = -jz * ex;
+        const uint32_t z = static_cast<uint32_t>(h / g.plane);
+        const uint32_t rest = static_cast<uint32_t>(h - static_cast<uint64_t>(z) * g.plane);
+        const uint32_t y = rest / g.nx, x = rest - y * g.nx;
+        const double rx = static_cast<double>(x) - q * jx;
+        const double ry = static_cast<double>(y) - q * jy;
+        const double rz = static_cast<double>(z) - q * jz;
+        acc[0] += fx;
+        acc[1] += fy;
+        acc[2] += fz;
+        acc[3] += ry * fz - rz * fy;
+        acc[4] += rz * fx - rx * fz;
+        acc[5] += rx * fy - ry * fx;
+    }
+    block_reduce_add<6>(acc, out);
+}
+
+// Sum of the stored populations over fluid nodes in binary64 (the shifted
+// forms add the node count on the host; CpuLbm3D::mass, lbm3d_cpu.cpp:205-215).
+template <class S>
+__global__ void mass3d_kernel(Geom3D g, const uint8_t* __restrict__ cls, const S* __restrict__ f,
+                              double* __restrict__ out) {
+    using T = Storage<S>;
+    double acc[1] = {0.0};
+    for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < g.cells;
+         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (cls[c] != kSolid) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) s += static_cast<double>(T::load(f + static_cast<uint64_t>(i) * g.cells + c));
+            acc[0] += s;
+        }
+    }
+    block_reduce_add<1>(acc, out);
+}
+
+} // namespace orr

@@ -1,0 +1,35 @@
+// Per-storage launch table of the D2Q9 kernels (instantiated next to the
+// D3Q19 ones in kernels_binary32.cu and kernels_binary64.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace orr {
+
+struct Geom2D;
+struct StepBuffers2D;
+
+struct Ops2D {
+    cudaError_t (*bulk)(const Geom2D& g, const void* phys, const void* src, void* dst,
+                        const StepBuffers2D& b, bool smag, uint32_t block, cudaStream_t s);
+    cudaError_t (*boundary)(const Geom2D& g, const void* phys, const void* src, void* dst,
+                            const StepBuffers2D& b, bool smag, cudaStream_t s);
+    cudaError_t (*init)(const Geom2D& g, const uint8_t* cls, const double* rho, const double* ux,
+                        const double* uy, double u0x, double u0y, void* f0, cudaStream_t s);
+    cudaError_t (*history)(const Geom2D& g, const void* f, void* hist, cudaStream_t s);
+    cudaError_t (*moments)(const Geom2D& g, const void* phys, const uint8_t* cls, const void* f,
+                           void* m, cudaStream_t s);
+    cudaError_t (*force)(const Geom2D& g, const void* f, const uint32_t* lcell,
+                         const uint32_t* ldir, uint64_t links, double* out, cudaStream_t s);
+    cudaError_t (*mass)(const Geom2D& g, const uint8_t* cls, const void* f, double* out,
+                        cudaStream_t s);
+};
+
+const Ops2D& ops2d_f32();
+const Ops2D& ops2d_f16();
+const Ops2D& ops2d_bf16();
+const Ops2D& ops2d_f64();
+
+} // namespace orr

@@ -1,0 +1,576 @@
+// Host-side planning and validation of D3Q19 and D2Q9 lattices.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <iomanip>
+#include <limits>
+#include <sstream>
+
+#include "lattice.h"
+
+namespace orr {
+
+namespace {
+
+constexpr double kMaxLatticeMach = 0.1; // max_lattice_mach (lattice_units.h:22)
+
+bool finite(double v) {
+    return std::isfinite(v);
+}
+
+double lattice_mach(double speed) {
+    // lattice_mach (src/aero/lbm/lattice_units.cpp:19-21): |u| / sqrt(c_s^2).
+    return std::abs(speed) / std::sqrt(1.0 / 3.0);
+}
+
+// check_mach (lbm3d_common.cpp:21-30; lbm2d_common.cpp:18-27).
+std::string check_mach(const char* family, const char* what, double speed) {
+    if (!(lattice_mach(speed) < kMaxLatticeMach)) {
+        std::ostringstream m;
+        m << family << ": " << what << " " << speed << " has lattice Mach number "
+          << lattice_mach(speed) << ", not below " << kMaxLatticeMach << " (APPROXIMATION A3)";
+        return m.str();
+    }
+    return {};
+}
+
+// a * b without wrapping.
+bool mul(std::size_t a, std::size_t b, std::size_t& out) {
+    if (a != 0 && b > std::numeric_limits<std::size_t>::max() / a) {
+        return false;
+    }
+    out = a * b;
+    return true;
+}
+
+bool add(std::size_t a, std::size_t b, std::size_t& out) {
+    if (b > std::numeric_limits<std::size_t>::max() - a) {
+        return false;
+    }
+    out = a + b;
+    return true;
+}
+
+// lattice_cells_3d (src/aero/lbm3d/solid_mask3d.cpp:22-36).
+std::optional<std::size_t> cells3d(std::size_t nx, std::size_t ny, std::size_t nz) {
+    std::size_t plane = 0, cells = 0;
+    if (nx == 0 || ny == 0 || nz == 0 || !mul(nx, ny, plane) || !mul(plane, nz, cells) ||
+        cells > kMaxGridCells) {
+        return std::nullopt;
+    }
+    return cells;
+}
+
+bool binary32_storage(int32_t storage) {
+    return storage != ORR_STORAGE_F64;
+}
+
+// The kernels see every real parameter rounded to binary32
+// (check_binary32, lbm3d_gpu.cpp:91-127).
+float to_float32(double v) {
+    if (std::abs(v) > static_cast<double>(std::numeric_limits<float>::max())) {
+        return v > 0.0 ? std::numeric_limits<float>::infinity()
+                       : -std::numeric_limits<float>::infinity();
+    }
+    return static_cast<float>(v);
+}
+
+struct Param {
+    const char* name;
+    double value;
+};
+
+std::string binary32_problem(const char* family, const Param* params, std::size_t n, double tau) {
+    for (std::size_t k = 0; k < n; ++k) {
+        if (!std::isfinite(to_float32(params[k].value))) {
+            std::ostringstream m;
+            m << family << " gpu: " << params[k].name << " " << params[k].value
+              << " is outside the binary32 range of the kernels";
+            return m.str();
+        }
+    }
+    if (!(static_cast<double>(to_float32(tau)) > 0.5)) {
+        std::ostringstream m;
+        m << std::setprecision(17) << family << " gpu: tau " << tau
+          << " rounds to 1/2 in binary32 (zero viscosity in the kernels); tau - 1/2 must "
+             "exceed 2^-25 (about 3e-8)";
+        return m.str();
+    }
+    return {};
+}
+
+} // namespace
+
+std::size_t storage_bytes(int32_t storage) {
+    switch (storage) {
+        case ORR_STORAGE_F16:
+        case ORR_STORAGE_BF16:
+            return 2;
+        case ORR_STORAGE_F64:
+            return 8;
+        default:
+            return 4;
+    }
+}
+
+std::size_t arithmetic_bytes(int32_t storage) {
+    return storage == ORR_STORAGE_F64 ? 8 : 4;
+}
+
+std::string mebibytes(std::size_t bytes) {
+    std::ostringstream out;
+    out << std::fixed << std::setprecision(1) << static_cast<double>(bytes) / (1024.0 * 1024.0)
+        << " MiB";
+    return out.str();
+}
+
+std::string problem3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* distance,
+                      int32_t storage, bool allow_high_mach) {
+    if (storage < ORR_STORAGE_F32 || storage > ORR_STORAGE_F64) {
+        return "lbm3d gpu: unknown population storage";
+    }
+    if (c.nx < 3 || c.ny < 3 || c.nz < 3) {
+        return "lbm3d: the lattice needs at least 3 nodes along each axis";
+    }
+    const auto cells = cells3d(c.nx, c.ny, c.nz);
+    if (!cells) {
+        return "lbm3d: more than geom::max_grid_cells nodes";
+    }
+    if (solid == nullptr) {
+        return "lbm3d: the solid mask does not match the lattice size";
+    }
+    if (!finite(c.tau) || !(c.tau > 0.5)) {
+        return "lbm3d: tau must be finite and above 1/2 (positive viscosity)";
+    }
+    for (const double v : {c.inlet_ux, c.inlet_uy, c.inlet_uz, c.body_force_x, c.body_force_y,
+                           c.body_force_z, c.y_low.velocity_x, c.y_high.velocity_x,
+                           c.z_low.velocity_x, c.z_high.velocity_x}) {
+        if (!finite(v)) {
+            return "lbm3d: velocities and body force must be finite";
+        }
+    }
+    if (c.smagorinsky_enabled &&
+        (!finite(c.smagorinsky_constant) || c.smagorinsky_constant < 0.0)) {
+        return "lbm3d: the Smagorinsky constant must be finite and non-negative";
+    }
+    for (const orr_wall* w : {&c.y_low, &c.y_high, &c.z_low, &c.z_high}) {
+        if (w->kind < ORR_WALL_PERIODIC || w->kind > ORR_WALL_NO_SLIP) {
+            return "lbm3d: unknown wall kind";
+        }
+    }
+    if ((c.y_low.kind == ORR_WALL_PERIODIC) != (c.y_high.kind == ORR_WALL_PERIODIC) ||
+        (c.z_low.kind == ORR_WALL_PERIODIC) != (c.z_high.kind == ORR_WALL_PERIODIC)) {
+        return "lbm3d: an axis is periodic on both sides or on neither";
+    }
+    if (!allow_high_mach) {
+        const struct {
+            const char* name;
+            double speed;
+        } sides[] = {{"y = 0 wall speed", c.y_low.velocity_x},
+                     {"y = ny - 1 wall speed", c.y_high.velocity_x},
+                     {"z = 0 wall speed", c.z_low.velocity_x},
+                     {"z = nz - 1 wall speed", c.z_high.velocity_x}};
+        for (const auto& s : sides) {
+            if (std::string bad = check_mach("lbm3d", s.name, s.speed); !bad.empty()) {
+                return bad;
+            }
+        }
+    }
+    if (!finite(c.sponge_strength) || c.sponge_strength < 0.0 || c.sponge_strength > 1.0) {
+        return "lbm3d: the absorbing-layer strength must be in [0, 1]";
+    }
+    if (c.sponge_strength > 0.0 &&
+        (c.x_boundary != ORR_X_INFLOW_OUTFLOW || c.sponge_inlet > c.nx || c.sponge_outlet > c.nx ||
+         c.sponge_sides > std::min(c.ny, c.nz))) {
+        return "lbm3d: absorbing layers need the inflow/outflow x boundary and must fit in the "
+               "lattice";
+    }
+    if (c.solid_wall == ORR_SOLID_INTERPOLATED) {
+        if (distance == nullptr) {
+            return "lbm3d: the interpolated wall needs the mask's signed distance";
+        }
+        for (std::size_t k = 0; k < *cells; ++k) {
+            if (std::isnan(distance[k])) {
+                return "lbm3d: the mask's signed distance must not be NaN";
+            }
+        }
+    } else if (c.solid_wall != ORR_SOLID_HALFWAY) {
+        return "lbm3d: unknown solid wall treatment";
+    }
+    if (c.x_boundary == ORR_X_INFLOW_OUTFLOW) {
+        if (!allow_high_mach) {
+            const double speed = std::sqrt(c.inlet_ux * c.inlet_ux + c.inlet_uy * c.inlet_uy +
+                                           c.inlet_uz * c.inlet_uz);
+            if (std::string bad = check_mach("lbm3d", "inlet speed", speed); !bad.empty()) {
+                return bad;
+            }
+        }
+        for (std::size_t z = 0; z < c.nz; ++z) {
+            for (std::size_t y = 0; y < c.ny; ++y) {
+                const std::size_t row = c.nx * (y + c.ny * z);
+                if (solid[row] != 0 || solid[row + c.nx - 1] != 0) {
+                    return "lbm3d: the inlet and outlet faces must be fluid";
+                }
+            }
+        }
+        if (c.outlet == ORR_OUTLET_CONVECTIVE && !(c.inlet_ux > 0.0)) {
+            return "lbm3d: the convective outlet needs a positive inlet speed";
+        }
+    } else if (c.x_boundary != ORR_X_PERIODIC) {
+        return "lbm3d: unknown x boundary";
+    }
+    // make_gpu_solver's bound on the kernels' 32-bit indices (lbm3d_gpu.cpp:492-497).
+    if (*cells > std::numeric_limits<uint32_t>::max() / static_cast<std::size_t>(d3::Q)) {
+        return "lbm3d gpu: lattice too large for 32-bit indices";
+    }
+    if (binary32_storage(storage)) {
+        const double k = c.smagorinsky_enabled ? c.smagorinsky_constant : 0.0;
+        const Param params[] = {{"tau", c.tau},
+                                {"y = 0 wall speed", c.y_low.velocity_x},
+                                {"y = ny - 1 wall speed", c.y_high.velocity_x},
+                                {"z = 0 wall speed", c.z_low.velocity_x},
+                                {"z = nz - 1 wall speed", c.z_high.velocity_x},
+                                {"inlet x velocity", c.inlet_ux},
+                                {"inlet y velocity", c.inlet_uy},
+                                {"inlet z velocity", c.inlet_uz},
+                                {"squared Smagorinsky constant", k * k},
+                                {"body force x", c.body_force_x},
+                                {"body force y", c.body_force_y},
+                                {"body force z", c.body_force_z}};
+        if (std::string bad =
+                binary32_problem("lbm3d", params, sizeof(params) / sizeof(params[0]), c.tau);
+            !bad.empty()) {
+            return bad;
+        }
+    }
+    return {};
+}
+
+std::string inlet_problem3d(const orr_lbm3d_config& c, const double v[3], bool allow_high_mach) {
+    if (c.x_boundary != ORR_X_INFLOW_OUTFLOW) {
+        return "lbm3d: a periodic lattice has no inlet";
+    }
+    if (!finite(v[0]) || !finite(v[1]) || !finite(v[2])) {
+        return "lbm3d: the inlet velocity must be finite";
+    }
+    if (allow_high_mach) {
+        return {};
+    }
+    return check_mach("lbm3d", "inlet speed", std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+}
+
+namespace {
+
+// Where population i of node (x, y, z) comes from, reduced to what planning
+// needs: whether the source is a solid node inside the domain after the side
+// rules (resolve_source, lbm3d_internal.h:87-130).
+bool bounces3d(const orr_lbm3d_config& c, const uint8_t* solid, long x, long y, long z, int i) {
+    const long nx = static_cast<long>(c.nx), ny = static_cast<long>(c.ny),
+               nz = static_cast<long>(c.nz);
+    long sx = x - d3::cx(i), sy = y - d3::cy(i), sz = z - d3::cz(i);
+    const auto side = [](const orr_wall& lo, const orr_wall& hi, long& s, long n, long own) {
+        if (s >= 0 && s < n) {
+            return false;
+        }
+        const orr_wall& w = s < 0 ? lo : hi;
+        if (w.kind == ORR_WALL_PERIODIC) {
+            s = (s + n) % n;
+            return false;
+        }
+        if (w.kind == ORR_WALL_SLIP) {
+            s = own;
+            return false;
+        }
+        return true; // no-slip domain wall: not a solid-node link
+    };
+    if (side(c.y_low, c.y_high, sy, ny, y) || side(c.z_low, c.z_high, sz, nz, z)) {
+        return false;
+    }
+    if (sx < 0 || sx >= nx) {
+        if (c.x_boundary != ORR_X_PERIODIC) {
+            return false; // inlet or outlet
+        }
+        sx = (sx + nx) % nx;
+    }
+    return solid[static_cast<std::size_t>(sx + nx * (sy + ny * sz))] != 0;
+}
+
+// link_fraction (lbm3d_internal.h:132-179).
+double link_fraction3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* distance,
+                       long x, long y, long z, int i) {
+    if (c.solid_wall != ORR_SOLID_INTERPOLATED || distance == nullptr) {
+        return 0.5;
+    }
+    const long nx = static_cast<long>(c.nx), ny = static_cast<long>(c.ny),
+               nz = static_cast<long>(c.nz);
+    const auto inside = [&](long a, long b, long d) {
+        return a >= 0 && b >= 0 && d >= 0 && a < nx && b < ny && d < nz;
+    };
+    const auto at = [&](long a, long b, long d) {
+        return static_cast<std::size_t>(a + nx * (b + ny * d));
+    };
+    const long sx = x - d3::cx(i), sy = y - d3::cy(i), sz = z - d3::cz(i);
+    if (!inside(sx, sy, sz)) {
+        return 0.5;
+    }
+    const double df = distance[at(x, y, z)];
+    const double ds = distance[at(sx, sy, sz)];
+    if (!std::isfinite(df) || !std::isfinite(ds) || df < 0.0 || ds > 0.0 ||
+        (df == 0.0 && ds == 0.0)) {
+        return 0.5;
+    }
+    const double span = df - ds;
+    const double ratio = std::isfinite(span) ? df / span : 0.5 * df / (0.5 * df - 0.5 * ds);
+    const double q = std::min(ratio, 1.0);
+    if (q < 0.5) {
+        const long fx = x + d3::cx(i), fy = y + d3::cy(i), fz = z + d3::cz(i);
+        if (!inside(fx, fy, fz) || solid[at(fx, fy, fz)] != 0) {
+            return 0.5;
+        }
+    }
+    return q;
+}
+
+} // namespace
+
+Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* distance) {
+    Plan3D p;
+    p.c = c;
+    const long nx = static_cast<long>(c.nx), ny = static_cast<long>(c.ny),
+               nz = static_cast<long>(c.nz);
+    p.cells = static_cast<std::size_t>(nx * ny * nz);
+    p.cls.assign(p.cells, kBulk);
+    const long plane = nx * ny;
+    long off[d3::Q];
+    for (int i = 0; i < d3::Q; ++i) {
+        off[i] = -d3::cx(i) - nx * d3::cy(i) - plane * d3::cz(i);
+    }
+    for (long z = 0; z < nz; ++z) {
+        for (long y = 0; y < ny; ++y) {
+            for (long x = 0; x < nx; ++x) {
+                const std::size_t h = static_cast<std::size_t>(x + nx * (y + ny * z));
+                if (solid[h] != 0) {
+                    p.cls[h] = kSolid;
+                    continue;
+                }
+                ++p.fluid;
+                bool boundary = x == 0 || y == 0 || z == 0 || x + 1 == nx || y + 1 == ny ||
+                                z + 1 == nz;
+                for (int i = 1; i < d3::Q && !boundary; ++i) {
+                    boundary = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+                }
+                if (boundary) {
+                    p.cls[h] = kBoundary;
+                    p.bnode.push_back(static_cast<uint32_t>(h));
+                }
+            }
+        }
+    }
+    // Links of the boundary nodes in scan order; bulk nodes have none.
+    const bool interpolated = c.solid_wall == ORR_SOLID_INTERPOLATED;
+    p.bslot.assign(p.bnode.size(), -1);
+    for (std::size_t b = 0; b < p.bnode.size(); ++b) {
+        const std::size_t h = p.bnode[b];
+        const long z = static_cast<long>(h / static_cast<std::size_t>(plane));
+        const long rest = static_cast<long>(h % static_cast<std::size_t>(plane));
+        const long y = rest / nx, x = rest % nx;
+        for (int i = 1; i < d3::Q; ++i) {
+            if (!bounces3d(c, solid, x, y, z, i)) {
+                continue;
+            }
+            const double q = link_fraction3d(c, solid, distance, x, y, z, i);
+            p.link_cell.push_back(static_cast<uint32_t>(h));
+            p.link_dir.push_back(static_cast<uint32_t>(i));
+            p.link_q.push_back(q);
+            if (interpolated) {
+                if (p.bslot[b] < 0) {
+                    p.bslot[b] = static_cast<int32_t>(p.wall_q.size() / d3::Q);
+                    p.wall_q.insert(p.wall_q.end(), d3::Q, 0.5);
+                }
+                p.wall_q[static_cast<std::size_t>(p.bslot[b]) * d3::Q + static_cast<std::size_t>(i)] =
+                    q;
+            }
+        }
+    }
+    return p;
+}
+
+std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links,
+                                    std::size_t boundary_nodes, std::size_t wall_slots,
+                                    int32_t storage) {
+    const auto cells = cells3d(c.nx, c.ny, c.nz);
+    if (!cells) {
+        return std::nullopt;
+    }
+    const std::size_t s = storage_bytes(storage), a = arithmetic_bytes(storage);
+    std::size_t total = 0, t = 0;
+    // Two population buffers.
+    if (!mul(*cells, d3::Q * s * 2, t) || !add(total, t, total)) return std::nullopt;
+    // Node classes (one byte) and four moment planes.
+    if (!mul(*cells, 1 + 4 * a, t) || !add(total, t, total)) return std::nullopt;
+    // Outlet history.
+    std::size_t face = 0;
+    if (!mul(c.ny, c.nz, face) || !mul(face, d3::kOutletSlots * a, t) || !add(total, t, total))
+        return std::nullopt;
+    // Boundary-node list (cell and wall slot) and wall fractions.
+    if (!mul(boundary_nodes, 8, t) || !add(total, t, total)) return std::nullopt;
+    if (!mul(std::max<std::size_t>(wall_slots, 1), d3::Q * a, t) || !add(total, t, total))
+        return std::nullopt;
+    // Links: cell, direction, fraction.
+    if (!mul(links, 16, t) || !add(total, t, total)) return std::nullopt;
+    // Force, mass and inlet buffers.
+    if (!add(total, 256, total)) return std::nullopt;
+    return total;
+}
+
+// ---- D2Q9 ----
+
+std::string problem2d(const orr_lbm2d_config& c, const uint8_t* solid, int32_t storage,
+                      bool allow_high_mach) {
+    if (storage < ORR_STORAGE_F32 || storage > ORR_STORAGE_F64) {
+        return "lbm2d gpu: unknown population storage";
+    }
+    if (c.nx < 3 || c.ny < 3) {
+        return "lbm2d: the lattice needs at least 3 x 3 nodes";
+    }
+    if (c.nx > kMaxGridCells / c.ny) {
+        return "lbm2d: more than geom::max_grid_cells nodes";
+    }
+    if (solid == nullptr) {
+        return "lbm2d: the solid mask does not match the lattice size";
+    }
+    if (!finite(c.tau) || !(c.tau > 0.5)) {
+        return "lbm2d: tau must be finite and above 1/2 (positive viscosity)";
+    }
+    if (!finite(c.inlet_ux) || !finite(c.inlet_uy) || !finite(c.body_force_x) ||
+        !finite(c.body_force_y) || !finite(c.bottom.velocity_x) || !finite(c.top.velocity_x)) {
+        return "lbm2d: velocities and body force must be finite";
+    }
+    if (c.smagorinsky_enabled &&
+        (!finite(c.smagorinsky_constant) || c.smagorinsky_constant < 0.0)) {
+        return "lbm2d: the Smagorinsky constant must be finite and non-negative";
+    }
+    for (const orr_wall* w : {&c.bottom, &c.top}) {
+        if (w->kind < ORR_WALL_PERIODIC || w->kind > ORR_WALL_NO_SLIP) {
+            return "lbm2d: unknown wall kind";
+        }
+    }
+    if ((c.bottom.kind == ORR_WALL_PERIODIC) != (c.top.kind == ORR_WALL_PERIODIC)) {
+        return "lbm2d: y is periodic on both sides or on neither";
+    }
+    if (!allow_high_mach) {
+        if (std::string bad = check_mach("lbm2d", "bottom wall speed", c.bottom.velocity_x);
+            !bad.empty()) {
+            return bad;
+        }
+        if (std::string bad = check_mach("lbm2d", "top wall speed", c.top.velocity_x);
+            !bad.empty()) {
+            return bad;
+        }
+    }
+    if (c.x_boundary == ORR_X_INFLOW_OUTFLOW) {
+        if (!allow_high_mach) {
+            if (std::string bad =
+                    check_mach("lbm2d", "inlet speed", std::hypot(c.inlet_ux, c.inlet_uy));
+                !bad.empty()) {
+                return bad;
+            }
+        }
+        for (std::size_t y = 0; y < c.ny; ++y) {
+            if (solid[c.nx * y] != 0 || solid[c.nx - 1 + c.nx * y] != 0) {
+                return "lbm2d: the inlet and outlet columns must be fluid";
+            }
+        }
+        if (c.outlet == ORR_OUTLET_CONVECTIVE && !(c.inlet_ux > 0.0)) {
+            return "lbm2d: the convective outlet needs a positive inlet speed";
+        }
+    } else if (c.x_boundary != ORR_X_PERIODIC) {
+        return "lbm2d: unknown x boundary";
+    }
+    if (binary32_storage(storage)) {
+        const double k = c.smagorinsky_enabled ? c.smagorinsky_constant : 0.0;
+        const Param params[] = {{"tau", c.tau},
+                                {"bottom wall speed", c.bottom.velocity_x},
+                                {"top wall speed", c.top.velocity_x},
+                                {"inlet x velocity", c.inlet_ux},
+                                {"inlet y velocity", c.inlet_uy},
+                                {"squared Smagorinsky constant", k * k},
+                                {"body force x", c.body_force_x},
+                                {"body force y", c.body_force_y}};
+        if (std::string bad =
+                binary32_problem("lbm2d", params, sizeof(params) / sizeof(params[0]), c.tau);
+            !bad.empty()) {
+            return bad;
+        }
+    }
+    return {};
+}
+
+Plan2D plan2d(const orr_lbm2d_config& c, const uint8_t* solid) {
+    Plan2D p;
+    p.c = c;
+    const long nx = static_cast<long>(c.nx), ny = static_cast<long>(c.ny);
+    p.cells = static_cast<std::size_t>(nx * ny);
+    p.cls.assign(p.cells, kBulk);
+    long off[d2::Q];
+    for (int i = 0; i < d2::Q; ++i) {
+        off[i] = -d2::cx(i) - nx * d2::cy(i);
+    }
+    for (long y = 0; y < ny; ++y) {
+        for (long x = 0; x < nx; ++x) {
+            const std::size_t h = static_cast<std::size_t>(x + nx * y);
+            if (solid[h] != 0) {
+                p.cls[h] = kSolid;
+                continue;
+            }
+            ++p.fluid;
+            bool boundary = x == 0 || y == 0 || x + 1 == nx || y + 1 == ny;
+            for (int i = 1; i < d2::Q && !boundary; ++i) {
+                boundary = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+            }
+            if (boundary) {
+                p.cls[h] = kBoundary;
+                p.bnode.push_back(static_cast<uint32_t>(h));
+            }
+        }
+    }
+    // boundary_links (lbm2d_common.cpp:79-97) over the boundary nodes.
+    for (const uint32_t h : p.bnode) {
+        const long x = static_cast<long>(h) % nx, y = static_cast<long>(h) / nx;
+        for (int i = 1; i < d2::Q; ++i) {
+            long sx = x - d2::cx(i), sy = y - d2::cy(i);
+            if (sy < 0 || sy >= ny) {
+                const orr_wall& w = sy < 0 ? c.bottom : c.top;
+                if (w.kind == ORR_WALL_NO_SLIP) {
+                    continue;
+                }
+                sy = w.kind == ORR_WALL_PERIODIC ? (sy + ny) % ny : y;
+            }
+            if (sx < 0 || sx >= nx) {
+                if (c.x_boundary != ORR_X_PERIODIC) {
+                    continue;
+                }
+                sx = (sx + nx) % nx;
+            }
+            if (solid[static_cast<std::size_t>(sx + nx * sy)] != 0) {
+                p.link_cell.push_back(h);
+                p.link_dir.push_back(static_cast<uint32_t>(i));
+            }
+        }
+    }
+    return p;
+}
+
+std::optional<std::size_t> memory2d(const orr_lbm2d_config& c, std::size_t links,
+                                    std::size_t boundary_nodes, int32_t storage) {
+    if (c.nx == 0 || c.ny == 0 || c.nx > kMaxGridCells / c.ny) {
+        return std::nullopt;
+    }
+    const std::size_t cells = c.nx * c.ny;
+    const std::size_t s = storage_bytes(storage), a = arithmetic_bytes(storage);
+    return cells * (d2::Q * s * 2 + 1 + 3 * a) + c.ny * d2::kOutletSlots * a +
+           boundary_nodes * 4 + links * 8 + 256;
+}
+
+} // namespace orr

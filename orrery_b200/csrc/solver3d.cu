@@ -1,0 +1,742 @@
+// The D3Q19 device solver behind the C ABI: the counterpart of the
+// reference's GpuLbm3D (src/aero/lbm3d/lbm3d_gpu.cpp:151-483) and
+// make_gpu_solver (:487-513), on CUDA instead of an IComputeBackend.
+//
+// Device layout (one allocation per table):
+//   populations   two buffers of 19 * cells storage values, structure of
+//                 arrays f[i * cells + x + nx (y + ny z)]; ping-pong (A-B)
+//   classes       one byte per node (solid / bulk / boundary)
+//   boundary list cell and wall slot of every boundary fluid node
+//   wall table    19 fractions per slot (interpolated wall)
+//   links         cell, direction and fraction of every boundary link
+//   moments       4 planes (rho or rho - 1, ux, uy, uz) for read-back
+//   history       5 * ny * nz convective-outlet values
+//   small         inlet velocity (3), force/moment (6) and mass accumulators
+// Steps run as CUDA graphs of kGraphSteps steps, each step a fork into the
+// boundary kernel (side stream) and the bulk kernel (main stream).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "kernels3d.cuh"
+#include "lattice.h"
+#include "ops3d.h"
+#include "plan.h"
+
+namespace {
+
+using namespace orr;
+
+constexpr uint32_t kGraphSteps = 16; // even: a graph returns to the buffer it started on
+constexpr uint32_t kDefaultBlock = 128;
+
+template <class T> T* device_alloc(std::size_t count, const char* what) {
+    void* p = nullptr;
+    check(cudaMalloc(&p, std::max<std::size_t>(count, 1) * sizeof(T)), what);
+    return static_cast<T*>(p);
+}
+
+const Ops3D& ops_for(int32_t storage) {
+    switch (storage) {
+        case ORR_STORAGE_F16:
+            return ops3d_f16();
+        case ORR_STORAGE_BF16:
+            return ops3d_bf16();
+        case ORR_STORAGE_F64:
+            return ops3d_f64();
+        default:
+            return ops3d_f32();
+    }
+}
+
+float to_f32(double v) {
+    return static_cast<float>(v);
+}
+
+} // namespace
+
+struct orr_lbm3d {
+    Plan3D plan;
+    int32_t storage = ORR_STORAGE_F32;
+    bool allow_high_mach = false;
+    int device = 0;
+    uint32_t block = kDefaultBlock;
+    const Ops3D* ops = nullptr;
+    Geom3D g{};
+    Phys3D<float> phys32{};
+    Phys3D<double> phys64{};
+    bool smag = false;
+    std::size_t sbytes = 4;
+    std::size_t abytes = 4;
+
+    cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join = nullptr;
+    cudaGraphExec_t graph = nullptr;
+
+    void* f[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t* cls = nullptr;
+    uint32_t* bnode = nullptr;
+    int32_t* bslot = nullptr;
+    void* wall_q = nullptr;
+    void* hist = nullptr;
+    void* moments = nullptr;
+    uint32_t* lcell = nullptr;
+    uint32_t* ldir = nullptr;
+    double* lq = nullptr;
+    void* small = nullptr;   // inlet (3 x arithmetic) at 0, accumulators at 64
+    double* host_small = nullptr; // pinned: inlet staging + results
+
+    uint64_t steps = 0;
+    uint64_t launches = 0;
+    double inlet[3] = {0.0, 0.0, 0.0};
+    std::string error;
+
+    const void* phys() const {
+        return storage == ORR_STORAGE_F64 ? static_cast<const void*>(&phys64)
+                                          : static_cast<const void*>(&phys32);
+    }
+    void* inlet_dev() const { return small; }
+    double* acc() const { return reinterpret_cast<double*>(static_cast<char*>(small) + 64); }
+
+    StepBuffers3D buffers() const {
+        StepBuffers3D b{};
+        b.cls = cls;
+        b.bnode = bnode;
+        b.bslot = bslot;
+        b.wall_q = wall_q;
+        b.hist = hist;
+        b.inlet = small;
+        return b;
+    }
+
+    ~orr_lbm3d() { release(); }
+
+    void release() noexcept {
+        if (device >= 0) {
+            cudaSetDevice(device);
+        }
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(bnode),
+                        static_cast<void*>(bslot), wall_q, hist, moments,
+                        static_cast<void*>(lcell), static_cast<void*>(ldir),
+                        static_cast<void*>(lq), small}) {
+            if (p) cudaFree(p);
+        }
+        if (host_small) cudaFreeHost(host_small);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
+        if (stream) cudaStreamDestroy(stream);
+        graph = nullptr;
+        f[0] = f[1] = nullptr;
+        cls = nullptr;
+        bnode = nullptr;
+        bslot = nullptr;
+        wall_q = hist = moments = small = nullptr;
+        lcell = ldir = nullptr;
+        lq = nullptr;
+        host_small = nullptr;
+        fork = join = nullptr;
+        side = stream = nullptr;
+    }
+
+    // Uploads the imposed inlet velocity in the arithmetic type.
+    void upload_inlet(const double v[3]) {
+        inlet[0] = v[0];
+        inlet[1] = v[1];
+        inlet[2] = v[2];
+        check(cudaStreamSynchronize(stream), "inlet upload");
+        if (storage == ORR_STORAGE_F64) {
+            std::memcpy(host_small, v, 3 * sizeof(double));
+        } else {
+            float* h = reinterpret_cast<float*>(host_small);
+            h[0] = to_f32(v[0]);
+            h[1] = to_f32(v[1]);
+            h[2] = to_f32(v[2]);
+        }
+        check(cudaMemcpyAsync(small, host_small, 3 * abytes, cudaMemcpyHostToDevice, stream),
+              "inlet upload");
+        check(cudaStreamSynchronize(stream), "inlet upload");
+    }
+
+    // One step src -> dst on `stream`; in capture mode the boundary kernel
+    // runs on the side stream as a parallel branch.
+    void launch_step(int from, bool branch) {
+        const StepBuffers3D b = buffers();
+        if (branch && g.boundary_nodes > 0) {
+            check(cudaEventRecord(fork, stream), "step fork");
+            check(cudaStreamWaitEvent(side, fork, 0), "step fork");
+            check(ops->boundary(g, phys(), f[from], f[1 - from], b, smag, side), "boundary kernel");
+            check(ops->bulk(g, phys(), f[from], f[1 - from], b, smag, block, stream), "bulk kernel");
+            check(cudaEventRecord(join, side), "step join");
+            check(cudaStreamWaitEvent(stream, join, 0), "step join");
+        } else {
+            check(ops->boundary(g, phys(), f[from], f[1 - from], b, smag, stream), "boundary kernel");
+            check(ops->bulk(g, phys(), f[from], f[1 - from], b, smag, block, stream), "bulk kernel");
+        }
+        launches += g.boundary_nodes > 0 ? 2 : 1;
+    }
+
+    void build_graph() {
+        cudaGraph_t captured = nullptr;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+        const uint64_t before = launches;
+        try {
+            for (uint32_t k = 0; k < kGraphSteps; ++k) {
+                launch_step(static_cast<int>(k & 1u), true);
+            }
+        } catch (...) {
+            cudaStreamEndCapture(stream, &captured);
+            if (captured) cudaGraphDestroy(captured);
+            launches = before;
+            throw;
+        }
+        launches = before;
+        check(cudaStreamEndCapture(stream, &captured), "graph capture");
+        const cudaError_t e = cudaGraphInstantiate(&graph, captured, 0);
+        cudaGraphDestroy(captured);
+        check(e, "graph instantiate");
+    }
+
+    void run(uint64_t count) {
+        uint64_t left = count;
+        if (left >= kGraphSteps) {
+            if (cur != 0) {
+                launch_step(cur, false);
+                cur = 1 - cur;
+                --left;
+            }
+            if (!graph) {
+                build_graph();
+            }
+            while (left >= kGraphSteps) {
+                check(cudaGraphLaunch(graph, stream), "graph launch");
+                launches += static_cast<uint64_t>(kGraphSteps) * (g.boundary_nodes > 0 ? 2 : 1);
+                left -= kGraphSteps;
+            }
+        }
+        for (; left > 0; --left) {
+            launch_step(cur, false);
+            cur = 1 - cur;
+        }
+        steps += count;
+    }
+};
+
+namespace {
+
+orr_lbm3d* handle_of(orr_lbm3d* h) {
+    if (h == nullptr) {
+        throw Refusal{ORR_ERR_INVALID, "null solver handle"};
+    }
+    check(cudaSetDevice(h->device), "cudaSetDevice");
+    return h;
+}
+
+template <class P> void fill_phys(P& p, const orr_lbm3d_config& c, bool binary32) {
+    using A = decltype(p.tau);
+    const auto cv = [binary32](double v) -> A {
+        return binary32 ? static_cast<A>(static_cast<float>(v)) : static_cast<A>(v);
+    };
+    const double k = c.smagorinsky_enabled ? c.smagorinsky_constant : 0.0;
+    p.tau = cv(c.tau);
+    p.smag_c = cv(k);
+    p.smag_c2 = cv(k * k);
+    p.fx = cv(c.body_force_x);
+    p.fy = cv(c.body_force_y);
+    p.fz = cv(c.body_force_z);
+    p.wall_ux[0] = cv(c.y_low.velocity_x);
+    p.wall_ux[1] = cv(c.y_high.velocity_x);
+    p.wall_ux[2] = cv(c.z_low.velocity_x);
+    p.wall_ux[3] = cv(c.z_high.velocity_x);
+    p.outlet_speed = cv(c.inlet_ux);
+    p.sponge_strength = cv(c.sponge_strength);
+}
+
+orr_solver_options options_or_default(const orr_solver_options* o) {
+    orr_solver_options d{};
+    d.storage = ORR_STORAGE_F32;
+    d.allow_high_mach = 0;
+    d.device = 0;
+    d.block_x = 0;
+    return o ? *o : d;
+}
+
+void copy_message(const std::string& text, char* message, size_t capacity) {
+    if (message == nullptr || capacity == 0) {
+        return;
+    }
+    const size_t n = std::min(text.size(), capacity - 1);
+    std::memcpy(message, text.data(), n);
+    message[n] = '\0';
+}
+
+void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const double* uy,
+                      const double* uz) {
+    const auto& c = h->plan.c;
+    const std::size_t cells = h->plan.cells;
+    double* staged[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (rho != nullptr) {
+        // Stage the four fields in the other population buffer: 32 bytes per
+        // node fit in 19 storage values of at least 2 bytes.
+        double* base = static_cast<double*>(h->f[1]);
+        const double* src[4] = {rho, ux, uy, uz};
+        for (int k = 0; k < 4; ++k) {
+            staged[k] = base + static_cast<std::size_t>(k) * cells;
+            check(cudaMemcpyAsync(staged[k], src[k], cells * sizeof(double), cudaMemcpyHostToDevice,
+                                  h->stream),
+                  "initial state upload");
+        }
+    }
+    const bool inflow = c.x_boundary == ORR_X_INFLOW_OUTFLOW;
+    check(h->ops->init(h->g, h->cls, staged[0], staged[1], staged[2], staged[3], 1.0,
+                       inflow ? c.inlet_ux : 0.0, inflow ? c.inlet_uy : 0.0,
+                       inflow ? c.inlet_uz : 0.0, h->f[0], h->stream),
+          "init kernel");
+    check(cudaMemcpyAsync(h->f[1], h->f[0], d3::Q * cells * h->sbytes, cudaMemcpyDeviceToDevice,
+                          h->stream),
+          "population copy");
+    check(h->ops->history(h->g, h->f[0], h->hist, h->stream), "history kernel");
+    h->launches += 2;
+    h->cur = 0;
+    h->steps = 0;
+    const double v[3] = {c.inlet_ux, c.inlet_uy, c.inlet_uz};
+    h->upload_inlet(v);
+}
+
+} // namespace
+
+extern "C" {
+
+orr_status orr_lbm3d_validate(const orr_lbm3d_config* config, const uint8_t* solid,
+                              const double* distance, const orr_solver_options* options,
+                              char* message, size_t capacity) {
+    if (config == nullptr) {
+        copy_message("null configuration", message, capacity);
+        return orr::fail(ORR_ERR_INVALID, "null configuration");
+    }
+    const orr_solver_options o = options_or_default(options);
+    const std::string problem =
+        orr::problem3d(*config, solid, distance, o.storage, o.allow_high_mach != 0);
+    copy_message(problem, message, capacity);
+    if (!problem.empty()) {
+        return orr::fail(ORR_ERR_INVALID, problem);
+    }
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_memory_bytes(const orr_lbm3d_config* config, uint64_t links,
+                                  uint64_t boundary_nodes, int32_t storage, uint64_t* bytes) {
+    if (config == nullptr || bytes == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    const auto m = orr::memory3d(*config, links, boundary_nodes,
+                                 config->solid_wall == ORR_SOLID_INTERPOLATED ? boundary_nodes : 0,
+                                 storage);
+    if (!m) {
+        return orr::fail(ORR_ERR_INVALID, "lbm3d gpu: the device memory of the lattice overflows std::size_t");
+    }
+    *bytes = *m;
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_plan(const orr_lbm3d_config* config, const uint8_t* solid,
+                          const double* distance, uint64_t* links, uint64_t* fluid,
+                          uint64_t* boundary_nodes, uint32_t* cell, uint32_t* direction,
+                          double* q) {
+    return orr::guarded(nullptr, [&]() -> orr_status {
+        if (config == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null configuration"};
+        }
+        if (std::string problem = problem3d(*config, solid, distance, ORR_STORAGE_F64, true);
+            !problem.empty()) {
+            throw Refusal{ORR_ERR_INVALID, problem};
+        }
+        const Plan3D p = plan3d(*config, solid, distance);
+        const std::size_t n = p.link_cell.size();
+        if (links) *links = n;
+        if (fluid) *fluid = p.fluid;
+        if (boundary_nodes) *boundary_nodes = p.bnode.size();
+        if (cell) std::memcpy(cell, p.link_cell.data(), n * 4);
+        if (direction) std::memcpy(direction, p.link_dir.data(), n * 4);
+        if (q) std::memcpy(q, p.link_q.data(), n * 8);
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid,
+                            const double* distance, const orr_solver_options* options,
+                            orr_lbm3d** out) {
+    if (out == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null output handle");
+    }
+    *out = nullptr;
+    return orr::guarded(nullptr, [&]() -> orr_status {
+        if (config == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null configuration"};
+        }
+        const orr_solver_options o = options_or_default(options);
+        // validate() and the binary32 checks, before anything is allocated.
+        if (std::string problem =
+                problem3d(*config, solid, distance, o.storage, o.allow_high_mach != 0);
+            !problem.empty()) {
+            throw Refusal{ORR_ERR_INVALID, problem};
+        }
+        if (o.block_x < 0 || o.block_x > 256 || (o.block_x % 32) != 0) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: block_x must be 0 or a multiple of 32 up to 256"};
+        }
+        require_device(o.device);
+        auto h = std::make_unique<orr_lbm3d>();
+        h->device = o.device;
+        h->storage = o.storage;
+        h->allow_high_mach = o.allow_high_mach != 0;
+        h->block = o.block_x > 0 ? static_cast<uint32_t>(o.block_x) : kDefaultBlock;
+        h->ops = &ops_for(o.storage);
+        h->sbytes = storage_bytes(o.storage);
+        h->abytes = arithmetic_bytes(o.storage);
+        h->plan = plan3d(*config, solid, distance);
+        const Plan3D& p = h->plan;
+        // The memory check counts every table the solver allocates
+        // (check_memory, lbm3d_gpu.cpp:129-149).
+        const std::size_t slots = p.wall_q.size() / d3::Q;
+        const auto need = memory3d(*config, p.link_cell.size(), p.bnode.size(), slots, o.storage);
+        if (!need) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the device memory of the lattice overflows std::size_t"};
+        }
+        std::size_t free_bytes = 0, total_bytes = 0;
+        check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
+        if (*need > free_bytes) {
+            throw Refusal{ORR_ERR_MEMORY, "lbm3d gpu: the lattice needs " + mebibytes(*need) +
+                                              " of device memory, " + mebibytes(free_bytes) +
+                                              " are available; use fewer cells"};
+        }
+        // Geometry and parameters.
+        Geom3D& g = h->g;
+        g.nx = static_cast<uint32_t>(config->nx);
+        g.ny = static_cast<uint32_t>(config->ny);
+        g.nz = static_cast<uint32_t>(config->nz);
+        g.plane = g.nx * g.ny;
+        g.cells = p.cells;
+        g.boundary_nodes = static_cast<uint32_t>(p.bnode.size());
+        g.x_mode = config->x_boundary;
+        g.outlet_mode = config->outlet;
+        g.y_lo = config->y_low.kind;
+        g.y_hi = config->y_high.kind;
+        g.z_lo = config->z_low.kind;
+        g.z_hi = config->z_high.kind;
+        g.forced = config->body_force_x != 0.0 || config->body_force_y != 0.0 ||
+                   config->body_force_z != 0.0;
+        g.sponge = config->sponge_strength > 0.0 && config->x_boundary == ORR_X_INFLOW_OUTFLOW;
+        g.sponge_inlet = static_cast<uint32_t>(config->sponge_inlet);
+        g.sponge_outlet = static_cast<uint32_t>(config->sponge_outlet);
+        g.sponge_sides = static_cast<uint32_t>(config->sponge_sides);
+        const bool binary32 = o.storage != ORR_STORAGE_F64;
+        if (binary32) {
+            g.forced = to_f32(config->body_force_x) != 0.0f || to_f32(config->body_force_y) != 0.0f ||
+                       to_f32(config->body_force_z) != 0.0f;
+        }
+        fill_phys(h->phys32, *config, true);
+        fill_phys(h->phys64, *config, false);
+        h->smag = config->smagorinsky_enabled != 0 &&
+                  (binary32 ? h->phys32.smag_c2 > 0.0f : true);
+        // Streams and device tables.
+        check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "event");
+        check(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "event");
+        const std::size_t cells = p.cells;
+        for (int k = 0; k < 2; ++k) {
+            check(cudaMalloc(&h->f[k], d3::Q * cells * h->sbytes), "population buffer");
+        }
+        h->cls = device_alloc<uint8_t>(cells, "node class buffer");
+        h->bnode = device_alloc<uint32_t>(p.bnode.size(), "boundary list");
+        h->bslot = device_alloc<int32_t>(p.bnode.size(), "boundary list");
+        check(cudaMalloc(&h->wall_q, std::max<std::size_t>(slots, 1) * d3::Q * h->abytes), "wall buffer");
+        check(cudaMalloc(&h->hist, static_cast<std::size_t>(d3::kOutletSlots) * config->ny * config->nz * h->abytes),
+              "outlet buffer");
+        check(cudaMalloc(&h->moments, 4 * cells * h->abytes), "moment buffer");
+        h->lcell = device_alloc<uint32_t>(p.link_cell.size(), "link buffer");
+        h->ldir = device_alloc<uint32_t>(p.link_cell.size(), "link buffer");
+        h->lq = device_alloc<double>(p.link_cell.size(), "link buffer");
+        check(cudaMalloc(&h->small, 256), "small buffer");
+        check(cudaMallocHost(reinterpret_cast<void**>(&h->host_small), 256), "pinned buffer");
+        // Uploads.
+        cudaStream_t s = h->stream;
+        check(cudaMemcpyAsync(h->cls, p.cls.data(), cells, cudaMemcpyHostToDevice, s), "class upload");
+        if (!p.bnode.empty()) {
+            check(cudaMemcpyAsync(h->bnode, p.bnode.data(), p.bnode.size() * 4, cudaMemcpyHostToDevice, s),
+                  "boundary upload");
+            check(cudaMemcpyAsync(h->bslot, p.bslot.data(), p.bslot.size() * 4, cudaMemcpyHostToDevice, s),
+                  "boundary upload");
+        }
+        {
+            std::vector<double> q = p.wall_q;
+            if (q.empty()) {
+                q.assign(d3::Q, 0.5);
+            }
+            if (binary32) {
+                std::vector<float> qf(q.begin(), q.end());
+                check(cudaMemcpyAsync(h->wall_q, qf.data(), qf.size() * 4, cudaMemcpyHostToDevice, s),
+                      "wall upload");
+                check(cudaStreamSynchronize(s), "wall upload");
+            } else {
+                check(cudaMemcpyAsync(h->wall_q, q.data(), q.size() * 8, cudaMemcpyHostToDevice, s),
+                      "wall upload");
+                check(cudaStreamSynchronize(s), "wall upload");
+            }
+        }
+        if (!p.link_cell.empty()) {
+            const std::size_t n = p.link_cell.size();
+            check(cudaMemcpyAsync(h->lcell, p.link_cell.data(), n * 4, cudaMemcpyHostToDevice, s), "link upload");
+            check(cudaMemcpyAsync(h->ldir, p.link_dir.data(), n * 4, cudaMemcpyHostToDevice, s), "link upload");
+            check(cudaMemcpyAsync(h->lq, p.link_q.data(), n * 8, cudaMemcpyHostToDevice, s), "link upload");
+        }
+        initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
+        check(cudaStreamSynchronize(s), "create");
+        // The plan's class array is on the device now; keep the links.
+        h->plan.cls.clear();
+        h->plan.cls.shrink_to_fit();
+        h->plan.bnode.shrink_to_fit();
+        *out = h.release();
+        return ORR_OK;
+    });
+}
+
+void orr_lbm3d_destroy(orr_lbm3d* solver) {
+    delete solver;
+}
+
+const char* orr_lbm3d_last_error(const orr_lbm3d* solver) {
+    return solver ? solver->error.c_str() : orr_last_error();
+}
+
+orr_status orr_lbm3d_initialize(orr_lbm3d* solver, const double* rho, const double* ux,
+                                const double* uy, const double* uz) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        const bool any = rho || ux || uy || uz;
+        const bool all = rho && ux && uy && uz;
+        if (any && !all) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d: initialize needs all four fields or none"};
+        }
+        initialize_state(h, rho, ux, uy, uz);
+        check(cudaStreamSynchronize(h->stream), "initialize");
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_step(orr_lbm3d* solver, uint64_t count) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        h->run(count);
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_steps(const orr_lbm3d* solver, uint64_t* steps) {
+    if (solver == nullptr || steps == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    *steps = solver->steps;
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_set_inlet_velocity(orr_lbm3d* solver, const double velocity[3]) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        if (velocity == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null velocity"};
+        }
+        if (std::string problem = inlet_problem3d(h->plan.c, velocity, h->allow_high_mach);
+            !problem.empty()) {
+            throw Refusal{ORR_ERR_INVALID, problem};
+        }
+        h->upload_inlet(velocity);
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_inlet_velocity(const orr_lbm3d* solver, double velocity[3]) {
+    if (solver == nullptr || velocity == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    std::memcpy(velocity, solver->inlet, 3 * sizeof(double));
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        if (force_moment == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null output"};
+        }
+        const std::size_t links = h->plan.link_cell.size();
+        check(h->ops->force(h->g, h->f[h->cur], h->lcell, h->ldir, h->lq, links, h->acc(), h->stream),
+              "force kernel");
+        if (links > 0) {
+            ++h->launches;
+        }
+        check(cudaMemcpyAsync(h->host_small + 8, h->acc(), 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream),
+              "force read-back");
+        check(cudaStreamSynchronize(h->stream), "force read-back");
+        std::memcpy(force_moment, h->host_small + 8, 6 * sizeof(double));
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, double* uy,
+                                 double* uz) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        const std::size_t cells = h->plan.cells;
+        check(h->ops->moments(h->g, h->phys(), h->cls, h->f[h->cur], h->moments, h->stream),
+              "moments kernel");
+        ++h->launches;
+        double* outs[4] = {rho, ux, uy, uz};
+        const bool shifted = h->storage != ORR_STORAGE_F64;
+        std::vector<float> tmp(shifted ? cells : 0);
+        for (int k = 0; k < 4; ++k) {
+            if (outs[k] == nullptr) {
+                continue;
+            }
+            const char* plane = static_cast<const char*>(h->moments) + k * cells * h->abytes;
+            if (shifted) {
+                check(cudaMemcpyAsync(tmp.data(), plane, cells * 4, cudaMemcpyDeviceToHost, h->stream),
+                      "moment read-back");
+                check(cudaStreamSynchronize(h->stream), "moment read-back");
+                for (std::size_t c = 0; c < cells; ++c) {
+                    outs[k][c] = static_cast<double>(tmp[c]) + (k == 0 ? 1.0 : 0.0);
+                }
+            } else {
+                check(cudaMemcpyAsync(outs[k], plane, cells * 8, cudaMemcpyDeviceToHost, h->stream),
+                      "moment read-back");
+                check(cudaStreamSynchronize(h->stream), "moment read-back");
+            }
+        }
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        if (f == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null output"};
+        }
+        const std::size_t cells = h->plan.cells;
+        const std::size_t n = d3::Q * cells;
+        if (h->storage == ORR_STORAGE_F64) {
+            check(cudaMemcpyAsync(f, h->f[h->cur], n * 8, cudaMemcpyDeviceToHost, h->stream),
+                  "population read-back");
+            check(cudaStreamSynchronize(h->stream), "population read-back");
+            return ORR_OK;
+        }
+        std::vector<unsigned char> raw(n * h->sbytes);
+        check(cudaMemcpyAsync(raw.data(), h->f[h->cur], raw.size(), cudaMemcpyDeviceToHost, h->stream),
+              "population read-back");
+        check(cudaStreamSynchronize(h->stream), "population read-back");
+        for (int i = 0; i < d3::Q; ++i) {
+            const double w = d3::w(i);
+            for (std::size_t c = 0; c < cells; ++c) {
+                const std::size_t k = static_cast<std::size_t>(i) * cells + c;
+                double v;
+                if (h->storage == ORR_STORAGE_F32) {
+                    float x;
+                    std::memcpy(&x, raw.data() + 4 * k, 4);
+                    v = x;
+                } else if (h->storage == ORR_STORAGE_F16) {
+                    __half x;
+                    std::memcpy(&x, raw.data() + 2 * k, 2);
+                    v = static_cast<double>(__half2float(x)) / 32768.0;
+                } else {
+                    __nv_bfloat16 x;
+                    std::memcpy(&x, raw.data() + 2 * k, 2);
+                    v = static_cast<double>(__bfloat162float(x));
+                }
+                f[k] = v + w;
+            }
+        }
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_mass(orr_lbm3d* solver, double* mass) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        if (mass == nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "null output"};
+        }
+        check(h->ops->mass(h->g, h->cls, h->f[h->cur], h->acc() + 6, h->stream), "mass kernel");
+        ++h->launches;
+        check(cudaMemcpyAsync(h->host_small + 16, h->acc() + 6, sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream),
+              "mass read-back");
+        check(cudaStreamSynchronize(h->stream), "mass read-back");
+        double m = h->host_small[16];
+        if (h->storage != ORR_STORAGE_F64) {
+            m += static_cast<double>(h->plan.fluid); // the weights of each fluid node add up to 1
+        }
+        *mass = m;
+        return ORR_OK;
+    });
+}
+
+orr_status orr_lbm3d_link_count(const orr_lbm3d* solver, uint64_t* count) {
+    if (solver == nullptr || count == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    *count = solver->plan.link_cell.size();
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_links(const orr_lbm3d* solver, uint32_t* cell, uint32_t* direction,
+                           double* q) {
+    if (solver == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    const Plan3D& p = solver->plan;
+    const std::size_t n = p.link_cell.size();
+    if (cell) std::memcpy(cell, p.link_cell.data(), n * 4);
+    if (direction) std::memcpy(direction, p.link_dir.data(), n * 4);
+    if (q) std::memcpy(q, p.link_q.data(), n * 8);
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* fluid, uint64_t* boundary) {
+    if (solver == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    if (fluid) *fluid = solver->plan.fluid;
+    if (boundary) *boundary = solver->g.boundary_nodes;
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream) {
+    if (solver == nullptr || stream == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    *stream = solver->stream;
+    return ORR_OK;
+}
+
+orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches) {
+    if (solver == nullptr || launches == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    *launches = solver->launches;
+    return ORR_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,80 @@
+// Population storage forms of the device solvers.
+//
+//   float          f - w in binary32, binary32 arithmetic (the plain form)
+//   __half         (f - w) * 2^15 in binary16 ("FP16S", Lehmann et al. 2022:
+//                  the scale puts the small shifted values in binary16's
+//                  normal range), binary32 arithmetic
+//   __nv_bfloat16  f - w in bfloat16, binary32 arithmetic
+//   double         f unshifted in binary64, binary64 arithmetic following the
+//                  reference CPU solver's operation order (the FP64 device
+//                  oracle)
+//
+// Storing f - w keeps the O(1e-2) deviations that carry the flow out of the
+// rounding error of the O(1) weights (src/aero/lbm3d/lbm3d_gpu.cpp:1-7).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+namespace orr {
+
+template <class S> struct Storage;
+
+template <> struct Storage<float> {
+    using A = float;
+    static constexpr bool kShifted = true;
+    __device__ __forceinline__ static A load(const float* p) { return __ldg(p); }
+    __device__ __forceinline__ static void store(float* p, A v) { *p = v; }
+    __host__ __device__ static float encode(double shifted) { return static_cast<float>(shifted); }
+    __host__ __device__ static double decode(float s) { return static_cast<double>(s); }
+};
+
+constexpr float kF16Scale = 32768.0f;
+constexpr float kF16InvScale = 1.0f / 32768.0f;
+
+template <> struct Storage<__half> {
+    using A = float;
+    static constexpr bool kShifted = true;
+    __device__ __forceinline__ static A load(const __half* p) {
+        return __half2float(__ldg(p)) * kF16InvScale;
+    }
+    __device__ __forceinline__ static void store(__half* p, A v) {
+        *p = __float2half_rn(v * kF16Scale);
+    }
+    __device__ static __half encode(double shifted) {
+        return __float2half_rn(static_cast<float>(shifted) * kF16Scale);
+    }
+    __device__ static double decode(__half s) {
+        return static_cast<double>(__half2float(s) * kF16InvScale);
+    }
+};
+
+template <> struct Storage<__nv_bfloat16> {
+    using A = float;
+    static constexpr bool kShifted = true;
+    __device__ __forceinline__ static A load(const __nv_bfloat16* p) {
+        return __bfloat162float(__ldg(p));
+    }
+    __device__ __forceinline__ static void store(__nv_bfloat16* p, A v) {
+        *p = __float2bfloat16_rn(v);
+    }
+    __device__ static __nv_bfloat16 encode(double shifted) {
+        return __float2bfloat16_rn(static_cast<float>(shifted));
+    }
+    __device__ static double decode(__nv_bfloat16 s) {
+        return static_cast<double>(__bfloat162float(s));
+    }
+};
+
+template <> struct Storage<double> {
+    using A = double;
+    static constexpr bool kShifted = false;
+    __device__ __forceinline__ static A load(const double* p) { return __ldg(p); }
+    __device__ __forceinline__ static void store(double* p, A v) { *p = v; }
+    __host__ __device__ static double encode(double unshifted) { return unshifted; }
+    __host__ __device__ static double decode(double s) { return s; }
+};
+
+} // namespace orr

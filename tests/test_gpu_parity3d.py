@@ -1,0 +1,194 @@
+"""D3Q19 CUDA path against the CPU oracle on identical inputs.
+
+The cases follow the reference's GPU-vs-CPU tests
+(tests/aero/lbm3d/test_lbm3d_gpu.cpp:197-289): the same sphere channel
+(64 x 32 x 32, D 8, Re 20, 800 steps) with BGK, LES, the interpolated wall and
+the extrapolation outlet with periodic y, the analytic flows, the Smagorinsky
+closure probe and co-moving walls.  Tolerances: the reference's 1e-4 on
+velocity, populations and force x, and 1e-5 on populations for the binary32
+form; the binary64 form must equal the oracle bit for bit.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import (copy_config, couette3d_config, duct_config, l2_relative, poiseuille3d_config,
+                     sphere_channel, uniform_state_error, velocity_l2)
+from oracle import oracle as O
+from orrery_b200 import masks as M
+from orrery_b200 import solver as S
+from orrery_b200.lbm3d import Outlet, Smagorinsky, SolidWall, Sponge, WallKind, periodic_box, wall
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(config, mask, steps, storage="f32", init=None, inlet=None):
+    g = S.make_gpu_solver(config, mask, storage=storage)
+    o = O.Restated3D(config, mask.solid, mask.distance)
+    if init is not None:
+        g.initialize(*init)
+        o.initialize(*init)
+    if inlet is not None:
+        g.set_inlet_velocity(inlet)
+        o.set_inlet_velocity(inlet)
+    g.step(steps)
+    o.step(steps)
+    return g, o
+
+
+def errors(g, o, mask):
+    mg = g.macroscopic()
+    ro, uxo, uyo, uzo = o.macroscopic()
+    vel = velocity_l2([mg.velocity_x, mg.velocity_y, mg.velocity_z], [uxo, uyo, uzo], mask.solid)
+    pops = l2_relative(g.populations(), o.populations())
+    fg = g.force().force[0]
+    fo = o.force()[0]
+    fx = abs(fg - fo) / abs(fo) if fo != 0.0 else abs(fg)
+    return vel, pops, fx
+
+
+SPHERE = sphere_channel(64, 32, 32, 8.0, 2.5, 0.05, 20.0)
+
+
+def variant(name):
+    cfg, mask = copy_config(SPHERE[0]), SPHERE[1]
+    if name == "les":
+        cfg.smagorinsky = Smagorinsky(True, 0.1)
+    elif name == "interpolated":
+        cfg.solid_wall = SolidWall.interpolated
+    elif name == "extrapolation_periodic_y":
+        cfg.outlet = Outlet.extrapolation
+        cfg.y_low = wall(WallKind.periodic)
+        cfg.y_high = wall(WallKind.periodic)
+    elif name == "sponge":
+        cfg.sponge = Sponge(0.5, 6, 8, 4)
+    return cfg, mask
+
+
+@pytest.mark.parametrize("name", ["bgk", "les", "interpolated", "extrapolation_periodic_y", "sponge"])
+def test_sphere_channel_binary32(name):
+    cfg, mask = variant(name)
+    g, o = run_both(cfg, mask, 800)
+    vel, pops, fx = errors(g, o, mask.solid if False else mask)
+    print(f"measured: f32 vs CPU sphere Re 20 {name}: velocity L2 {vel:.3e}, populations L2 {pops:.3e}, "
+          f"force x rel {fx:.3e}")
+    assert vel < 1e-4
+    assert pops < 1e-5
+    assert fx < 1e-4
+
+
+@pytest.mark.parametrize("name", ["bgk", "les", "interpolated", "extrapolation_periodic_y", "sponge"])
+def test_sphere_channel_binary64_is_bitwise(name):
+    cfg, mask = variant(name)
+    g, o = run_both(cfg, mask, 300, storage="f64")
+    fg, fo = g.populations(), o.populations()
+    assert np.array_equal(fg, fo), f"max diff {np.max(np.abs(fg - fo))}"
+    mg = g.macroscopic()
+    mo = o.macroscopic()
+    assert np.array_equal(mg.density, mo[0])
+    assert np.array_equal(mg.velocity_x, mo[1])
+    f = g.force()
+    ref = o.force()
+    assert np.allclose(f.force, ref[:3], rtol=1e-12, atol=1e-15)
+    assert np.allclose(f.moment, ref[3:], rtol=1e-12, atol=1e-12)
+    assert g.mass() == pytest.approx(o.mass(), rel=1e-14)
+
+
+def test_inlet_velocity_and_walls_binary64_bitwise():
+    """Moving walls, body force, slip and periodic sides and a skewed inlet in one lattice."""
+    cfg, mask = copy_config(SPHERE[0]), SPHERE[1]
+    cfg.z_low = wall(WallKind.no_slip, 0.01)
+    cfg.z_high = wall(WallKind.no_slip, -0.02)
+    cfg.body_force_x = 1e-6
+    cfg.body_force_y = -2e-7
+    cfg.smagorinsky = Smagorinsky(True, 0.15)
+    cfg.outlet = Outlet.convective
+    g, o = run_both(cfg, mask, 200, storage="f64", inlet=(0.04, 0.004, -0.003))
+    assert np.array_equal(g.populations(), o.populations())
+
+
+def test_graph_replay_equals_single_steps():
+    cfg, mask = variant("les")
+    a = S.make_gpu_solver(cfg, mask)
+    b = S.make_gpu_solver(cfg, mask)
+    a.step(40)             # graph replays plus single steps
+    for _ in range(40):
+        b.step(1)          # single launches only
+    assert a.steps() == b.steps() == 40
+    assert np.array_equal(a.populations(), b.populations())
+
+
+def test_deterministic_split():
+    """Bitwise across a 150 vs 100 + 50 step split (test_lbm3d_flows.cpp:232-240)."""
+    cfg, mask = sphere_channel(32, 16, 16, 6.0, 2.0, 0.05, 50.0)
+    a = S.make_gpu_solver(cfg, mask)
+    b = S.make_gpu_solver(cfg, mask)
+    a.step(150)
+    b.step(100)
+    b.step(50)
+    assert np.array_equal(a.populations(), b.populations())
+
+
+def profile_error(fields, exact):
+    keep = fields.solid == 0
+    return math.sqrt(np.sum((fields.velocity_x[keep] - exact[keep]) ** 2) / np.sum(exact[keep] ** 2))
+
+
+def test_analytic_flows_against_cpu():
+    """test_lbm3d_gpu.cpp:197-209: Poiseuille, duct and Couette, velocity L2 below 1e-4."""
+    cases = [(poiseuille3d_config(4, 32, 4, 0.8, 1e-6), "Poiseuille"),
+             (duct_config(4, 20, 20, 0.8, 1e-6), "duct"),
+             (couette3d_config(4, 4, 16, 0.8, 0.02), "Couette")]
+    for cfg, label in cases:
+        mask = M.fluid_mask_3d(cfg.nx, cfg.ny, cfg.nz)
+        g, o = run_both(cfg, mask, 4000)
+        vel, _, _ = errors(g, o, mask)
+        print(f"measured: f32 vs CPU {label}: velocity L2 {vel:.3e}")
+        assert vel < 1e-4
+
+
+def test_co_moving_walls_stay_uniform():
+    """test_lbm3d_gpu.cpp:270-289: uniform stream between co-moving walls at any density."""
+    for rho in (0.7, 2.0):
+        cfg = periodic_box(4, 8, 8, 0.7)
+        u = 0.03
+        for side in ("y_low", "y_high", "z_low", "z_high"):
+            setattr(cfg, side, wall(WallKind.no_slip, u))
+        mask = M.fluid_mask_3d(4, 8, 8)
+        g = S.make_gpu_solver(cfg, mask)
+        n = cfg.cells
+        g.initialize(np.full(n, rho), np.full(n, u), np.zeros(n), np.zeros(n))
+        g.step(300)
+        m = g.macroscopic()
+        worst = uniform_state_error(m.density, m.velocity_x, m.velocity_y, m.velocity_z, rho, (u, 0, 0), u)
+        print(f"measured: f32 co-moving walls at density {rho}: {worst:.3e}")
+        assert worst < 1e-4
+
+
+def test_mass_conservation_periodic():
+    cfg = periodic_box(12, 10, 9, 0.62)
+    cfg.y_low = wall(WallKind.slip)
+    cfg.y_high = wall(WallKind.slip)
+    cfg.z_low = wall(WallKind.no_slip, 0.02)
+    cfg.z_high = wall(WallKind.no_slip, -0.01)
+    cfg.smagorinsky = Smagorinsky(True, 0.15)
+    mask = M.sphere_mask(12, 10, 9, (6.0, 4.6, 4.2), 2.4)
+    g = S.make_gpu_solver(cfg, mask, storage="f64")
+    x = np.tile(np.arange(12.0), 10 * 9)
+    y = np.tile(np.repeat(np.arange(10.0), 12), 9)
+    z = np.repeat(np.arange(9.0), 120)
+    a = 2 * math.pi * x / 12.0
+    g.initialize(1 + 0.01 * np.sin(a), 0.03 * np.cos(a), 0.01 * np.sin(0.7 * y), 0.01 * np.cos(0.5 * z))
+    before = g.mass()
+    g.step(1500)
+    after = g.mass()
+    assert abs(after - before) / before < 1e-12
+
+
+def test_links_match_the_oracle():
+    cfg, mask = variant("interpolated")
+    g = S.make_gpu_solver(cfg, mask)
+    o = O.Restated3D(cfg, mask.solid, mask.distance)
+    for a, b in zip(g.links(), o.links()):
+        assert np.array_equal(a, b)
