@@ -95,7 +95,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -236,7 +236,7 @@ def main(argv=None) -> int:
     # mask, initialise from host fields, step with the force read back every
     # 10 steps (the reference adapter's sampling), read the moments back.
     e2e = None
-    if rank == 0 or world > 1:
+    if args.e2e_steps >= 10:
         import numpy as np
         barrier()
         t0 = time.perf_counter()

@@ -6,17 +6,8 @@
 //   GPU   lbm_d3q19_step                  (src/render/shaders/lbm/lbm_d3q19_step.comp.glsl,
 //                                          lbm_d3q19_common.glsl:87-368)
 // with the boundary rules of resolve_source (src/aero/lbm3d/lbm3d_internal.h:57-130).
-// A step is two kernels over disjoint node sets, writing disjoint entries:
-//   boundary3d   one thread per entry of the compact list of boundary fluid
-//                nodes: the general gather (sides, inlet, outlet, walls,
-//                bounce-back);
-//   bulk3d       one thread per node of the interior rows y in [1, ny-2],
-//                z in [1, nz-2]; bulk nodes take 19 plain pulls, every other
-//                node returns at once.
-// So bulk warps never diverge into the boundary path and keep a small
-// register budget; the solver runs the two as parallel branches of the
-// step's CUDA graph, so the boundary list (a few percent of the nodes)
-// overlaps the bulk.
+// A step is one launch of step3d_kernel over all rows; lanes branch by node
+// class (see there).
 //
 // Shifted storage forms collide in binary32 on f - w (the GLSL formulation);
 // the binary64 form stores f itself and evaluates every expression in the
@@ -37,8 +28,7 @@ struct Geom3D {
     uint32_t nx, ny, nz;
     uint32_t plane;           // nx * ny
     uint64_t cells;           // nx * ny * nz
-    uint32_t tiles_x;         // bulk blocks per interior row
-    uint32_t boundary_nodes;  // entries of the boundary list
+    uint32_t tiles_x;         // blocks per row (set by the launcher)
     int32_t x_mode;           // ORR_X_PERIODIC / ORR_X_INFLOW_OUTFLOW
     int32_t outlet_mode;      // ORR_OUTLET_*
     int32_t y_lo, y_hi, z_lo, z_hi; // ORR_WALL_*
@@ -95,6 +85,16 @@ __device__ __forceinline__ double w_rt(int j) {
     return j == 0 ? 1.0 / 3.0 : (j <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
 }
 
+// Reciprocal of the binary32 collision (rho and tau near 1: the hardware
+// approximation, 2 ulp, is far inside the form's tolerance); exact division
+// in binary64.
+__device__ __forceinline__ float fast_rcp(float x) {
+    return __fdividef(1.0f, x);
+}
+__device__ __forceinline__ double fast_rcp(double x) {
+    return 1.0 / x;
+}
+
 // ---------------------------------------------------------------- collide --
 
 // BGK collision with Guo forcing and the optional Smagorinsky closure.
@@ -111,7 +111,7 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
         const A jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
         const A jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
         const A rho = A(1) + drho;
-        const A inv = A(1) / rho;
+        const A inv = fast_rcp(rho);
         const A ux = (jx + A(0.5) * p.fx) * inv;
         const A uy = (jy + A(0.5) * p.fy) * inv;
         const A uz = (jz + A(0.5) * p.fz) * inv;
@@ -140,12 +140,22 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
                 sqrt(pxx * pxx + pyy * pyy + pzz * pzz + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
             tau = A(0.5) * (tau + sqrt(tau * tau + A(kSmagFactor) * p.smag_c2 * strain * inv));
         }
-        const A omega = A(1) / tau;
+        const A omega = fast_rcp(tau);
+        // Relaxation towards f_eq,i - w_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2
+        // - 1.5 u.u)), by opposite pairs (c_{i+1} = -c_i for odd i): the even
+        // part w (drho - 1.5 rho u.u + 4.5 rho (c.u)^2) is shared and the odd
+        // part 3 w rho c.u changes sign.
+        const A base = drho - A(1.5) * rho * uu;
+        const A rho45 = A(4.5) * rho;
+        f[0] += omega * (A(d3::w(0)) * base - f[0]);
 #pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
+        for (int i = 1; i < d3::Q; i += 2) {
+            const A w = A(d3::w(i));
             const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
-            const A feq = A(d3::w(i)) * (drho + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu));
-            f[i] = f[i] - omega * (f[i] - feq);
+            const A even = w * (base + rho45 * cu * cu);
+            const A odd = (A(3) * w * rho) * cu;
+            f[i] += omega * (even + odd - f[i]);
+            f[i + 1] += omega * (even - odd - f[i + 1]);
         }
         if (forced) {
             const A scale = A(1) - A(0.5) * omega;
@@ -295,6 +305,32 @@ __device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
         }
     }
     const A uu = ux * ux + uy * uy + uz * uz;
+    if constexpr (kShifted) {
+        // Pi_neq from the second moments of the reconstructed set (sum c c f_eq
+        // = rho (c_s^2 I + u u); shifted: drho c_s^2 I + rho u u), then
+        // f = f_eq + 4.5 w (c c - c_s^2 I) : Pi_neq with f_eq formed on the fly.
+        const A iso = drho * A(1.0 / 3.0);
+        const A pxx = f[1] + f[2] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] + f[14] -
+                      iso - rho * ux * ux;
+        const A pyy = f[3] + f[4] + f[7] + f[8] + f[9] + f[10] + f[15] + f[16] + f[17] + f[18] -
+                      iso - rho * uy * uy;
+        const A pzz = f[5] + f[6] + f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18] -
+                      iso - rho * uz * uz;
+        const A pxy = f[7] + f[8] - f[9] - f[10] - rho * ux * uy;
+        const A pxz = f[11] + f[12] - f[13] - f[14] - rho * ux * uz;
+        const A pyz = f[15] + f[16] - f[17] - f[18] - rho * uy * uz;
+        const A cs2 = A(1.0 / 3.0);
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
+            const A cu = ex * ux + ey * uy + ez * uz;
+            const A feq = A(d3::w(i)) * (drho + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu));
+            f[i] = feq + A(4.5) * A(d3::w(i)) *
+                             ((ex * ex - cs2) * pxx + (ey * ey - cs2) * pyy + (ez * ez - cs2) * pzz +
+                              A(2) * (ex * ey * pxy + ex * ez * pxz + ey * ez * pyz));
+        }
+        return;
+    }
     A feq[d3::Q];
     A pi0 = 0, pi1 = 0, pi2 = 0, pi3 = 0, pi4 = 0, pi5 = 0;
 #pragma unroll
@@ -328,8 +364,8 @@ __device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
 
 struct StepBuffers3D {
     const uint8_t* cls;      // node classes
-    const uint32_t* bnode;   // boundary-node list (cells)
-    const int32_t* bslot;    // wall slot per boundary node, -1 none
+    const uint32_t* nmask;   // per node, bit i: direction i bounces back (solid source)
+    const int32_t* nslot;    // per node wall slot of the interpolated wall, -1 none (or null)
     const void* wall_q;      // 19 fractions per slot (arithmetic type)
     void* hist;              // convective-outlet history (arithmetic type)
     const void* inlet;       // imposed inlet velocity, 3 values (arithmetic type)
@@ -357,12 +393,16 @@ __device__ __forceinline__ typename Storage<S>::A reflected3(const S* __restrict
            (A(2) * q);
 }
 
-// General gather of direction I at boundary node (x, y, z) (resolve_source,
+// General gather of direction I at node (x, y, z) (resolve_source,
 // lbm3d_internal.h:87-130, and the CPU's per-kind handling, lbm3d_cpu.cpp:281-312).
-template <class S, int I>
+// Whether the source is solid comes from the plan's per-node mask (bit i),
+// so no load waits on another; kSolid = false drops the test for nodes the
+// plan knows have no solid source.
+template <class S, int I, bool kSolid>
 __device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
                                             const S* __restrict__ src, const StepBuffers3D& b,
-                                            int32_t slot, int x, int y, int z, uint64_t here,
+                                            int32_t slot, uint32_t mask, int x, int y, int z,
+                                            uint64_t here,
                                             typename Storage<S>::A& wall_rho,
                                             typename Storage<S>::A& out) {
     using A = typename Storage<S>::A;
@@ -440,7 +480,7 @@ __device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typena
     const uint64_t source = static_cast<uint64_t>(sx) +
                             static_cast<uint64_t>(g.nx) * (static_cast<uint64_t>(sy) +
                                                            static_cast<uint64_t>(g.ny) * sz);
-    if (b.cls[source] == kSolid) {
+    if (kSolid && ((mask >> I) & 1u) != 0u) {
         const A q = slot >= 0 ? static_cast<const A*>(b.wall_q)[static_cast<uint64_t>(slot) * d3::Q + I]
                               : A(0.5);
         const int64_t farther_off = static_cast<int64_t>(CX) + static_cast<int64_t>(g.nx) * CY +
@@ -451,15 +491,15 @@ __device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typena
     out = T::load(src + static_cast<uint64_t>(dir) * cells + source);
 }
 
-template <class S, int I>
+template <class S, int I, bool kSolid>
 __device__ __forceinline__ void gather_all3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
                                             const S* __restrict__ src, const StepBuffers3D& b,
-                                            int32_t slot, int x, int y, int z, uint64_t here,
-                                            typename Storage<S>::A& wall_rho,
+                                            int32_t slot, uint32_t mask, int x, int y, int z,
+                                            uint64_t here, typename Storage<S>::A& wall_rho,
                                             typename Storage<S>::A (&f)[d3::Q]) {
     if constexpr (I < d3::Q) {
-        gather_one3<S, I>(g, p, src, b, slot, x, y, z, here, wall_rho, f[I]);
-        gather_all3<S, I + 1>(g, p, src, b, slot, x, y, z, here, wall_rho, f);
+        gather_one3<S, I, kSolid>(g, p, src, b, slot, mask, x, y, z, here, wall_rho, f[I]);
+        gather_all3<S, I + 1, kSolid>(g, p, src, b, slot, mask, x, y, z, here, wall_rho, f);
     }
 }
 
@@ -485,63 +525,88 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
     }
 }
 
-// Bulk nodes: one thread per node of the interior rows y in [1, ny-2],
-// z in [1, nz-2]; block (tile, row) covers x in [tile * blockDim.x, ...).
-// Every source node is inside the lattice and fluid, so the gather is 19
-// plain pulls f_i(x) = f*_i(x - c_i) (lbm3d_cpu.cpp:272-276).
+// One fused step src -> dst: one thread per node, one block per tile of a
+// row (blockDim.x nodes along x), every row of the lattice.  Every lane of a
+// row stores all 19 populations of its node in the same step, so each
+// 32-byte sector of the destination is written whole while it sits in L2:
+// a sector written in parts at different times costs the DRAM a
+// read-modify-write (ECC), about a fifth of the bandwidth.  Per lane:
+//   solid       stores its rest populations, which the reference never changes
+//               (initial_populations puts solids at rest; the step skips them);
+//   bulk        interior rows (y in [1, ny-2], z in [1, nz-2]) with no solid
+//               source: 19 plain pulls f_i(x) = f*_i(x - c_i)
+//               (lbm3d_cpu.cpp:272-276); the x-edge lanes shift their x
+//               sources (periodic wrap, outlet copy) and then take the
+//               convective-outlet blend or the inlet reconstruction;
+//   face        a node of a y or z face row without a solid source: the general
+//               gather, whose side rules are uniform along the row;
+//   boundary    a node with a solid source (bounce-back / interpolated wall):
+//               the general gather with the plan's per-node direction mask.
+template <class S> constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 4;
+
 template <class S, bool kSmag>
-__global__ void __launch_bounds__(256) bulk3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
-                                                     const S* __restrict__ src, S* __restrict__ dst,
-                                                     StepBuffers3D b) {
+__global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
+                                                        const S* __restrict__ src,
+                                                        S* __restrict__ dst, StepBuffers3D b) {
     using A = typename Storage<S>::A;
     using T = Storage<S>;
+    const uint64_t cells = g.cells;
     const uint32_t row = blockIdx.x / g.tiles_x;
     const uint32_t x = (blockIdx.x - row * g.tiles_x) * blockDim.x + threadIdx.x;
-    const uint32_t inner = g.ny - 2u;
-    const uint32_t y = 1u + row % inner;
-    const uint32_t z = 1u + row / inner;
-    if (x == 0 || x >= g.nx - 1u) {
+    const uint32_t y = row % g.ny;
+    const uint32_t z = row / g.ny;
+    if (x >= g.nx) {
         return;
     }
     const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
-    if (b.cls[here] != kBulk) {
-        return;
-    }
-    const uint64_t cells = g.cells;
-    const int64_t nx = g.nx, plane = g.plane;
-    A f[d3::Q];
+    const uint8_t cls = b.cls[here];
+    if (cls == kSolid) {
 #pragma unroll
-    for (int i = 0; i < d3::Q; ++i) {
-        const int64_t off = d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i);
-        f[i] = T::load(src + static_cast<uint64_t>(i) * cells +
-                       static_cast<uint64_t>(static_cast<int64_t>(here) - off));
-    }
-    finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
-}
-
-// Boundary nodes: one thread per entry of the compact boundary-node list;
-// the general gather, then the inlet reconstruction on the west face.
-template <class S, bool kSmag>
-__global__ void __launch_bounds__(128) boundary3d_kernel(Geom3D g,
-                                                         Phys3D<typename Storage<S>::A> p,
-                                                         const S* __restrict__ src,
-                                                         S* __restrict__ dst, StepBuffers3D b) {
-    using A = typename Storage<S>::A;
-    using T = Storage<S>;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.boundary_nodes) {
+        for (int i = 0; i < d3::Q; ++i) {
+            T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
+        }
         return;
     }
-    const uint64_t here = b.bnode[k];
-    const uint32_t z = static_cast<uint32_t>(here / g.plane);
-    const uint32_t rest = static_cast<uint32_t>(here - static_cast<uint64_t>(z) * g.plane);
-    const uint32_t y = rest / g.nx;
-    const uint32_t x = rest - y * g.nx;
     A f[d3::Q];
-    A wall_rho = A(-1);
-    gather_all3<S, 0>(g, p, src, b, b.bslot[k], static_cast<int>(x), static_cast<int>(y),
-                      static_cast<int>(z), here, wall_rho, f);
-    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0) {
+    if (cls == kBulk) {
+        const int64_t nx = g.nx, plane = g.plane;
+        const bool xlo = x == 0u, xhi = x + 1u == g.nx;
+        // x = -1 wraps to nx - 1 (periodic) or is an inlet unknown whose read
+        // is discarded; x = nx wraps to 0 or copies the outlet node x = nx - 1.
+        const int64_t shift_lo = g.x_mode == ORR_X_PERIODIC ? nx : 0;
+        const int64_t shift_hi = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            int64_t source = static_cast<int64_t>(here) -
+                             (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+            if (d3::cx(i) > 0 && xlo) source += shift_lo;
+            if (d3::cx(i) < 0 && xhi) source += shift_hi;
+            f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+        }
+        if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
+            // Convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).
+            A* hist = static_cast<A*>(b.hist);
+            const A u = p.outlet_speed;
+            const uint64_t at = static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
+            const uint64_t face = static_cast<uint64_t>(g.ny) * g.nz;
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                if (d3::cx(i) < 0) {
+                    const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
+                    const A v = (hist[k] + u * f[i]) / (A(1) + u);
+                    hist[k] = v;
+                    f[i] = v;
+                }
+            }
+        }
+    } else {
+        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+        const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
+        A wall_rho = A(-1);
+        gather_all3<S, 0, true>(g, p, src, b, slot, mask, static_cast<int>(x), static_cast<int>(y),
+                                static_cast<int>(z), here, wall_rho, f);
+    }
+    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
         inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
     }
     finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);

@@ -84,8 +84,10 @@ ORR_HD constexpr int outlet_slot(int i) {
 constexpr int kOutletSlots = 3;
 } // namespace d2
 
-// Node classes of the step: solid (skipped), bulk fluid (plain pull
-// streaming) and boundary fluid (the general gather).
-enum : uint8_t { kSolid = 0, kBulk = 1, kBoundary = 2 };
+// Node classes of the step: solid (skipped), bulk fluid (interior, plain pull
+// streaming), listed fluid (a solid source, or an x-edge node of an interior
+// row: the general gather over the node list) and face fluid (a node of a
+// row on the y or z faces with no solid source: the row-uniform side rules).
+enum : uint8_t { kSolid = 0, kBulk = 1, kBoundary = 2, kFace = 3 };
 
 } // namespace orr

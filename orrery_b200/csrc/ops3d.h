@@ -14,14 +14,11 @@ struct Geom3D;
 struct StepBuffers3D;
 
 struct Ops3D {
-    // The two halves of one fused step src -> dst, over disjoint nodes:
-    // the interior-row bulk nodes and the boundary-node list.  `phys` points
-    // at a Phys3D of the storage's arithmetic type; `block` is the bulk
-    // block width (threads along x).
-    cudaError_t (*bulk)(const Geom3D& g, const void* phys, const void* src, void* dst,
+    // One fused step src -> dst (one launch).  `phys` points at a Phys3D of
+    // the storage's arithmetic type; `block` is the block width (threads
+    // along x of a row, and list entries per block).
+    cudaError_t (*step)(const Geom3D& g, const void* phys, const void* src, void* dst,
                         const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s);
-    cudaError_t (*boundary)(const Geom3D& g, const void* phys, const void* src, void* dst,
-                            const StepBuffers3D& b, bool smag, cudaStream_t s);
     // Equilibrium initialisation of a population buffer; rho..uz may be
     // device arrays (all non-null) or null for the uniform state (r0, u0).
     cudaError_t (*init)(const Geom3D& g, const uint8_t* cls, const double* rho, const double* ux,
@@ -35,8 +32,8 @@ struct Ops3D {
                          cudaStream_t s);
     cudaError_t (*mass)(const Geom3D& g, const uint8_t* cls, const void* f, double* out,
                         cudaStream_t s);
-    // Registers per thread of the bulk kernel (for the tuner and the docs).
-    int (*bulk_registers)(bool smag);
+    // Registers per thread of the step kernel (for the tuner and the docs).
+    int (*step_registers)(bool smag);
 };
 
 const Ops3D& ops3d_f32();

@@ -12,37 +12,18 @@ namespace orr {
 template <class S> struct Launch3D {
     using A = typename Storage<S>::A;
 
-    static constexpr unsigned kBoundaryBlock = 128;
-
-    static cudaError_t bulk(const Geom3D& g, const void* phys, const void* src, void* dst,
+    static cudaError_t step(const Geom3D& g, const void* phys, const void* src, void* dst,
                             const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s) {
         Geom3D gg = g;
         gg.tiles_x = (g.nx + block - 1) / block;
-        const uint64_t blocks = static_cast<uint64_t>(g.ny - 2) * (g.nz - 2) * gg.tiles_x;
+        const uint64_t blocks = static_cast<uint64_t>(g.ny) * g.nz * gg.tiles_x;
         const auto& p = *static_cast<const Phys3D<A>*>(phys);
         if (smag) {
-            bulk3d_kernel<S, true><<<static_cast<unsigned>(blocks), block, 0, s>>>(
+            step3d_kernel<S, true><<<static_cast<unsigned>(blocks), block, 0, s>>>(
                 gg, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
         } else {
-            bulk3d_kernel<S, false><<<static_cast<unsigned>(blocks), block, 0, s>>>(
+            step3d_kernel<S, false><<<static_cast<unsigned>(blocks), block, 0, s>>>(
                 gg, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
-        }
-        return cudaGetLastError();
-    }
-
-    static cudaError_t boundary(const Geom3D& g, const void* phys, const void* src, void* dst,
-                                const StepBuffers3D& b, bool smag, cudaStream_t s) {
-        if (g.boundary_nodes == 0) {
-            return cudaSuccess;
-        }
-        const unsigned blocks = (g.boundary_nodes + kBoundaryBlock - 1) / kBoundaryBlock;
-        const auto& p = *static_cast<const Phys3D<A>*>(phys);
-        if (smag) {
-            boundary3d_kernel<S, true><<<blocks, kBoundaryBlock, 0, s>>>(
-                g, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
-        } else {
-            boundary3d_kernel<S, false><<<blocks, kBoundaryBlock, 0, s>>>(
-                g, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
         }
         return cudaGetLastError();
     }
@@ -95,16 +76,15 @@ template <class S> struct Launch3D {
         return cudaGetLastError();
     }
 
-    static int bulk_registers(bool smag) {
+    static int step_registers(bool smag) {
         cudaFuncAttributes a{};
-        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, bulk3d_kernel<S, true>)
-                                   : cudaFuncGetAttributes(&a, bulk3d_kernel<S, false>);
+        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, step3d_kernel<S, true>)
+                                   : cudaFuncGetAttributes(&a, step3d_kernel<S, false>);
         return e == cudaSuccess ? a.numRegs : -1;
     }
 
     static const Ops3D& table() {
-        static const Ops3D ops{&bulk, &boundary, &init, &history, &moments, &force, &mass,
-                               &bulk_registers};
+        static const Ops3D ops{&step, &init, &history, &moments, &force, &mass, &step_registers};
         return ops;
     }
 };

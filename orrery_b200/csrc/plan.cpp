@@ -346,6 +346,17 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     for (int i = 0; i < d3::Q; ++i) {
         off[i] = -d3::cx(i) - nx * d3::cy(i) - plane * d3::cz(i);
     }
+    // Classes for the step kernel's lanes (the result does not depend on
+    // them): nodes with a solid source after the side rules are boundary
+    // nodes (bounce-back mask per node); the other nodes of interior rows are
+    // bulk (x-edges included) and those of the y and z face rows take the
+    // face path.  Links are collected in scan order (cell, then direction),
+    // the order of boundary_links.
+    const bool interpolated = c.solid_wall == ORR_SOLID_INTERPOLATED;
+    p.nmask.assign(p.cells, 0u);
+    if (interpolated) {
+        p.nslot.assign(p.cells, -1);
+    }
     for (long z = 0; z < nz; ++z) {
         for (long y = 0; y < ny; ++y) {
             for (long x = 0; x < nx; ++x) {
@@ -355,41 +366,51 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
                     continue;
                 }
                 ++p.fluid;
-                bool boundary = x == 0 || y == 0 || z == 0 || x + 1 == nx || y + 1 == ny ||
-                                z + 1 == nz;
-                for (int i = 1; i < d3::Q && !boundary; ++i) {
-                    boundary = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+                const bool face_row = y == 0 || z == 0 || y + 1 == ny || z + 1 == nz;
+                const bool x_edge = x == 0 || x + 1 == nx;
+                if (!face_row && !x_edge) {
+                    bool near = false;
+                    for (int i = 1; i < d3::Q && !near; ++i) {
+                        near = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+                    }
+                    if (!near) {
+                        continue; // kBulk
+                    }
                 }
-                if (boundary) {
-                    p.cls[h] = kBoundary;
-                    p.bnode.push_back(static_cast<uint32_t>(h));
+                int32_t slot = -1;
+                bool linked = false;
+                uint32_t mask = 0;
+                for (int i = 1; i < d3::Q; ++i) {
+                    if (!bounces3d(c, solid, x, y, z, i)) {
+                        continue;
+                    }
+                    linked = true;
+                    mask |= 1u << i;
+                    const double q = link_fraction3d(c, solid, distance, x, y, z, i);
+                    p.link_cell.push_back(static_cast<uint32_t>(h));
+                    p.link_dir.push_back(static_cast<uint32_t>(i));
+                    p.link_q.push_back(q);
+                    if (interpolated) {
+                        if (slot < 0) {
+                            slot = static_cast<int32_t>(p.wall_q.size() / d3::Q);
+                            p.wall_q.insert(p.wall_q.end(), d3::Q, 0.5);
+                        }
+                        p.wall_q[static_cast<std::size_t>(slot) * d3::Q + static_cast<std::size_t>(i)] = q;
+                    }
                 }
-            }
-        }
-    }
-    // Links of the boundary nodes in scan order; bulk nodes have none.
-    const bool interpolated = c.solid_wall == ORR_SOLID_INTERPOLATED;
-    p.bslot.assign(p.bnode.size(), -1);
-    for (std::size_t b = 0; b < p.bnode.size(); ++b) {
-        const std::size_t h = p.bnode[b];
-        const long z = static_cast<long>(h / static_cast<std::size_t>(plane));
-        const long rest = static_cast<long>(h % static_cast<std::size_t>(plane));
-        const long y = rest / nx, x = rest % nx;
-        for (int i = 1; i < d3::Q; ++i) {
-            if (!bounces3d(c, solid, x, y, z, i)) {
-                continue;
-            }
-            const double q = link_fraction3d(c, solid, distance, x, y, z, i);
-            p.link_cell.push_back(static_cast<uint32_t>(h));
-            p.link_dir.push_back(static_cast<uint32_t>(i));
-            p.link_q.push_back(q);
-            if (interpolated) {
-                if (p.bslot[b] < 0) {
-                    p.bslot[b] = static_cast<int32_t>(p.wall_q.size() / d3::Q);
-                    p.wall_q.insert(p.wall_q.end(), d3::Q, 0.5);
+                if (!linked) {
+                    if (face_row) {
+                        p.cls[h] = kFace;
+                        ++p.general;
+                    }
+                    continue; // interior-row x-edge node: bulk
                 }
-                p.wall_q[static_cast<std::size_t>(p.bslot[b]) * d3::Q + static_cast<std::size_t>(i)] =
-                    q;
+                p.cls[h] = kBoundary;
+                ++p.general;
+                p.nmask[h] = mask;
+                if (interpolated) {
+                    p.nslot[h] = slot;
+                }
             }
         }
     }
@@ -397,8 +418,7 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
 }
 
 std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links,
-                                    std::size_t boundary_nodes, std::size_t wall_slots,
-                                    int32_t storage) {
+                                    std::size_t wall_slots, int32_t storage) {
     const auto cells = cells3d(c.nx, c.ny, c.nz);
     if (!cells) {
         return std::nullopt;
@@ -407,14 +427,14 @@ std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links
     std::size_t total = 0, t = 0;
     // Two population buffers.
     if (!mul(*cells, d3::Q * s * 2, t) || !add(total, t, total)) return std::nullopt;
-    // Node classes (one byte) and four moment planes.
-    if (!mul(*cells, 1 + 4 * a, t) || !add(total, t, total)) return std::nullopt;
+    // Node classes (one byte), bounce-back masks, wall slots and four moment planes.
+    const std::size_t slot_bytes = c.solid_wall == ORR_SOLID_INTERPOLATED ? 4 : 0;
+    if (!mul(*cells, 1 + 4 + slot_bytes + 4 * a, t) || !add(total, t, total)) return std::nullopt;
     // Outlet history.
     std::size_t face = 0;
     if (!mul(c.ny, c.nz, face) || !mul(face, d3::kOutletSlots * a, t) || !add(total, t, total))
         return std::nullopt;
-    // Boundary-node list (cell and wall slot) and wall fractions.
-    if (!mul(boundary_nodes, 8, t) || !add(total, t, total)) return std::nullopt;
+    // Wall fractions.
     if (!mul(std::max<std::size_t>(wall_slots, 1), d3::Q * a, t) || !add(total, t, total))
         return std::nullopt;
     // Links: cell, direction, fraction.

@@ -32,9 +32,10 @@ struct Plan3D {
     orr_lbm3d_config c{};
     std::size_t cells = 0;
     std::size_t fluid = 0;
-    std::vector<uint8_t> cls;           // kSolid / kBulk / kBoundary per cell
-    std::vector<uint32_t> bnode;        // boundary node cells, scan order
-    std::vector<int32_t> bslot;         // wall slot per boundary node, -1 none
+    std::vector<uint8_t> cls;           // kSolid / kBulk / kBoundary / kFace per cell
+    std::vector<uint32_t> nmask;        // per cell, bit i: direction i bounces back
+    std::vector<int32_t> nslot;         // per cell wall slot (interpolated wall only), -1 none
+    std::size_t general = 0;            // nodes on the general gather (face + boundary)
     std::vector<double> wall_q;         // 19 fractions per slot
     std::vector<uint32_t> link_cell;    // boundary links, scan order
     std::vector<uint32_t> link_dir;
@@ -47,11 +48,11 @@ struct Plan3D {
 Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* distance);
 
 // Bytes the device solver allocates for a lattice: populations twice, node
-// classes, moments, outlet history, boundary-node list, wall table, links and
-// the small reduction buffers.  Empty on overflow.
+// classes and bounce-back masks (and wall slots for the interpolated wall),
+// moments, outlet history, wall table, links and the small reduction buffers.
+// Empty on overflow.
 std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links,
-                                    std::size_t boundary_nodes, std::size_t wall_slots,
-                                    int32_t storage);
+                                    std::size_t wall_slots, int32_t storage);
 
 // ---- D2Q9 ----
 

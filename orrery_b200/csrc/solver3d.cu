@@ -5,15 +5,15 @@
 // Device layout (one allocation per table):
 //   populations   two buffers of 19 * cells storage values, structure of
 //                 arrays f[i * cells + x + nx (y + ny z)]; ping-pong (A-B)
-//   classes       one byte per node (solid / bulk / boundary)
-//   boundary list cell and wall slot of every boundary fluid node
+//   classes       one byte per node (solid / bulk / face / boundary)
+//   masks         per node, the directions that bounce back (solid source)
+//   slots         per node, the wall-table slot (interpolated wall only)
 //   wall table    19 fractions per slot (interpolated wall)
 //   links         cell, direction and fraction of every boundary link
 //   moments       4 planes (rho or rho - 1, ux, uy, uz) for read-back
 //   history       5 * ny * nz convective-outlet values
 //   small         inlet velocity (3), force/moment (6) and mass accumulators
-// Steps run as CUDA graphs of kGraphSteps steps, each step a fork into the
-// boundary kernel (side stream) and the bulk kernel (main stream).
+// Steps run as CUDA graphs of kGraphSteps steps, one kernel launch each.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -78,16 +78,13 @@ struct orr_lbm3d {
     std::size_t abytes = 4;
 
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr;
-    cudaEvent_t join = nullptr;
     cudaGraphExec_t graph = nullptr;
 
     void* f[2] = {nullptr, nullptr};
     int cur = 0;
     uint8_t* cls = nullptr;
-    uint32_t* bnode = nullptr;
-    int32_t* bslot = nullptr;
+    uint32_t* nmask = nullptr;
+    int32_t* nslot = nullptr;
     void* wall_q = nullptr;
     void* hist = nullptr;
     void* moments = nullptr;
@@ -112,8 +109,8 @@ struct orr_lbm3d {
     StepBuffers3D buffers() const {
         StepBuffers3D b{};
         b.cls = cls;
-        b.bnode = bnode;
-        b.bslot = bslot;
+        b.nmask = nmask;
+        b.nslot = nslot;
         b.wall_q = wall_q;
         b.hist = hist;
         b.inlet = small;
@@ -127,28 +124,24 @@ struct orr_lbm3d {
             cudaSetDevice(device);
         }
         if (graph) cudaGraphExecDestroy(graph);
-        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(bnode),
-                        static_cast<void*>(bslot), wall_q, hist, moments,
+        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(nmask),
+                        static_cast<void*>(nslot), wall_q, hist, moments,
                         static_cast<void*>(lcell), static_cast<void*>(ldir),
                         static_cast<void*>(lq), small}) {
             if (p) cudaFree(p);
         }
         if (host_small) cudaFreeHost(host_small);
-        if (fork) cudaEventDestroy(fork);
-        if (join) cudaEventDestroy(join);
-        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
         graph = nullptr;
         f[0] = f[1] = nullptr;
         cls = nullptr;
-        bnode = nullptr;
-        bslot = nullptr;
+        nmask = nullptr;
+        nslot = nullptr;
         wall_q = hist = moments = small = nullptr;
         lcell = ldir = nullptr;
         lq = nullptr;
         host_small = nullptr;
-        fork = join = nullptr;
-        side = stream = nullptr;
+        stream = nullptr;
     }
 
     // Uploads the imposed inlet velocity in the arithmetic type.
@@ -170,22 +163,10 @@ struct orr_lbm3d {
         check(cudaStreamSynchronize(stream), "inlet upload");
     }
 
-    // One step src -> dst on `stream`; in capture mode the boundary kernel
-    // runs on the side stream as a parallel branch.
-    void launch_step(int from, bool branch) {
-        const StepBuffers3D b = buffers();
-        if (branch && g.boundary_nodes > 0) {
-            check(cudaEventRecord(fork, stream), "step fork");
-            check(cudaStreamWaitEvent(side, fork, 0), "step fork");
-            check(ops->boundary(g, phys(), f[from], f[1 - from], b, smag, side), "boundary kernel");
-            check(ops->bulk(g, phys(), f[from], f[1 - from], b, smag, block, stream), "bulk kernel");
-            check(cudaEventRecord(join, side), "step join");
-            check(cudaStreamWaitEvent(stream, join, 0), "step join");
-        } else {
-            check(ops->boundary(g, phys(), f[from], f[1 - from], b, smag, stream), "boundary kernel");
-            check(ops->bulk(g, phys(), f[from], f[1 - from], b, smag, block, stream), "bulk kernel");
-        }
-        launches += g.boundary_nodes > 0 ? 2 : 1;
+    // One step src -> dst on `stream` (one kernel launch).
+    void launch_step(int from) {
+        check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream), "step kernel");
+        ++launches;
     }
 
     void build_graph() {
@@ -194,7 +175,7 @@ struct orr_lbm3d {
         const uint64_t before = launches;
         try {
             for (uint32_t k = 0; k < kGraphSteps; ++k) {
-                launch_step(static_cast<int>(k & 1u), true);
+                launch_step(static_cast<int>(k & 1u));
             }
         } catch (...) {
             cudaStreamEndCapture(stream, &captured);
@@ -213,7 +194,7 @@ struct orr_lbm3d {
         uint64_t left = count;
         if (left >= kGraphSteps) {
             if (cur != 0) {
-                launch_step(cur, false);
+                launch_step(cur);
                 cur = 1 - cur;
                 --left;
             }
@@ -222,12 +203,12 @@ struct orr_lbm3d {
             }
             while (left >= kGraphSteps) {
                 check(cudaGraphLaunch(graph, stream), "graph launch");
-                launches += static_cast<uint64_t>(kGraphSteps) * (g.boundary_nodes > 0 ? 2 : 1);
+                launches += kGraphSteps;
                 left -= kGraphSteps;
             }
         }
         for (; left > 0; --left) {
-            launch_step(cur, false);
+            launch_step(cur);
             cur = 1 - cur;
         }
         steps += count;
@@ -341,7 +322,7 @@ orr_status orr_lbm3d_memory_bytes(const orr_lbm3d_config* config, uint64_t links
     if (config == nullptr || bytes == nullptr) {
         return orr::fail(ORR_ERR_INVALID, "null argument");
     }
-    const auto m = orr::memory3d(*config, links, boundary_nodes,
+    const auto m = orr::memory3d(*config, links,
                                  config->solid_wall == ORR_SOLID_INTERPOLATED ? boundary_nodes : 0,
                                  storage);
     if (!m) {
@@ -367,7 +348,7 @@ orr_status orr_lbm3d_plan(const orr_lbm3d_config* config, const uint8_t* solid,
         const std::size_t n = p.link_cell.size();
         if (links) *links = n;
         if (fluid) *fluid = p.fluid;
-        if (boundary_nodes) *boundary_nodes = p.bnode.size();
+        if (boundary_nodes) *boundary_nodes = p.general;
         if (cell) std::memcpy(cell, p.link_cell.data(), n * 4);
         if (direction) std::memcpy(direction, p.link_dir.data(), n * 4);
         if (q) std::memcpy(q, p.link_q.data(), n * 8);
@@ -410,7 +391,7 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         // The memory check counts every table the solver allocates
         // (check_memory, lbm3d_gpu.cpp:129-149).
         const std::size_t slots = p.wall_q.size() / d3::Q;
-        const auto need = memory3d(*config, p.link_cell.size(), p.bnode.size(), slots, o.storage);
+        const auto need = memory3d(*config, p.link_cell.size(), slots, o.storage);
         if (!need) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the device memory of the lattice overflows std::size_t"};
         }
@@ -428,7 +409,6 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         g.nz = static_cast<uint32_t>(config->nz);
         g.plane = g.nx * g.ny;
         g.cells = p.cells;
-        g.boundary_nodes = static_cast<uint32_t>(p.bnode.size());
         g.x_mode = config->x_boundary;
         g.outlet_mode = config->outlet;
         g.y_lo = config->y_low.kind;
@@ -452,16 +432,15 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
                   (binary32 ? h->phys32.smag_c2 > 0.0f : true);
         // Streams and device tables.
         check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
-        check(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "stream");
-        check(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "event");
-        check(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "event");
         const std::size_t cells = p.cells;
         for (int k = 0; k < 2; ++k) {
             check(cudaMalloc(&h->f[k], d3::Q * cells * h->sbytes), "population buffer");
         }
         h->cls = device_alloc<uint8_t>(cells, "node class buffer");
-        h->bnode = device_alloc<uint32_t>(p.bnode.size(), "boundary list");
-        h->bslot = device_alloc<int32_t>(p.bnode.size(), "boundary list");
+        h->nmask = device_alloc<uint32_t>(cells, "bounce-back mask buffer");
+        if (!p.nslot.empty()) {
+            h->nslot = device_alloc<int32_t>(cells, "wall slot buffer");
+        }
         check(cudaMalloc(&h->wall_q, std::max<std::size_t>(slots, 1) * d3::Q * h->abytes), "wall buffer");
         check(cudaMalloc(&h->hist, static_cast<std::size_t>(d3::kOutletSlots) * config->ny * config->nz * h->abytes),
               "outlet buffer");
@@ -474,11 +453,11 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         // Uploads.
         cudaStream_t s = h->stream;
         check(cudaMemcpyAsync(h->cls, p.cls.data(), cells, cudaMemcpyHostToDevice, s), "class upload");
-        if (!p.bnode.empty()) {
-            check(cudaMemcpyAsync(h->bnode, p.bnode.data(), p.bnode.size() * 4, cudaMemcpyHostToDevice, s),
-                  "boundary upload");
-            check(cudaMemcpyAsync(h->bslot, p.bslot.data(), p.bslot.size() * 4, cudaMemcpyHostToDevice, s),
-                  "boundary upload");
+        check(cudaMemcpyAsync(h->nmask, p.nmask.data(), cells * 4, cudaMemcpyHostToDevice, s),
+              "mask upload");
+        if (!p.nslot.empty()) {
+            check(cudaMemcpyAsync(h->nslot, p.nslot.data(), cells * 4, cudaMemcpyHostToDevice, s),
+                  "slot upload");
         }
         {
             std::vector<double> q = p.wall_q;
@@ -504,10 +483,13 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         }
         initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
         check(cudaStreamSynchronize(s), "create");
-        // The plan's class array is on the device now; keep the links.
+        // The per-node tables are on the device now; keep the links.
         h->plan.cls.clear();
         h->plan.cls.shrink_to_fit();
-        h->plan.bnode.shrink_to_fit();
+        h->plan.nmask.clear();
+        h->plan.nmask.shrink_to_fit();
+        h->plan.nslot.clear();
+        h->plan.nslot.shrink_to_fit();
         *out = h.release();
         return ORR_OK;
     });
@@ -719,7 +701,7 @@ orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* fluid, uint6
         return orr::fail(ORR_ERR_INVALID, "null argument");
     }
     if (fluid) *fluid = solver->plan.fluid;
-    if (boundary) *boundary = solver->g.boundary_nodes;
+    if (boundary) *boundary = solver->plan.general;
     return ORR_OK;
 }
 
