@@ -5,9 +5,9 @@
 //   CPU   CpuLbm2D::update_row + collide  (src/aero/lbm/lbm2d_cpu.cpp:26-75, 352-404)
 //   GPU   lbm_d2q9_step                   (src/render/shaders/lbm/lbm_d2q9_step.comp.glsl,
 //                                          lbm_d2q9_common.glsl)
-// with resolve_source (src/aero/lbm/lbm2d_internal.h:36-75), split like the
-// D3Q19 step into a bulk kernel over the interior rows and a boundary kernel
-// over the compact boundary-node list.
+// with resolve_source (src/aero/lbm/lbm2d_internal.h:36-75), organised like
+// the D3Q19 step: one thread per node over all rows, every lane storing its
+// node in the same step (whole sectors), lanes branching by node class.
 #pragma once
 
 #include <cstdint>
@@ -23,7 +23,6 @@ struct Geom2D {
     uint32_t nx, ny;
     uint64_t cells;
     uint32_t tiles_x;
-    uint32_t boundary_nodes;
     int32_t x_mode, outlet_mode;
     int32_t bottom, top; // ORR_WALL_*
     int32_t forced;
@@ -190,14 +189,14 @@ __device__ __forceinline__ void inlet_west2(A (&f)[d2::Q], A ux, A uy) {
 
 struct StepBuffers2D {
     const uint8_t* cls;
-    const uint32_t* bnode;
+    const uint32_t* nmask; // per node, bit i: direction i bounces back
     void* hist;
 };
 
 template <class S, int I>
 __device__ __forceinline__ void gather_one2(const Geom2D& g, const Phys2D<typename Storage<S>::A>& p,
                                             const S* __restrict__ src, const StepBuffers2D& b,
-                                            int x, int y, uint64_t here,
+                                            uint32_t mask, int x, int y, uint64_t here,
                                             typename Storage<S>::A& wall_rho,
                                             typename Storage<S>::A& out) {
     using A = typename Storage<S>::A;
@@ -249,7 +248,7 @@ __device__ __forceinline__ void gather_one2(const Geom2D& g, const Phys2D<typena
         }
     }
     const uint64_t source = static_cast<uint64_t>(sx) + static_cast<uint64_t>(g.nx) * static_cast<uint64_t>(sy);
-    if (b.cls[source] == kSolid) {
+    if (((mask >> I) & 1u) != 0u) {
         out = T::load(src + static_cast<uint64_t>(d2::opposite(I)) * cells + here);
         return;
     }
@@ -258,60 +257,73 @@ __device__ __forceinline__ void gather_one2(const Geom2D& g, const Phys2D<typena
 
 template <class S, int I>
 __device__ __forceinline__ void gather_all2(const Geom2D& g, const Phys2D<typename Storage<S>::A>& p,
-                                            const S* __restrict__ src, const StepBuffers2D& b, int x,
-                                            int y, uint64_t here, typename Storage<S>::A& wall_rho,
+                                            const S* __restrict__ src, const StepBuffers2D& b,
+                                            uint32_t mask, int x, int y, uint64_t here,
+                                            typename Storage<S>::A& wall_rho,
                                             typename Storage<S>::A (&f)[d2::Q]) {
     if constexpr (I < d2::Q) {
-        gather_one2<S, I>(g, p, src, b, x, y, here, wall_rho, f[I]);
-        gather_all2<S, I + 1>(g, p, src, b, x, y, here, wall_rho, f);
+        gather_one2<S, I>(g, p, src, b, mask, x, y, here, wall_rho, f[I]);
+        gather_all2<S, I + 1>(g, p, src, b, mask, x, y, here, wall_rho, f);
     }
 }
 
+// One fused step src -> dst: one thread per node, one block per row tile,
+// all rows; solid lanes store their rest populations, bulk lanes (interior
+// rows, x-edges shifted) pull plainly, face and boundary lanes take the
+// general gather (see step3d_kernel for the reasons).
 template <class S, bool kSmag>
-__global__ void __launch_bounds__(256) bulk2d_kernel(Geom2D g, Phys2D<typename Storage<S>::A> p,
+__global__ void __launch_bounds__(256) step2d_kernel(Geom2D g, Phys2D<typename Storage<S>::A> p,
                                                      const S* __restrict__ src, S* __restrict__ dst,
                                                      StepBuffers2D b) {
     using A = typename Storage<S>::A;
     using T = Storage<S>;
-    const uint32_t row = blockIdx.x / g.tiles_x;
-    const uint32_t x = (blockIdx.x - row * g.tiles_x) * blockDim.x + threadIdx.x;
-    const uint32_t y = 1u + row;
-    if (x == 0 || x >= g.nx - 1u) {
+    const uint32_t y = blockIdx.x / g.tiles_x;
+    const uint32_t x = (blockIdx.x - y * g.tiles_x) * blockDim.x + threadIdx.x;
+    if (x >= g.nx) {
         return;
     }
     const uint64_t here = x + static_cast<uint64_t>(g.nx) * y;
-    if (b.cls[here] != kBulk) {
+    const uint8_t cls = b.cls[here];
+    if (cls == kSolid) {
+#pragma unroll
+        for (int i = 0; i < d2::Q; ++i) {
+            T::store(dst + static_cast<uint64_t>(i) * g.cells + here, T::kShifted ? A(0) : A(d2::w(i)));
+        }
         return;
     }
-    const int64_t nx = g.nx;
     A f[d2::Q];
+    if (cls == kBulk) {
+        const int64_t nx = g.nx;
+        const bool xlo = x == 0u, xhi = x + 1u == g.nx;
+        const int64_t shift_lo = g.x_mode == ORR_X_PERIODIC ? nx : 0;
+        const int64_t shift_hi = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
 #pragma unroll
-    for (int i = 0; i < d2::Q; ++i) {
-        const int64_t off = d2::cx(i) + nx * d2::cy(i);
-        f[i] = T::load(src + static_cast<uint64_t>(i) * g.cells + static_cast<uint64_t>(static_cast<int64_t>(here) - off));
-    }
-    collide2<A, T::kShifted, kSmag>(f, p, g.forced);
+        for (int i = 0; i < d2::Q; ++i) {
+            int64_t source = static_cast<int64_t>(here) - (d2::cx(i) + nx * d2::cy(i));
+            if (d2::cx(i) > 0 && xlo) source += shift_lo;
+            if (d2::cx(i) < 0 && xhi) source += shift_hi;
+            f[i] = T::load(src + static_cast<uint64_t>(i) * g.cells + static_cast<uint64_t>(source));
+        }
+        if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
+            A* hist = static_cast<A*>(b.hist);
+            const A u = p.outlet_speed;
 #pragma unroll
-    for (int i = 0; i < d2::Q; ++i) T::store(dst + static_cast<uint64_t>(i) * g.cells + here, f[i]);
-}
-
-template <class S, bool kSmag>
-__global__ void __launch_bounds__(128) boundary2d_kernel(Geom2D g, Phys2D<typename Storage<S>::A> p,
-                                                         const S* __restrict__ src, S* __restrict__ dst,
-                                                         StepBuffers2D b) {
-    using A = typename Storage<S>::A;
-    using T = Storage<S>;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.boundary_nodes) {
-        return;
+            for (int i = 0; i < d2::Q; ++i) {
+                if (d2::cx(i) < 0) {
+                    const uint64_t k = static_cast<uint64_t>(d2::outlet_slot(i)) * g.ny + y;
+                    const A v = (hist[k] + u * f[i]) / (A(1) + u);
+                    hist[k] = v;
+                    f[i] = v;
+                }
+            }
+        }
+    } else {
+        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+        A wall_rho = A(-1);
+        gather_all2<S, 0>(g, p, src, b, mask, static_cast<int>(x), static_cast<int>(y), here,
+                          wall_rho, f);
     }
-    const uint64_t here = b.bnode[k];
-    const uint32_t y = static_cast<uint32_t>(here / g.nx);
-    const uint32_t x = static_cast<uint32_t>(here - static_cast<uint64_t>(y) * g.nx);
-    A f[d2::Q];
-    A wall_rho = A(-1);
-    gather_all2<S, 0>(g, p, src, b, static_cast<int>(x), static_cast<int>(y), here, wall_rho, f);
-    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0) {
+    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
         inlet_west2<A, T::kShifted>(f, p.inlet_ux, p.inlet_uy);
     }
     collide2<A, T::kShifted, kSmag>(f, p, g.forced);

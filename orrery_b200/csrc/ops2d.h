@@ -12,10 +12,9 @@ struct Geom2D;
 struct StepBuffers2D;
 
 struct Ops2D {
-    cudaError_t (*bulk)(const Geom2D& g, const void* phys, const void* src, void* dst,
+    // One fused step src -> dst (one launch over all rows).
+    cudaError_t (*step)(const Geom2D& g, const void* phys, const void* src, void* dst,
                         const StepBuffers2D& b, bool smag, uint32_t block, cudaStream_t s);
-    cudaError_t (*boundary)(const Geom2D& g, const void* phys, const void* src, void* dst,
-                            const StepBuffers2D& b, bool smag, cudaStream_t s);
     cudaError_t (*init)(const Geom2D& g, const uint8_t* cls, const double* rho, const double* ux,
                         const double* uy, double u0x, double u0y, void* f0, cudaStream_t s);
     cudaError_t (*history)(const Geom2D& g, const void* f, void* hist, cudaStream_t s);

@@ -10,37 +10,18 @@ namespace orr {
 
 template <class S> struct Launch2D {
     using A = typename Storage<S>::A;
-    static constexpr unsigned kBoundaryBlock = 128;
-
-    static cudaError_t bulk(const Geom2D& g, const void* phys, const void* src, void* dst,
+    static cudaError_t step(const Geom2D& g, const void* phys, const void* src, void* dst,
                             const StepBuffers2D& b, bool smag, uint32_t block, cudaStream_t s) {
         Geom2D gg = g;
         gg.tiles_x = (g.nx + block - 1) / block;
-        const unsigned blocks = (g.ny - 2) * gg.tiles_x;
+        const unsigned blocks = g.ny * gg.tiles_x;
         const auto& p = *static_cast<const Phys2D<A>*>(phys);
         if (smag) {
-            bulk2d_kernel<S, true><<<blocks, block, 0, s>>>(gg, p, static_cast<const S*>(src),
+            step2d_kernel<S, true><<<blocks, block, 0, s>>>(gg, p, static_cast<const S*>(src),
                                                             static_cast<S*>(dst), b);
         } else {
-            bulk2d_kernel<S, false><<<blocks, block, 0, s>>>(gg, p, static_cast<const S*>(src),
+            step2d_kernel<S, false><<<blocks, block, 0, s>>>(gg, p, static_cast<const S*>(src),
                                                              static_cast<S*>(dst), b);
-        }
-        return cudaGetLastError();
-    }
-
-    static cudaError_t boundary(const Geom2D& g, const void* phys, const void* src, void* dst,
-                                const StepBuffers2D& b, bool smag, cudaStream_t s) {
-        if (g.boundary_nodes == 0) {
-            return cudaSuccess;
-        }
-        const unsigned blocks = (g.boundary_nodes + kBoundaryBlock - 1) / kBoundaryBlock;
-        const auto& p = *static_cast<const Phys2D<A>*>(phys);
-        if (smag) {
-            boundary2d_kernel<S, true><<<blocks, kBoundaryBlock, 0, s>>>(
-                g, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
-        } else {
-            boundary2d_kernel<S, false><<<blocks, kBoundaryBlock, 0, s>>>(
-                g, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
         }
         return cudaGetLastError();
     }
@@ -90,7 +71,7 @@ template <class S> struct Launch2D {
     }
 
     static const Ops2D& table() {
-        static const Ops2D ops{&bulk, &boundary, &init, &history, &moments, &force, &mass};
+        static const Ops2D ops{&step, &init, &history, &moments, &force, &mass};
         return ops;
     }
 };

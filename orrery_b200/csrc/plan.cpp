@@ -537,6 +537,10 @@ Plan2D plan2d(const orr_lbm2d_config& c, const uint8_t* solid) {
     for (int i = 0; i < d2::Q; ++i) {
         off[i] = -d2::cx(i) - nx * d2::cy(i);
     }
+    p.nmask.assign(p.cells, 0u);
+    // Classes as in plan3d: nodes with a solid source are boundary nodes,
+    // other interior-row nodes bulk, other bottom/top-row nodes face nodes;
+    // links (boundary_links, lbm2d_common.cpp:79-97) in scan order.
     for (long y = 0; y < ny; ++y) {
         for (long x = 0; x < nx; ++x) {
             const std::size_t h = static_cast<std::size_t>(x + nx * y);
@@ -545,37 +549,46 @@ Plan2D plan2d(const orr_lbm2d_config& c, const uint8_t* solid) {
                 continue;
             }
             ++p.fluid;
-            bool boundary = x == 0 || y == 0 || x + 1 == nx || y + 1 == ny;
-            for (int i = 1; i < d2::Q && !boundary; ++i) {
-                boundary = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+            const bool face_row = y == 0 || y + 1 == ny;
+            const bool x_edge = x == 0 || x + 1 == nx;
+            if (!face_row && !x_edge) {
+                bool near = false;
+                for (int i = 1; i < d2::Q && !near; ++i) {
+                    near = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
+                }
+                if (!near) {
+                    continue; // kBulk
+                }
             }
-            if (boundary) {
+            uint32_t mask = 0;
+            for (int i = 1; i < d2::Q; ++i) {
+                long sx = x - d2::cx(i), sy = y - d2::cy(i);
+                if (sy < 0 || sy >= ny) {
+                    const orr_wall& w = sy < 0 ? c.bottom : c.top;
+                    if (w.kind == ORR_WALL_NO_SLIP) {
+                        continue;
+                    }
+                    sy = w.kind == ORR_WALL_PERIODIC ? (sy + ny) % ny : y;
+                }
+                if (sx < 0 || sx >= nx) {
+                    if (c.x_boundary != ORR_X_PERIODIC) {
+                        continue;
+                    }
+                    sx = (sx + nx) % nx;
+                }
+                if (solid[static_cast<std::size_t>(sx + nx * sy)] != 0) {
+                    mask |= 1u << i;
+                    p.link_cell.push_back(static_cast<uint32_t>(h));
+                    p.link_dir.push_back(static_cast<uint32_t>(i));
+                }
+            }
+            if (mask != 0u) {
                 p.cls[h] = kBoundary;
-                p.bnode.push_back(static_cast<uint32_t>(h));
-            }
-        }
-    }
-    // boundary_links (lbm2d_common.cpp:79-97) over the boundary nodes.
-    for (const uint32_t h : p.bnode) {
-        const long x = static_cast<long>(h) % nx, y = static_cast<long>(h) / nx;
-        for (int i = 1; i < d2::Q; ++i) {
-            long sx = x - d2::cx(i), sy = y - d2::cy(i);
-            if (sy < 0 || sy >= ny) {
-                const orr_wall& w = sy < 0 ? c.bottom : c.top;
-                if (w.kind == ORR_WALL_NO_SLIP) {
-                    continue;
-                }
-                sy = w.kind == ORR_WALL_PERIODIC ? (sy + ny) % ny : y;
-            }
-            if (sx < 0 || sx >= nx) {
-                if (c.x_boundary != ORR_X_PERIODIC) {
-                    continue;
-                }
-                sx = (sx + nx) % nx;
-            }
-            if (solid[static_cast<std::size_t>(sx + nx * sy)] != 0) {
-                p.link_cell.push_back(h);
-                p.link_dir.push_back(static_cast<uint32_t>(i));
+                p.nmask[h] = mask;
+                ++p.general;
+            } else if (face_row) {
+                p.cls[h] = kFace;
+                ++p.general;
             }
         }
     }
@@ -583,14 +596,14 @@ Plan2D plan2d(const orr_lbm2d_config& c, const uint8_t* solid) {
 }
 
 std::optional<std::size_t> memory2d(const orr_lbm2d_config& c, std::size_t links,
-                                    std::size_t boundary_nodes, int32_t storage) {
+                                    int32_t storage) {
     if (c.nx == 0 || c.ny == 0 || c.nx > kMaxGridCells / c.ny) {
         return std::nullopt;
     }
     const std::size_t cells = c.nx * c.ny;
     const std::size_t s = storage_bytes(storage), a = arithmetic_bytes(storage);
     return cells * (d2::Q * s * 2 + 1 + 3 * a) + c.ny * d2::kOutletSlots * a +
-           boundary_nodes * 4 + links * 8 + 256;
+           cells * 4 + links * 8 + 256;
 }
 
 } // namespace orr

@@ -65,8 +65,9 @@ struct Plan2D {
     orr_lbm2d_config c{};
     std::size_t cells = 0;
     std::size_t fluid = 0;
+    std::size_t general = 0;            // nodes on the general gather
     std::vector<uint8_t> cls;
-    std::vector<uint32_t> bnode;
+    std::vector<uint32_t> nmask;        // per cell, bit i: direction i bounces back
     std::vector<uint32_t> link_cell;
     std::vector<uint32_t> link_dir;
 };
@@ -74,7 +75,7 @@ struct Plan2D {
 Plan2D plan2d(const orr_lbm2d_config& c, const uint8_t* solid);
 
 std::optional<std::size_t> memory2d(const orr_lbm2d_config& c, std::size_t links,
-                                    std::size_t boundary_nodes, int32_t storage);
+                                    int32_t storage);
 
 std::size_t storage_bytes(int32_t storage);
 std::size_t arithmetic_bytes(int32_t storage);

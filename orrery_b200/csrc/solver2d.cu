@@ -1,9 +1,8 @@
 // The D2Q9 device solver behind the C ABI: the counterpart of the
 // reference's GpuLbm2D (src/aero/lbm/lbm2d_gpu.cpp) and the 2D make_gpu_solver
 // (src/aero/lbm/include/orrery/aero/lbm/lbm2d.h:205-212).  Same layout and
-// execution as the D3Q19 solver: ping-pong SoA populations, a bulk kernel over
-// the interior rows and a boundary kernel over the compact boundary list,
-// replayed as CUDA graphs.
+// execution as the D3Q19 solver: ping-pong SoA populations and one all-rows
+// step kernel per step, replayed as CUDA graphs.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -58,7 +57,7 @@ struct orr_lbm2d {
     void* f[2] = {nullptr, nullptr};
     int cur = 0;
     uint8_t* cls = nullptr;
-    uint32_t* bnode = nullptr;
+    uint32_t* nmask = nullptr;
     void* hist = nullptr;
     void* moments = nullptr;
     uint32_t* lcell = nullptr;
@@ -72,12 +71,12 @@ struct orr_lbm2d {
         return storage == ORR_STORAGE_F64 ? static_cast<const void*>(&phys64)
                                           : static_cast<const void*>(&phys32);
     }
-    StepBuffers2D buffers() const { return StepBuffers2D{cls, bnode, hist}; }
+    StepBuffers2D buffers() const { return StepBuffers2D{cls, nmask, hist}; }
 
     ~orr_lbm2d() {
         cudaSetDevice(device);
         if (graph) cudaGraphExecDestroy(graph);
-        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(bnode), hist, moments,
+        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(nmask), hist, moments,
                         static_cast<void*>(lcell), static_cast<void*>(ldir), static_cast<void*>(acc)}) {
             if (p) cudaFree(p);
         }
@@ -87,9 +86,8 @@ struct orr_lbm2d {
 
     void launch_step(int from) {
         const StepBuffers2D b = buffers();
-        check(ops->boundary(g, phys(), f[from], f[1 - from], b, smag, stream), "boundary kernel");
-        check(ops->bulk(g, phys(), f[from], f[1 - from], b, smag, block, stream), "bulk kernel");
-        launches += g.boundary_nodes > 0 ? 2 : 1;
+        check(ops->step(g, phys(), f[from], f[1 - from], b, smag, block, stream), "step kernel");
+        ++launches;
     }
 
     void run(uint64_t count) {
@@ -122,7 +120,7 @@ struct orr_lbm2d {
             }
             while (left >= kGraphSteps2) {
                 check(cudaGraphLaunch(graph, stream), "graph launch");
-                launches += static_cast<uint64_t>(kGraphSteps2) * (g.boundary_nodes > 0 ? 2 : 1);
+                launches += kGraphSteps2;
                 left -= kGraphSteps2;
             }
         }
@@ -246,7 +244,7 @@ orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid
         h->abytes = arithmetic_bytes(o.storage);
         h->plan = plan2d(*config, solid);
         const Plan2D& p = h->plan;
-        const auto need = memory2d(*config, p.link_cell.size(), p.bnode.size(), o.storage);
+        const auto need = memory2d(*config, p.link_cell.size(), o.storage);
         std::size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
         if (!need || *need > free_bytes) {
@@ -258,7 +256,6 @@ orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid
         g.nx = static_cast<uint32_t>(config->nx);
         g.ny = static_cast<uint32_t>(config->ny);
         g.cells = p.cells;
-        g.boundary_nodes = static_cast<uint32_t>(p.bnode.size());
         g.x_mode = config->x_boundary;
         g.outlet_mode = config->outlet;
         g.bottom = config->bottom.kind;
@@ -276,8 +273,7 @@ orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid
             check(cudaMalloc(&h->f[k], d2::Q * cells * h->sbytes), "population buffer");
         }
         check(cudaMalloc(reinterpret_cast<void**>(&h->cls), cells), "node class buffer");
-        check(cudaMalloc(reinterpret_cast<void**>(&h->bnode), std::max<std::size_t>(p.bnode.size(), 1) * 4),
-              "boundary list");
+        check(cudaMalloc(reinterpret_cast<void**>(&h->nmask), cells * 4), "bounce-back mask buffer");
         check(cudaMalloc(&h->hist, static_cast<std::size_t>(d2::kOutletSlots) * config->ny * h->abytes),
               "outlet buffer");
         check(cudaMalloc(&h->moments, 3 * cells * h->abytes), "moment buffer");
@@ -289,10 +285,7 @@ orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid
         check(cudaMallocHost(reinterpret_cast<void**>(&h->host_acc), 8 * sizeof(double)), "pinned buffer");
         cudaStream_t s = h->stream;
         check(cudaMemcpyAsync(h->cls, p.cls.data(), cells, cudaMemcpyHostToDevice, s), "class upload");
-        if (!p.bnode.empty()) {
-            check(cudaMemcpyAsync(h->bnode, p.bnode.data(), p.bnode.size() * 4, cudaMemcpyHostToDevice, s),
-                  "boundary upload");
-        }
+        check(cudaMemcpyAsync(h->nmask, p.nmask.data(), cells * 4, cudaMemcpyHostToDevice, s), "mask upload");
         if (!p.link_cell.empty()) {
             check(cudaMemcpyAsync(h->lcell, p.link_cell.data(), p.link_cell.size() * 4, cudaMemcpyHostToDevice, s),
                   "link upload");

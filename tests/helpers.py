@@ -110,3 +110,41 @@ def cylinder_setup(nx, ny, diameter, cx, cy, u, reynolds):
 def copy_config(c):
     import copy
     return copy.deepcopy(c)
+
+
+# D3Q19 tables (d3q19.h:15-36) for the test-side probes.
+CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0])
+CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1])
+W19 = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+
+def _stress(f):
+    rho = float(np.sum(f))
+    u = np.array([np.sum(CX * f), np.sum(CY * f), np.sum(CZ * f)]) / rho
+    cu = CX * u[0] + CY * u[1] + CZ * u[2]
+    feq = W19 * rho * (1 + 3 * cu + 4.5 * cu * cu - 1.5 * float(u @ u))
+    neq = f - feq
+    c = np.stack([CX, CY, CZ])
+    return np.einsum("pi,si,i->ps", c, c, neq), rho
+
+
+def closure_probe(initial, after, node, a, b, tau, constant, n=8):
+    """Effective relaxation time of the first collision at `node` of a
+    periodic n^3 box, and the Smagorinsky closure's prediction
+    (lbm3d_test_support.h:171-239).  initial/after: (19, cells) arrays."""
+    here = node[0] + n * (node[1] + n * node[2])
+    before = np.empty(19)
+    post = np.empty(19)
+    for i in range(19):
+        sx = (node[0] - CX[i]) % n
+        sy = (node[1] - CY[i]) % n
+        sz = (node[2] - CZ[i]) % n
+        before[i] = initial[i, sx + n * (sy + n * sz)]
+        post[i] = after[i, here]
+    pi_before, rho = _stress(before)
+    pi_after, _ = _stress(post)
+    q2 = float(np.sum(pi_before * pi_before))
+    measured = 1.0 / (1.0 - pi_after[a, b] / pi_before[a, b])
+    predicted = 0.5 * (tau + math.sqrt(tau * tau + 18.0 * math.sqrt(2.0) * constant ** 2 * math.sqrt(q2) / rho))
+    return measured, predicted
