@@ -40,9 +40,10 @@ def measured_peak():
 
 
 def dram_traffic(workload: str, storage: str):
-    """Per-launch DRAM bytes of the bulk kernel from the committed ncu summary
-    of this workload (profiles/*.txt line 'traffic_bytes_per_step <storage> <B>')."""
-    path = os.path.join(ROOT, "profiles", f"bulk3d_{workload}.txt")
+    """Per-launch DRAM bytes (read + write) of the step kernel from the
+    committed ncu summary of this workload (the profiles/ line
+    'traffic_bytes_per_step <storage> <bytes>')."""
+    path = os.path.join(ROOT, "profiles", f"step3d_{workload}.md")
     try:
         with open(path) as fh:
             for line in fh:

@@ -85,11 +85,11 @@ __device__ __forceinline__ double w_rt(int j) {
     return j == 0 ? 1.0 / 3.0 : (j <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
 }
 
-// Reciprocal of the binary32 collision (rho and tau near 1: the hardware
-// approximation, 2 ulp, is far inside the form's tolerance); exact division
-// in binary64.
+// Reciprocal of the collision, correctly rounded: an approximate reciprocal
+// biases omega = 1 / tau the same way at every node and step, which shows up
+// as a small systematic viscosity error in the force.
 __device__ __forceinline__ float fast_rcp(float x) {
-    return __fdividef(1.0f, x);
+    return 1.0f / x;
 }
 __device__ __forceinline__ double fast_rcp(double x) {
     return 1.0 / x;
@@ -104,12 +104,19 @@ template <class A, bool kShifted, bool kSmag>
 __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int forced,
                                          A& out_ux, A& out_uy, A& out_uz) {
     if constexpr (kShifted) {
-        A drho = 0;
-#pragma unroll
-        for (int i = 0; i < d3::Q; ++i) drho += f[i];
-        const A jx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[11] - f[12] + f[13] - f[14];
-        const A jy = f[3] - f[4] + f[7] - f[8] - f[9] + f[10] + f[15] - f[16] + f[17] - f[18];
-        const A jz = f[5] - f[6] + f[11] - f[12] - f[13] + f[14] + f[15] - f[16] - f[17] + f[18];
+        // Pairwise sums: the density deviation (about 1e-3) is a sum of
+        // terms about ten times larger, so a balanced tree keeps more digits
+        // than a running sum.
+        const A p1 = f[1] + f[2], p3 = f[3] + f[4], p5 = f[5] + f[6], p7 = f[7] + f[8],
+                p9 = f[9] + f[10], p11 = f[11] + f[12], p13 = f[13] + f[14], p15 = f[15] + f[16],
+                p17 = f[17] + f[18];
+        const A drho = f[0] + (((p1 + p3) + (p5 + p7)) + ((p9 + p11) + ((p13 + p15) + p17)));
+        const A m1 = f[1] - f[2], m3 = f[3] - f[4], m5 = f[5] - f[6], m7 = f[7] - f[8],
+                m9 = f[9] - f[10], m11 = f[11] - f[12], m13 = f[13] - f[14], m15 = f[15] - f[16],
+                m17 = f[17] - f[18];
+        const A jx = (m1 + m7) + (m9 + (m11 + m13));
+        const A jy = (m3 + m7) + ((m15 + m17) - m9);
+        const A jz = (m5 + m11) + ((m15 - m13) - m17);
         const A rho = A(1) + drho;
         const A inv = fast_rcp(rho);
         const A ux = (jx + A(0.5) * p.fx) * inv;
