@@ -200,6 +200,38 @@ ORR_API orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream);
 /* Kernels launched by this handle since creation (step, force, moments, ...). */
 ORR_API orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches);
 
+/* Inputs of orr_lbm3d_force_static: device pointers the caller owns. */
+typedef struct orr_force_links {
+    uint64_t nx, ny, nz;        /* lattice dimensions */
+    int32_t storage;            /* ORR_STORAGE_* of `populations` */
+    int32_t device;             /* CUDA device the pointers belong to */
+    const void* populations;    /* 19 * nx*ny*nz values, layout of orr_lbm3d_populations,
+                                   stored as the storage form holds them (f - w for the
+                                   binary32 forms, FP16S scaled by 2^15, f for binary64) */
+    const uint32_t* link_cell;  /* per link: node index x + nx (y + ny z) */
+    const uint32_t* link_dir;   /* per link: direction j (its source x - c_j is solid) */
+    const double* link_q;       /* per link: wall fraction q */
+    uint64_t links;             /* number of links, at most ORR_FORCE_STATIC_MAX_LINKS */
+    void* stream;               /* cudaStream_t to run on; NULL is the legacy default stream */
+} orr_force_links;
+
+#define ORR_FORCE_STATIC_MAX_LINKS 8388608u
+
+/* No counterpart in the reference: an allocation-free twin of
+ * orr_lbm3d_force for callers that may not allocate device memory (a host
+ * application whose device memory belongs to another allocator or pool, a
+ * real-time loop that must not call into the allocator, a process that has
+ * reserved all device memory up front).  It computes the same momentum-
+ * exchange force and moment over links the caller already holds on the
+ * device, using as scratch a fixed 192 KiB array compiled into the library
+ * (held by every GPU that loads the library until exit), so it calls no
+ * cudaMalloc or cudaFree.  More than ORR_FORCE_STATIC_MAX_LINKS links are
+ * refused with ORR_ERR_INVALID.  The first call on a device looks up the
+ * array's device address (make it before any stream capture).  All calls
+ * share the array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller.  Blocks until the result is in force_moment. */
+ORR_API orr_status orr_lbm3d_force_static(const orr_force_links* args, double force_moment[6]);
+
 /* ---- D2Q9 -------------------------------------------------------------- */
 
 /* validate (lbm2d.h:85-86; lbm2d_common.cpp:31-77) plus the binary32 checks

@@ -62,6 +62,18 @@ class CLbm2DConfig(ctypes.Structure):
     ]
 
 
+class CForceLinks(ctypes.Structure):
+    """orr_force_links: device inputs of orr_lbm3d_force_static."""
+    _fields_ = [("nx", ctypes.c_uint64), ("ny", ctypes.c_uint64), ("nz", ctypes.c_uint64),
+                ("storage", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("populations", ctypes.c_void_p), ("link_cell", ctypes.c_void_p),
+                ("link_dir", ctypes.c_void_p), ("link_q", ctypes.c_void_p),
+                ("links", ctypes.c_uint64), ("stream", ctypes.c_void_p)]
+
+
+ORR_FORCE_STATIC_MAX_LINKS = 8388608
+
+
 class CSolverOptions(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int32), ("allow_high_mach", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("block_x", ctypes.c_int32)]

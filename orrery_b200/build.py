@@ -35,6 +35,7 @@ SOURCES = {
     "kernels_binary64.cu": ["-fmad=false"],
     "solver3d.cu": [],
     "solver2d.cu": [],
+    "force_static.cu": [],
 }
 
 
