@@ -62,7 +62,7 @@ enum { ORR_OUTLET_CONVECTIVE = 0, ORR_OUTLET_EXTRAPOLATION = 1 };
 enum { ORR_SOLID_HALFWAY = 0, ORR_SOLID_INTERPOLATED = 1 };
 /* Population storage on the device.  All forms collide in binary32 except
  * F64, which computes in binary64 throughout (the FP64 device oracle).
- * F32 holds f - w; F16 holds (f - w) scaled by 2^15 (FP16S); BF16 holds f - w. */
+ * F32, F16 and BF16 hold f - w. */
 enum { ORR_STORAGE_F32 = 0, ORR_STORAGE_F16 = 1, ORR_STORAGE_BF16 = 2, ORR_STORAGE_F64 = 3 };
 
 /* Wall (lbm2d.h:53-56). velocity_x is the tangential speed of a no-slip wall. */
@@ -207,7 +207,7 @@ typedef struct orr_force_links {
     int32_t device;             /* CUDA device the pointers belong to */
     const void* populations;    /* 19 * nx*ny*nz values, layout of orr_lbm3d_populations,
                                    stored as the storage form holds them (f - w for the
-                                   binary32 forms, FP16S scaled by 2^15, f for binary64) */
+                                   binary32, binary16 and bfloat16 forms, f for binary64) */
     const uint32_t* link_cell;  /* per link: node index x + nx (y + ny z) */
     const uint32_t* link_dir;   /* per link: direction j (its source x - c_j is solid) */
     const double* link_q;       /* per link: wall fraction q */

@@ -85,14 +85,27 @@ __device__ __forceinline__ double w_rt(int j) {
     return j == 0 ? 1.0 / 3.0 : (j <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
 }
 
-// Reciprocal of the collision, correctly rounded: an approximate reciprocal
-// biases omega = 1 / tau the same way at every node and step, which shows up
-// as a small systematic viscosity error in the force.
+// Reciprocal and square root of the binary32 collision: the hardware
+// approximations refined by one Newton-Raphson step, r' = r + r (1 - x r)
+// and s' = s + (y / 2)(x - s^2) with s = x y, y ~ 1/sqrt(x), which lands
+// within about half an ulp of the exact value for the positive, normal
+// arguments the collision forms (rho, tau, strain sums); a zero square-root
+// argument gives zero.  Binary64 keeps exact division and sqrt (it follows
+// the reference CPU solver's rounding).
 __device__ __forceinline__ float fast_rcp(float x) {
-    return 1.0f / x;
+    const float r = __fdividef(1.0f, x);
+    return fmaf(r, fmaf(-x, r, 1.0f), r);
 }
 __device__ __forceinline__ double fast_rcp(double x) {
     return 1.0 / x;
+}
+__device__ __forceinline__ float fast_sqrt(float x) {
+    const float y = rsqrtf(x);
+    const float s = x * y;
+    return x == 0.0f ? 0.0f : fmaf(0.5f * y, fmaf(-s, s, x), s);
+}
+__device__ __forceinline__ double fast_sqrt(double x) {
+    return sqrt(x);
 }
 
 // ---------------------------------------------------------------- collide --
@@ -129,13 +142,14 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
             // equilibrium sum c_a c_b f_eq = rho (c_s^2 delta_ab + u_a u_b)
             // exactly, and sum c c w = c_s^2 delta, so on shifted values
             // Pi_neq = sum c c f_s - drho c_s^2 delta - rho u u; f_eq is then
-            // formed on the fly in the relaxation below.
-            const A sxx = f[1] + f[2] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] + f[14];
-            const A syy = f[3] + f[4] + f[7] + f[8] + f[9] + f[10] + f[15] + f[16] + f[17] + f[18];
-            const A szz = f[5] + f[6] + f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
-            const A sxy = f[7] + f[8] - f[9] - f[10];
-            const A sxz = f[11] + f[12] - f[13] - f[14];
-            const A syz = f[15] + f[16] - f[17] - f[18];
+            // formed on the fly in the relaxation below.  The second moments
+            // reuse the opposite-pair sums of the density.
+            const A sxx = (p1 + p7) + (p9 + (p11 + p13));
+            const A syy = (p3 + p7) + (p9 + (p15 + p17));
+            const A szz = (p5 + p11) + (p13 + (p15 + p17));
+            const A sxy = p7 - p9;
+            const A sxz = p11 - p13;
+            const A syz = p15 - p17;
             const A iso = drho * A(1.0 / 3.0);
             const A pxx = sxx - iso - rho * ux * ux;
             const A pyy = syy - iso - rho * uy * uy;
@@ -144,8 +158,8 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
             const A pxz = sxz - rho * ux * uz;
             const A pyz = syz - rho * uy * uz;
             const A strain =
-                sqrt(pxx * pxx + pyy * pyy + pzz * pzz + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
-            tau = A(0.5) * (tau + sqrt(tau * tau + A(kSmagFactor) * p.smag_c2 * strain * inv));
+                fast_sqrt(pxx * pxx + pyy * pyy + pzz * pzz + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+            tau = A(0.5) * (tau + fast_sqrt(tau * tau + A(kSmagFactor) * p.smag_c2 * strain * inv));
         }
         const A omega = fast_rcp(tau);
         // Relaxation towards f_eq,i - w_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2
@@ -558,10 +572,10 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
     using A = typename Storage<S>::A;
     using T = Storage<S>;
     const uint64_t cells = g.cells;
-    const uint32_t row = blockIdx.x / g.tiles_x;
-    const uint32_t x = (blockIdx.x - row * g.tiles_x) * blockDim.x + threadIdx.x;
-    const uint32_t y = row % g.ny;
-    const uint32_t z = row / g.ny;
+    // Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B).
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y;
+    const uint32_t z = blockIdx.z;
     if (x >= g.nx) {
         return;
     }
@@ -577,18 +591,38 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
     A f[d3::Q];
     if (cls == kBulk) {
         const int64_t nx = g.nx, plane = g.plane;
-        const bool xlo = x == 0u, xhi = x + 1u == g.nx;
-        // x = -1 wraps to nx - 1 (periodic) or is an inlet unknown whose read
-        // is discarded; x = nx wraps to 0 or copies the outlet node x = nx - 1.
-        const int64_t shift_lo = g.x_mode == ORR_X_PERIODIC ? nx : 0;
-        const int64_t shift_hi = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
 #pragma unroll
         for (int i = 0; i < d3::Q; ++i) {
-            int64_t source = static_cast<int64_t>(here) -
-                             (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-            if (d3::cx(i) > 0 && xlo) source += shift_lo;
-            if (d3::cx(i) < 0 && xhi) source += shift_hi;
+            const int64_t source = static_cast<int64_t>(here) -
+                                   (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
             f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+        }
+        // The x-edge lanes of an interior row (two per row) read their c_x != 0
+        // sources again: x = -1 wraps to nx - 1 (periodic) or is an inlet
+        // unknown, rebuilt below; x = nx wraps to 0 or copies the outlet node
+        // x = nx - 1.  The first reads stayed inside the lattice (neighbouring
+        // rows) and are discarded.
+        const bool xlo = x == 0u, xhi = x + 1u == g.nx;
+        if (xlo && g.x_mode == ORR_X_PERIODIC) {
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                if (d3::cx(i) > 0) {
+                    const int64_t source = static_cast<int64_t>(here) + nx -
+                                           (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                    f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+                }
+            }
+        }
+        if (xhi) {
+            const int64_t shift = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                if (d3::cx(i) < 0) {
+                    const int64_t source = static_cast<int64_t>(here) + shift -
+                                           (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                    f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+                }
+            }
         }
         if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
             // Convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).

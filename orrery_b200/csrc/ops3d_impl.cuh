@@ -16,14 +16,14 @@ template <class S> struct Launch3D {
                             const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s) {
         Geom3D gg = g;
         gg.tiles_x = (g.nx + block - 1) / block;
-        const uint64_t blocks = static_cast<uint64_t>(g.ny) * g.nz * gg.tiles_x;
+        const dim3 grid(gg.tiles_x, g.ny, g.nz);
         const auto& p = *static_cast<const Phys3D<A>*>(phys);
         if (smag) {
-            step3d_kernel<S, true><<<static_cast<unsigned>(blocks), block, 0, s>>>(
-                gg, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
+            step3d_kernel<S, true><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
+                                                          static_cast<S*>(dst), b);
         } else {
-            step3d_kernel<S, false><<<static_cast<unsigned>(blocks), block, 0, s>>>(
-                gg, p, static_cast<const S*>(src), static_cast<S*>(dst), b);
+            step3d_kernel<S, false><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
+                                                           static_cast<S*>(dst), b);
         }
         return cudaGetLastError();
     }

@@ -641,7 +641,7 @@ orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
                 } else if (h->storage == ORR_STORAGE_F16) {
                     __half x;
                     std::memcpy(&x, raw.data() + 2 * k, 2);
-                    v = static_cast<double>(__half2float(x)) / 32768.0;
+                    v = static_cast<double>(__half2float(x));
                 } else {
                     __nv_bfloat16 x;
                     std::memcpy(&x, raw.data() + 2 * k, 2);
