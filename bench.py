@@ -160,6 +160,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
+    ap.add_argument("--stages", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1000)
     args = ap.parse_args(argv)
@@ -187,7 +189,8 @@ def main(argv=None) -> int:
 
     w = W.sphere3d(seed=1 + rank)
     solver = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank,
-                               block_x=args.block)
+                               block_x=args.block, kernel=args.kernel, stages=args.stages)
+    kinfo = solver.kernel_info()
     solver.initialize(w.rho, w.ux, w.uy, w.uz)
     stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local_rank))
     solver.step(max(args.warmup, 3))
@@ -241,7 +244,8 @@ def main(argv=None) -> int:
         import numpy as np
         barrier()
         t0 = time.perf_counter()
-        s2 = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank, block_x=args.block)
+        s2 = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank, block_x=args.block,
+                               kernel=args.kernel, stages=args.stages)
         s2.initialize(w.rho, w.ux, w.uy, w.uz)
         samples = 0
         for _ in range(args.e2e_steps // 10):
@@ -283,7 +287,7 @@ def main(argv=None) -> int:
             "config": {"workload": w.name, "nodes": w.cells, "storage": args.storage,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": f"inputs larger than L2: {w.cells * 19 * {'f32': 4, 'f16': 2, 'bf16': 2, 'f64': 8}[args.storage] / 1e6:.0f} MB per population buffer",
-                       "seed": 1},
+                       "seed": 1, "kernel": kinfo},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": traffic,
                          "peak_source": peak_kind,

@@ -109,7 +109,17 @@ typedef struct orr_solver_options {
     int32_t allow_high_mach;  /* 1: skip the lattice Mach guard (opt-in; off by default) */
     int32_t device;           /* CUDA device ordinal */
     int32_t block_x;          /* threads per block of the step kernel; 0 = tuned default */
+    int32_t kernel;           /* ORR_KERNEL_*: the D3Q19 step kernel (0 = automatic) */
+    int32_t stages;           /* pipeline stages of ORR_KERNEL_STAGED; 0 = tuned default */
 } orr_solver_options;
+
+/* D3Q19 step kernels.  ROWS: one block per row tile, every population read
+ * straight from global memory.  STAGED: a persistent kernel whose interior
+ * row tiles receive their 19 source row segments through a shared-memory
+ * pipeline of bulk asynchronous copies (lattices whose nx is a multiple of 16;
+ * other rows take the per-node path).  AUTO picks STAGED when the lattice
+ * qualifies.  Both give the same result bit for bit. */
+enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2 };
 
 typedef struct orr_lbm3d orr_lbm3d;
 typedef struct orr_lbm2d orr_lbm2d;
@@ -143,6 +153,25 @@ ORR_API orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_
                                     orr_lbm3d** out);
 ORR_API void orr_lbm3d_destroy(orr_lbm3d* solver);
 ORR_API const char* orr_lbm3d_last_error(const orr_lbm3d* solver);
+
+/* The step kernel a solver runs and its launch shape (no counterpart in the
+ * reference, whose GL backend has one dispatch shape): kernel ORR_KERNEL_ROWS
+ * or ORR_KERNEL_STAGED, threads per CTA, pipeline stages and shared bytes
+ * per CTA (staged), CTAs per launch, resident CTAs per SM (staged),
+ * registers per thread, and the staged / per-node work items. */
+typedef struct orr_kernel_info {
+    int32_t kernel;
+    uint32_t block;
+    uint32_t stages;
+    uint32_t grid;
+    int32_t ctas_per_sm;
+    int32_t registers;
+    uint32_t shared_bytes;
+    uint32_t reserved;
+    uint64_t staged_items;
+    uint64_t direct_items;
+} orr_kernel_info;
+ORR_API orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info);
 
 /* Lbm3DSolver::initialize (lbm3d.h:211): equilibrium of the given fields at
  * every fluid node (solids at rest), step count reset, inlet velocity back to
@@ -199,6 +228,68 @@ ORR_API orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* flui
 ORR_API orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream);
 /* Kernels launched by this handle since creation (step, force, moments, ...). */
 ORR_API orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches);
+
+/* ---- D3Q19 batches ------------------------------------------------------ */
+
+/* A batch advances several D3Q19 solvers together.  The reference has no
+ * counterpart: it steps one lattice per solver (Lbm3DSolver::step,
+ * lbm3d.h:213), and a drag table or sweep runs its lattices one after
+ * another.  Members are ordinary solver handles created with
+ * orr_lbm3d_create; they keep every read-back entry point (force,
+ * macroscopic, populations, mass), while orr_lbm3d_step is refused for a
+ * member.  Members share the device, the storage form and the collision
+ * model (Smagorinsky on or off); their sizes, boundaries and parameters may
+ * all differ.  A batch step gives every member exactly the populations its
+ * own steps would give (bit for bit), whatever the schedule and the mix.
+ * Not thread-safe; one batch per thread. */
+typedef struct orr_batch3d orr_batch3d;
+
+/* How a batch step runs.  kernel ORR_KERNEL_STAGED: one launch of the
+ * persistent staged kernel over every member's row tiles (block 128 or 256,
+ * stages 0 = tuned default); ORR_KERNEL_ROWS: one row-tile launch per member
+ * (block 32..256).  Steps run as CUDA graphs.  grid and ms_per_step are
+ * outputs (CTAs of the staged launch; the time per batch step a tuning trial
+ * measured). */
+typedef struct orr_batch_schedule {
+    int32_t kernel;
+    uint32_t block;
+    uint32_t stages;
+    uint32_t grid;
+    double ms_per_step;
+} orr_batch_schedule;
+
+ORR_API orr_status orr_batch3d_create(int32_t device, orr_batch3d** out);
+/* Destroys the batch; its members become ordinary solvers again. */
+ORR_API void orr_batch3d_destroy(orr_batch3d* batch);
+ORR_API const char* orr_batch3d_last_error(const orr_batch3d* batch);
+ORR_API orr_status orr_batch3d_add(orr_batch3d* batch, orr_lbm3d* solver);
+ORR_API orr_status orr_batch3d_remove(orr_batch3d* batch, orr_lbm3d* solver);
+/* Members and their total nodes. */
+ORR_API orr_status orr_batch3d_size(const orr_batch3d* batch, uint32_t* members, uint64_t* cells);
+ORR_API orr_status orr_batch3d_set_schedule(orr_batch3d* batch, const orr_batch_schedule* schedule);
+ORR_API orr_status orr_batch3d_schedule(const orr_batch3d* batch, orr_batch_schedule* schedule);
+/* `count` steps of every member (asynchronous on the batch stream). */
+ORR_API orr_status orr_batch3d_step(orr_batch3d* batch, uint64_t count);
+/* `count` steps of every member with the momentum-exchange force and moment
+ * summed after every `sample_every` steps (even, dividing count) - the
+ * reference adapter's sampling (lbm_aero_solver3d.cpp:385-441).  `sums`
+ * (6 doubles per member, in the order members were added; may be NULL)
+ * receives the sums over the samples, added in a fixed order. */
+ORR_API orr_status orr_batch3d_step_sampled(orr_batch3d* batch, uint64_t count, uint32_t sample_every,
+                                            double* sums);
+/* Force and moment (about the lattice origin) of every member now, 6 doubles
+ * per member, summed in a fixed order (after an even number of batch steps). */
+ORR_API orr_status orr_batch3d_forces(orr_batch3d* batch, double* force_moment);
+/* Autotuner: times every candidate schedule on the batch itself for
+ * `graphs_per_trial` graphs of 16 steps (after one untimed graph) and keeps
+ * the fastest.  The trial steps are real steps of every member.  The
+ * candidates' timings go to `trials` (up to `capacity`), their number to
+ * `count`. */
+ORR_API orr_status orr_batch3d_tune(orr_batch3d* batch, uint32_t graphs_per_trial,
+                                    orr_batch_schedule* trials, uint32_t capacity, uint32_t* count);
+ORR_API orr_status orr_batch3d_synchronize(orr_batch3d* batch);
+ORR_API orr_status orr_batch3d_stream(const orr_batch3d* batch, void** stream);
+ORR_API orr_status orr_batch3d_launch_count(const orr_batch3d* batch, uint64_t* launches);
 
 /* Inputs of orr_lbm3d_force_static: device pointers the caller owns. */
 typedef struct orr_force_links {

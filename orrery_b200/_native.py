@@ -51,6 +51,7 @@ SIGNATURES = {
     "orr_lbm3d_node_counts": (_st, [_vp, _u64p, _u64p]),
     "orr_lbm3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
     "orr_lbm3d_launch_count": (_st, [_vp, _u64p]),
+    "orr_lbm3d_kernel_info": (_st, [_vp, ctypes.POINTER(abi.CKernelInfo)]),
     "orr_lbm3d_force_static": (_st, [ctypes.POINTER(abi.CForceLinks), _dp]),
     "orr_lbm2d_validate": (_st, [_c2, _u8p, _opt, ctypes.c_char_p, ctypes.c_size_t]),
     "orr_lbm2d_create": (_st, [_c2, _u8p, _opt, ctypes.POINTER(_vp)]),
@@ -67,6 +68,21 @@ SIGNATURES = {
     "orr_lbm2d_links": (_st, [_vp, _u32p, _u32p]),
     "orr_lbm2d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
     "orr_lbm2d_launch_count": (_st, [_vp, _u64p]),
+    "orr_batch3d_create": (_st, [ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "orr_batch3d_destroy": (None, [_vp]),
+    "orr_batch3d_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_batch3d_add": (_st, [_vp, _vp]),
+    "orr_batch3d_remove": (_st, [_vp, _vp]),
+    "orr_batch3d_size": (_st, [_vp, _u32p, _u64p]),
+    "orr_batch3d_set_schedule": (_st, [_vp, ctypes.POINTER(abi.CBatchSchedule)]),
+    "orr_batch3d_schedule": (_st, [_vp, ctypes.POINTER(abi.CBatchSchedule)]),
+    "orr_batch3d_step": (_st, [_vp, ctypes.c_uint64]),
+    "orr_batch3d_step_sampled": (_st, [_vp, ctypes.c_uint64, ctypes.c_uint32, _dp]),
+    "orr_batch3d_forces": (_st, [_vp, _dp]),
+    "orr_batch3d_tune": (_st, [_vp, ctypes.c_uint32, ctypes.POINTER(abi.CBatchSchedule), ctypes.c_uint32, _u32p]),
+    "orr_batch3d_synchronize": (_st, [_vp]),
+    "orr_batch3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
+    "orr_batch3d_launch_count": (_st, [_vp, _u64p]),
 }
 
 

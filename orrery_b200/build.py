@@ -31,11 +31,14 @@ COMMON = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 SOURCES = {
     "common.cpp": [],
     "plan.cpp": [],
-    "kernels_binary32.cu": [],
-    "kernels_binary64.cu": ["-fmad=false"],
+    "kernels_f32.cu": [],
+    "kernels_f16.cu": [],
+    "kernels_bf16.cu": [],
+    "kernels_f64.cu": ["-fmad=false"],
     "solver3d.cu": [],
     "solver2d.cu": [],
     "force_static.cu": [],
+    "batch3d.cu": [],
 }
 
 

@@ -546,6 +546,61 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
     }
 }
 
+// Fix-ups of a bulk node after its 19 plain pulls f_i = f*_i(x - c_i).  The
+// x-edge lanes of an interior row (two per row) read their c_x != 0 sources
+// again: x = -1 wraps to nx - 1 (periodic) or is an inlet unknown, rebuilt by
+// the inlet; x = nx wraps to 0 or copies the outlet node x = nx - 1.  The
+// first reads stayed inside the lattice (neighbouring rows) and are
+// discarded.
+template <class S>
+__device__ __forceinline__ void bulk_edges3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                            const S* __restrict__ src, const StepBuffers3D& b,
+                                            uint32_t x, uint32_t y, uint32_t z, uint64_t here,
+                                            typename Storage<S>::A (&f)[d3::Q]) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint64_t cells = g.cells;
+    const int64_t nx = g.nx, plane = g.plane;
+    const bool xlo = x == 0u, xhi = x + 1u == g.nx;
+    if (xlo && g.x_mode == ORR_X_PERIODIC) {
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            if (d3::cx(i) > 0) {
+                const int64_t source = static_cast<int64_t>(here) + nx -
+                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+            }
+        }
+    }
+    if (xhi) {
+        const int64_t shift = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            if (d3::cx(i) < 0) {
+                const int64_t source = static_cast<int64_t>(here) + shift -
+                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+            }
+        }
+    }
+    if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
+        // Convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).
+        A* hist = static_cast<A*>(b.hist);
+        const A u = p.outlet_speed;
+        const uint64_t at = static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
+        const uint64_t face = static_cast<uint64_t>(g.ny) * g.nz;
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            if (d3::cx(i) < 0) {
+                const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
+                const A v = (hist[k] + u * f[i]) / (A(1) + u);
+                hist[k] = v;
+                f[i] = v;
+            }
+        }
+    }
+}
+
 // One fused step src -> dst: one thread per node, one block per tile of a
 // row (blockDim.x nodes along x), every row of the lattice.  Every lane of a
 // row stores all 19 populations of its node in the same step, so each
@@ -563,22 +618,14 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
 //               gather, whose side rules are uniform along the row;
 //   boundary    a node with a solid source (bounce-back / interpolated wall):
 //               the general gather with the plan's per-node direction mask.
-template <class S> constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 4;
-
 template <class S, bool kSmag>
-__global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
-                                                        const S* __restrict__ src,
-                                                        S* __restrict__ dst, StepBuffers3D b) {
+__device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                           const S* __restrict__ src, S* __restrict__ dst,
+                                           const StepBuffers3D& b, uint32_t x, uint32_t y,
+                                           uint32_t z) {
     using A = typename Storage<S>::A;
     using T = Storage<S>;
     const uint64_t cells = g.cells;
-    // Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B).
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t y = blockIdx.y;
-    const uint32_t z = blockIdx.z;
-    if (x >= g.nx) {
-        return;
-    }
     const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
     const uint8_t cls = b.cls[here];
     if (cls == kSolid) {
@@ -597,49 +644,7 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
                                    (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
             f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
         }
-        // The x-edge lanes of an interior row (two per row) read their c_x != 0
-        // sources again: x = -1 wraps to nx - 1 (periodic) or is an inlet
-        // unknown, rebuilt below; x = nx wraps to 0 or copies the outlet node
-        // x = nx - 1.  The first reads stayed inside the lattice (neighbouring
-        // rows) and are discarded.
-        const bool xlo = x == 0u, xhi = x + 1u == g.nx;
-        if (xlo && g.x_mode == ORR_X_PERIODIC) {
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                if (d3::cx(i) > 0) {
-                    const int64_t source = static_cast<int64_t>(here) + nx -
-                                           (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-                    f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
-                }
-            }
-        }
-        if (xhi) {
-            const int64_t shift = g.x_mode == ORR_X_PERIODIC ? -nx : -1;
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                if (d3::cx(i) < 0) {
-                    const int64_t source = static_cast<int64_t>(here) + shift -
-                                           (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-                    f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
-                }
-            }
-        }
-        if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
-            // Convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).
-            A* hist = static_cast<A*>(b.hist);
-            const A u = p.outlet_speed;
-            const uint64_t at = static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
-            const uint64_t face = static_cast<uint64_t>(g.ny) * g.nz;
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                if (d3::cx(i) < 0) {
-                    const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
-                    const A v = (hist[k] + u * f[i]) / (A(1) + u);
-                    hist[k] = v;
-                    f[i] = v;
-                }
-            }
-        }
+        bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
     } else {
         const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
         const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
@@ -651,6 +656,21 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
         inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
     }
     finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
+}
+
+template <class S> constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 4;
+
+// Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B)
+// of row (y, z).
+template <class S, bool kSmag>
+__global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
+                                                        const S* __restrict__ src,
+                                                        S* __restrict__ dst, StepBuffers3D b) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= g.nx) {
+        return;
+    }
+    step_node3<S, kSmag>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------ init / misc --
@@ -835,6 +855,141 @@ __global__ void force3d_kernel(Geom3D g, const S* __restrict__ f, const uint32_t
         acc[5] += rx * fy - ry * fx;
     }
     block_reduce_add<6>(acc, out);
+}
+
+// ------------------------------------------------------ batched forces --
+
+// One boundary link's momentum exchange and its moment about the origin,
+// added to acc (the per-link arithmetic of force3d_kernel).
+template <class S>
+__device__ __forceinline__ void add_link3(uint64_t nx, uint64_t plane, uint64_t cells,
+                                          const S* __restrict__ f, uint64_t h, int j, double q,
+                                          double (&acc)[6]) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const int o = opposite_rt(j);
+    int jx, jy, jz;
+    c_rt(j, jx, jy, jz);
+    const A qa = static_cast<A>(q);
+    const A leaving = T::load(f + static_cast<uint64_t>(o) * cells + h);
+    A back;
+    if (q == 0.5) {
+        back = leaving;
+    } else if (q < 0.5) {
+        const uint64_t farther = static_cast<uint64_t>(static_cast<int64_t>(h) + jx +
+                                                       static_cast<int64_t>(nx) * jy +
+                                                       static_cast<int64_t>(plane) * jz);
+        back = A(2) * qa * leaving + (A(1) - A(2) * qa) * T::load(f + static_cast<uint64_t>(o) * cells + farther);
+    } else {
+        back = (leaving + (A(2) * qa - A(1)) * T::load(f + static_cast<uint64_t>(j) * cells + h)) / (A(2) * qa);
+    }
+    double ex = static_cast<double>(leaving) + static_cast<double>(back);
+    if (T::kShifted) {
+        ex += 2.0 * w_rt(o);
+    }
+    const double fx = -jx * ex, fy = -jy * ex, fz = -jz * ex;
+    const uint64_t z = h / plane, rest = h - z * plane;
+    const uint64_t y = rest / nx, x = rest - y * nx;
+    const double rx = static_cast<double>(x) - q * jx;
+    const double ry = static_cast<double>(y) - q * jy;
+    const double rz = static_cast<double>(z) - q * jz;
+    acc[0] += fx;
+    acc[1] += fy;
+    acc[2] += fz;
+    acc[3] += ry * fz - rz * fy;
+    acc[4] += rz * fx - rx * fz;
+    acc[5] += rx * fy - ry * fx;
+}
+
+// The links of one lattice for the batched force (device table entry).
+struct ForceJob {
+    const void* f;            // populations the force reads (the current buffer)
+    const uint32_t* lcell;
+    const uint32_t* ldir;
+    const double* lq;
+    uint64_t links;
+    uint64_t chunk_begin;     // first global chunk of this lattice
+    uint64_t nx, plane, cells;
+};
+
+constexpr uint32_t kForceThreads = 256;
+constexpr uint64_t kForceChunk = 2048; // links per block of pass 1
+
+// Sum of six doubles over the block in a fixed order; valid in thread 0.
+__device__ __forceinline__ void block_sum6_fixed(double (&v)[6]) {
+    __shared__ double part[6][kForceThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) part[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < static_cast<int>(kForceThreads / 32); ++w) t += part[k][w];
+            v[k] = t;
+        }
+    }
+}
+
+// Pass 1 of the batched force: block b sums global chunk b (kForceChunk
+// links of one lattice) into partial[6 b .. 6 b + 5].
+template <class S>
+__global__ void __launch_bounds__(kForceThreads) force_batch_partials(const ForceJob* __restrict__ jobs,
+                                                                      uint32_t n, double* __restrict__ partial) {
+    const uint64_t chunk = blockIdx.x;
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].chunk_begin <= chunk) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    const ForceJob& J = jobs[lo];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const uint64_t begin = (chunk - J.chunk_begin) * kForceChunk;
+    const uint64_t end = begin + kForceChunk < J.links ? begin + kForceChunk : J.links;
+    const S* f = static_cast<const S*>(J.f);
+    for (uint64_t k = begin + threadIdx.x; k < end; k += kForceThreads) {
+        add_link3<S>(J.nx, J.plane, J.cells, f, J.lcell[k], static_cast<int>(J.ldir[k]), J.lq[k], acc);
+    }
+    block_sum6_fixed(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int v = 0; v < 6; ++v) partial[chunk * 6 + v] = acc[v];
+    }
+}
+
+// Pass 2: lattice blockIdx.x adds its chunks' partial sums in chunk order
+// and adds (accumulate) or writes the six totals to out[6 l ..].
+// (A template, instantiated per storage unit like the other kernels.)
+template <class S>
+__global__ void __launch_bounds__(kForceThreads) force_batch_totals(const ForceJob* __restrict__ jobs,
+                                                                    const double* __restrict__ partial,
+                                                                    double* __restrict__ out, int accumulate) {
+    const ForceJob& J = jobs[blockIdx.x];
+    const uint64_t chunks = (J.links + kForceChunk - 1) / kForceChunk;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint64_t c = threadIdx.x; c < chunks; c += kForceThreads) {
+#pragma unroll
+        for (int v = 0; v < 6; ++v) acc[v] += partial[(J.chunk_begin + c) * 6 + v];
+    }
+    block_sum6_fixed(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+            out[blockIdx.x * 6 + v] = accumulate ? out[blockIdx.x * 6 + v] + acc[v] : acc[v];
+        }
+    }
 }
 
 // Sum of the stored populations over fluid nodes in binary64 (the shifted

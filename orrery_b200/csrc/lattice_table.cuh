@@ -1,0 +1,87 @@
+// Host side of the persistent step: lattice-table entries, item numbering
+// and the launch shape.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "ops3d.h"
+#include "staged3d.cuh"
+
+namespace orr {
+
+// A lattice's interior rows can be staged: rows of a multiple of 16 nodes
+// (every row segment and class row starts on a 16-byte boundary for all
+// storage forms) and at least one interior row.
+inline bool stageable(const Geom3D& g) {
+    return g.nx % 16 == 0 && g.ny >= 3 && g.nz >= 3;
+}
+
+struct ItemCounts {
+    uint64_t staged = 0;
+    uint64_t direct = 0;
+};
+
+// Numbers the items of lattices[0, n) for tiles of `block` nodes: sets each
+// tiles_x and the prefix offsets, returns the totals.
+template <class A> ItemCounts number_items(Lattice3D<A>* lats, std::size_t n, uint32_t block) {
+    ItemCounts c;
+    for (std::size_t k = 0; k < n; ++k) {
+        Lattice3D<A>& L = lats[k];
+        L.g.tiles_x = (L.g.nx + block - 1) / block;
+        const uint64_t tiles = L.g.tiles_x;
+        L.staged_begin = c.staged;
+        L.direct_begin = c.direct;
+        if (L.staged) {
+            c.staged += tiles * (L.g.ny - 2ull) * (L.g.nz - 2ull);
+            c.direct += tiles * (2ull * L.g.ny + 2ull * (L.g.nz - 2ull));
+        } else {
+            c.direct += tiles * L.g.ny * static_cast<uint64_t>(L.g.nz);
+        }
+    }
+    return c;
+}
+
+// Launch shape of the persistent step.
+struct StagedShape {
+    uint32_t block = 256;
+    uint32_t stages = 0;
+    uint32_t grid = 0;     // CTAs (resident CTAs per SM x SMs)
+    int per_sm = 0;
+};
+
+// Picks the stages (the most, up to 4, that keep the register-limited
+// residency, unless `stages` is given) and the grid for `block`.  A shape
+// with per_sm == 0 cannot launch.
+inline StagedShape staged_shape(const Ops3D& ops, bool smag, uint32_t block, uint32_t stages,
+                                int device) {
+    StagedShape s;
+    s.block = block;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        return s;
+    }
+    if (stages != 0) {
+        s.stages = stages;
+        s.per_sm = ops.staged_occupancy(smag, block, stages);
+    } else {
+        const int best = ops.staged_occupancy(smag, block, 1);
+        s.stages = 2;
+        s.per_sm = ops.staged_occupancy(smag, block, 2);
+        for (uint32_t k = 4; k > 2; --k) {
+            const int o = ops.staged_occupancy(smag, block, k);
+            if (o == best && o > 0) {
+                s.stages = k;
+                s.per_sm = o;
+                break;
+            }
+        }
+    }
+    s.grid = static_cast<uint32_t>(std::max(s.per_sm, 0)) * static_cast<uint32_t>(sms);
+    return s;
+}
+
+} // namespace orr

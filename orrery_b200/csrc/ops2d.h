@@ -1,5 +1,5 @@
 // Per-storage launch table of the D2Q9 kernels (instantiated next to the
-// D3Q19 ones in kernels_binary32.cu and kernels_binary64.cu).
+// D3Q19 ones in kernels_f32/f16/bf16/f64.cu).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -1,6 +1,6 @@
 // Per-storage launch table of the D3Q19 kernels.  The kernels are
-// instantiated in kernels_binary32.cu (float, FP16S, bfloat16) and
-// kernels_binary64.cu (double, built without FMA contraction); the solver
+// instantiated in kernels_f32.cu, kernels_f16.cu, kernels_bf16.cu and
+// kernels_f64.cu (double, built without FMA contraction); the solver
 // reaches them only through this table.
 #pragma once
 
@@ -34,6 +34,28 @@ struct Ops3D {
                         cudaStream_t s);
     // Registers per thread of the step kernel (for the tuner and the docs).
     int (*step_registers)(bool smag);
+    // Persistent step over a device table of n Lattice3D entries of the
+    // storage's arithmetic type (staged3d.cuh): `grid` CTAs of `block`
+    // consumer threads (128 or 256) plus a producer warp, `stages` pipeline
+    // stages, source buffer f[parity ^ flip] of every lattice.  With n == 1
+    // and `host_one` (a host copy of the entry) the entry is passed by value.
+    cudaError_t (*staged)(const void* host_one, const void* table, uint32_t n, uint64_t staged_items,
+                          uint64_t direct_items, uint32_t flip, uint32_t stages, bool smag,
+                          uint32_t block, uint32_t grid, uint32_t* status, cudaStream_t s);
+    // Resident CTAs per SM of the persistent step for (smag, block, stages),
+    // after raising the kernel's dynamic shared-memory limit; 0 if it cannot
+    // launch.
+    int (*staged_occupancy)(bool smag, uint32_t block, uint32_t stages);
+    // Dynamic shared memory of the persistent step, bytes.
+    uint32_t (*staged_smem)(uint32_t block, uint32_t stages);
+    // Registers per thread of the persistent step.
+    int (*staged_registers)(bool smag, uint32_t block);
+    // Momentum exchange of n lattices (device table of ForceJob, kernels3d.cuh)
+    // summed in a fixed order: pass 1 over `chunks` link chunks into
+    // `partial` (6 doubles per chunk), pass 2 into out[6 l ..] (added to it
+    // when `accumulate`).
+    cudaError_t (*force_batch)(const void* jobs, uint32_t n, uint64_t chunks, double* partial,
+                               double* out, bool accumulate, cudaStream_t s);
 };
 
 const Ops3D& ops3d_f32();

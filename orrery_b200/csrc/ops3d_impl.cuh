@@ -6,6 +6,7 @@
 
 #include "kernels3d.cuh"
 #include "ops3d.h"
+#include "staged3d.cuh"
 
 namespace orr {
 
@@ -83,8 +84,136 @@ template <class S> struct Launch3D {
         return e == cudaSuccess ? a.numRegs : -1;
     }
 
+    template <bool kSmag, int B, bool kSingle> static constexpr auto staged_kernel() {
+        return &step3d_staged_kernel<S, kSmag, B, kSingle>;
+    }
+
+    // One lattice (host_one non-null, n == 1) travels by value, so its fields
+    // are constant-bank operands; otherwise the kernel reads the device table.
+    template <bool kSmag, int B>
+    static void launch_staged(const Lattice3D<A>* host_one, const Lattice3D<A>* lats, uint32_t n,
+                              uint32_t staged_items, uint32_t direct_items, uint32_t flip, uint32_t stages,
+                              uint32_t grid, uint32_t smem, uint32_t* status, cudaStream_t s) {
+        if (host_one != nullptr && n == 1) {
+            staged_kernel<kSmag, B, true>()<<<grid, kStagedThreads<B>, smem, s>>>(
+                *host_one, lats, n, staged_items, direct_items, flip, stages, status);
+        } else {
+            staged_kernel<kSmag, B, false>()<<<grid, kStagedThreads<B>, smem, s>>>(
+                Lattice3D<A>{}, lats, n, staged_items, direct_items, flip, stages, status);
+        }
+    }
+
+    static cudaError_t staged(const void* host_one, const void* table, uint32_t n, uint64_t staged_items,
+                              uint64_t direct_items, uint32_t flip, uint32_t stages, bool smag,
+                              uint32_t block, uint32_t grid, uint32_t* status, cudaStream_t s) {
+        if (stages == 0 || stages > kMaxStages || grid == 0 || staged_items >= (1ull << 31) ||
+            direct_items >= (1ull << 31)) {
+            return cudaErrorInvalidValue;
+        }
+        const auto* one = static_cast<const Lattice3D<A>*>(host_one);
+        const auto* lats = static_cast<const Lattice3D<A>*>(table);
+        const uint32_t smem = staged_smem(block, stages);
+        const auto si = static_cast<uint32_t>(staged_items), di = static_cast<uint32_t>(direct_items);
+        if (block == 256) {
+            if (smag) {
+                launch_staged<true, 256>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+            } else {
+                launch_staged<false, 256>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+            }
+        } else if (block == 128) {
+            if (smag) {
+                launch_staged<true, 128>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+            } else {
+                launch_staged<false, 128>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+            }
+        } else {
+            return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+
+    static uint32_t staged_smem(uint32_t block, uint32_t stages) {
+        return block == 256 ? staged_smem_bytes<S, 256>(stages) : staged_smem_bytes<S, 128>(stages);
+    }
+
+    // The kernel's dynamic shared-memory limit is raised to the device's
+    // opt-in maximum (not to `smem`: solvers with different stage counts
+    // share the kernel).
+    template <class K> static int occupancy_of(K kernel, uint32_t threads, uint32_t smem) {
+        int device = 0, optin = 0;
+        if (cudaGetDevice(&device) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        if (static_cast<int>(smem) > optin) {
+            return 0;
+        }
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, static_cast<int>(threads), smem) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return blocks;
+    }
+
+    // Both variants (single and table) get the attribute; the occupancy is
+    // the smaller of the two.
+    template <bool kSmag, int B> static int occupancy_both(uint32_t stages) {
+        const uint32_t smem = staged_smem_bytes<S, B>(stages);
+        const int a = occupancy_of(staged_kernel<kSmag, B, true>(), kStagedThreads<B>, smem);
+        const int b = occupancy_of(staged_kernel<kSmag, B, false>(), kStagedThreads<B>, smem);
+        return a < b ? a : b;
+    }
+
+    static int staged_occupancy(bool smag, uint32_t block, uint32_t stages) {
+        if (stages == 0 || stages > kMaxStages) {
+            return 0;
+        }
+        if (block == 256) {
+            return smag ? occupancy_both<true, 256>(stages) : occupancy_both<false, 256>(stages);
+        }
+        if (block == 128) {
+            return smag ? occupancy_both<true, 128>(stages) : occupancy_both<false, 128>(stages);
+        }
+        return 0;
+    }
+
+    static int staged_registers(bool smag, uint32_t block) {
+        cudaFuncAttributes a{};
+        cudaError_t e = cudaErrorInvalidValue;
+        if (block == 256) {
+            e = smag ? cudaFuncGetAttributes(&a, staged_kernel<true, 256, true>())
+                     : cudaFuncGetAttributes(&a, staged_kernel<false, 256, true>());
+        } else if (block == 128) {
+            e = smag ? cudaFuncGetAttributes(&a, staged_kernel<true, 128, true>())
+                     : cudaFuncGetAttributes(&a, staged_kernel<false, 128, true>());
+        }
+        return e == cudaSuccess ? a.numRegs : -1;
+    }
+
+    static cudaError_t force_batch(const void* jobs, uint32_t n, uint64_t chunks, double* partial,
+                                   double* out, bool accumulate, cudaStream_t s) {
+        if (n == 0) {
+            return cudaSuccess;
+        }
+        const auto* j = static_cast<const ForceJob*>(jobs);
+        if (chunks > 0) {
+            force_batch_partials<S><<<static_cast<unsigned>(chunks), kForceThreads, 0, s>>>(j, n, partial);
+        }
+        force_batch_totals<S><<<n, kForceThreads, 0, s>>>(j, partial, out, accumulate ? 1 : 0);
+        return cudaGetLastError();
+    }
+
     static const Ops3D& table() {
-        static const Ops3D ops{&step, &init, &history, &moments, &force, &mass, &step_registers};
+        static const Ops3D ops{&step,   &init,   &history,          &moments,     &force,
+                               &mass,   &step_registers, &staged, &staged_occupancy,
+                               &staged_smem, &staged_registers, &force_batch};
         return ops;
     }
 };

@@ -439,8 +439,8 @@ std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links
         return std::nullopt;
     // Links: cell, direction, fraction.
     if (!mul(links, 16, t) || !add(total, t, total)) return std::nullopt;
-    // Force, mass and inlet buffers.
-    if (!add(total, 256, total)) return std::nullopt;
+    // Force, mass and inlet buffers; slack of the staged step; table entry.
+    if (!add(total, 256 + 4 * kPopPad * s + kClassPad + kTableBytes, total)) return std::nullopt;
     return total;
 }
 

@@ -16,6 +16,14 @@ namespace orr {
 
 inline constexpr std::size_t kMaxGridCells = std::size_t{1} << 27; // geom::max_grid_cells
 
+// Slack of the D3Q19 device arrays for the staged step: elements before and
+// after each population buffer and bytes after the class array (a staged row
+// segment may reach one tile plus its halo past either end; those values are
+// never used), and the device bytes of the solver's lattice-table entry.
+inline constexpr std::size_t kPopPad = 1024;
+inline constexpr std::size_t kClassPad = 1024;
+inline constexpr std::size_t kTableBytes = 512;
+
 // Refusal text of validate() for a D3Q19 lattice (empty when accepted):
 // problem_of (src/aero/lbm3d/lbm3d_common.cpp:74-155), the 32-bit index
 // bound and check_binary32 of make_gpu_solver (lbm3d_gpu.cpp:94-127, 492-500;
@@ -47,9 +55,10 @@ struct Plan3D {
 // lbm3d_common.cpp:176-198).
 Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* distance);
 
-// Bytes the device solver allocates for a lattice: populations twice, node
-// classes and bounce-back masks (and wall slots for the interpolated wall),
-// moments, outlet history, wall table, links and the small reduction buffers.
+// Bytes the device solver allocates for a lattice: populations twice (with
+// their slack), node classes and bounce-back masks (and wall slots for the
+// interpolated wall), moments, outlet history, wall table, links, the
+// lattice-table entry and the small reduction buffers.
 // Empty on overflow.
 std::optional<std::size_t> memory3d(const orr_lbm3d_config& c, std::size_t links,
                                     std::size_t wall_slots, int32_t storage);

@@ -1,19 +1,7 @@
 // The D3Q19 device solver behind the C ABI: the counterpart of the
 // reference's GpuLbm3D (src/aero/lbm3d/lbm3d_gpu.cpp:151-483) and
-// make_gpu_solver (:487-513), on CUDA instead of an IComputeBackend.
-//
-// Device layout (one allocation per table):
-//   populations   two buffers of 19 * cells storage values, structure of
-//                 arrays f[i * cells + x + nx (y + ny z)]; ping-pong (A-B)
-//   classes       one byte per node (solid / bulk / face / boundary)
-//   masks         per node, the directions that bounce back (solid source)
-//   slots         per node, the wall-table slot (interpolated wall only)
-//   wall table    19 fractions per slot (interpolated wall)
-//   links         cell, direction and fraction of every boundary link
-//   moments       4 planes (rho or rho - 1, ux, uy, uz) for read-back
-//   history       5 * ny * nz convective-outlet values
-//   small         inlet velocity (3), force/moment (6) and mass accumulators
-// Steps run as CUDA graphs of kGraphSteps steps, one kernel launch each.
+// make_gpu_solver (:487-513), on CUDA instead of an IComputeBackend.  The
+// handle's state and device layout are in solver3d_state.cuh.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -28,192 +16,12 @@
 #include "common.h"
 #include "kernels3d.cuh"
 #include "lattice.h"
+#include "lattice_table.cuh"
 #include "ops3d.h"
 #include "plan.h"
-
-namespace {
+#include "solver3d_state.cuh"
 
 using namespace orr;
-
-constexpr uint32_t kGraphSteps = 16; // even: a graph returns to the buffer it started on
-constexpr uint32_t kDefaultBlock = 128;
-
-template <class T> T* device_alloc(std::size_t count, const char* what) {
-    void* p = nullptr;
-    check(cudaMalloc(&p, std::max<std::size_t>(count, 1) * sizeof(T)), what);
-    return static_cast<T*>(p);
-}
-
-const Ops3D& ops_for(int32_t storage) {
-    switch (storage) {
-        case ORR_STORAGE_F16:
-            return ops3d_f16();
-        case ORR_STORAGE_BF16:
-            return ops3d_bf16();
-        case ORR_STORAGE_F64:
-            return ops3d_f64();
-        default:
-            return ops3d_f32();
-    }
-}
-
-float to_f32(double v) {
-    return static_cast<float>(v);
-}
-
-} // namespace
-
-struct orr_lbm3d {
-    Plan3D plan;
-    int32_t storage = ORR_STORAGE_F32;
-    bool allow_high_mach = false;
-    int device = 0;
-    uint32_t block = kDefaultBlock;
-    const Ops3D* ops = nullptr;
-    Geom3D g{};
-    Phys3D<float> phys32{};
-    Phys3D<double> phys64{};
-    bool smag = false;
-    std::size_t sbytes = 4;
-    std::size_t abytes = 4;
-
-    cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph = nullptr;
-
-    void* f[2] = {nullptr, nullptr};
-    int cur = 0;
-    uint8_t* cls = nullptr;
-    uint32_t* nmask = nullptr;
-    int32_t* nslot = nullptr;
-    void* wall_q = nullptr;
-    void* hist = nullptr;
-    void* moments = nullptr;
-    uint32_t* lcell = nullptr;
-    uint32_t* ldir = nullptr;
-    double* lq = nullptr;
-    void* small = nullptr;   // inlet (3 x arithmetic) at 0, accumulators at 64
-    double* host_small = nullptr; // pinned: inlet staging + results
-
-    uint64_t steps = 0;
-    uint64_t launches = 0;
-    double inlet[3] = {0.0, 0.0, 0.0};
-    std::string error;
-
-    const void* phys() const {
-        return storage == ORR_STORAGE_F64 ? static_cast<const void*>(&phys64)
-                                          : static_cast<const void*>(&phys32);
-    }
-    void* inlet_dev() const { return small; }
-    double* acc() const { return reinterpret_cast<double*>(static_cast<char*>(small) + 64); }
-
-    StepBuffers3D buffers() const {
-        StepBuffers3D b{};
-        b.cls = cls;
-        b.nmask = nmask;
-        b.nslot = nslot;
-        b.wall_q = wall_q;
-        b.hist = hist;
-        b.inlet = small;
-        return b;
-    }
-
-    ~orr_lbm3d() { release(); }
-
-    void release() noexcept {
-        if (device >= 0) {
-            cudaSetDevice(device);
-        }
-        if (graph) cudaGraphExecDestroy(graph);
-        for (void* p : {f[0], f[1], static_cast<void*>(cls), static_cast<void*>(nmask),
-                        static_cast<void*>(nslot), wall_q, hist, moments,
-                        static_cast<void*>(lcell), static_cast<void*>(ldir),
-                        static_cast<void*>(lq), small}) {
-            if (p) cudaFree(p);
-        }
-        if (host_small) cudaFreeHost(host_small);
-        if (stream) cudaStreamDestroy(stream);
-        graph = nullptr;
-        f[0] = f[1] = nullptr;
-        cls = nullptr;
-        nmask = nullptr;
-        nslot = nullptr;
-        wall_q = hist = moments = small = nullptr;
-        lcell = ldir = nullptr;
-        lq = nullptr;
-        host_small = nullptr;
-        stream = nullptr;
-    }
-
-    // Uploads the imposed inlet velocity in the arithmetic type.
-    void upload_inlet(const double v[3]) {
-        inlet[0] = v[0];
-        inlet[1] = v[1];
-        inlet[2] = v[2];
-        check(cudaStreamSynchronize(stream), "inlet upload");
-        if (storage == ORR_STORAGE_F64) {
-            std::memcpy(host_small, v, 3 * sizeof(double));
-        } else {
-            float* h = reinterpret_cast<float*>(host_small);
-            h[0] = to_f32(v[0]);
-            h[1] = to_f32(v[1]);
-            h[2] = to_f32(v[2]);
-        }
-        check(cudaMemcpyAsync(small, host_small, 3 * abytes, cudaMemcpyHostToDevice, stream),
-              "inlet upload");
-        check(cudaStreamSynchronize(stream), "inlet upload");
-    }
-
-    // One step src -> dst on `stream` (one kernel launch).
-    void launch_step(int from) {
-        check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream), "step kernel");
-        ++launches;
-    }
-
-    void build_graph() {
-        cudaGraph_t captured = nullptr;
-        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-        const uint64_t before = launches;
-        try {
-            for (uint32_t k = 0; k < kGraphSteps; ++k) {
-                launch_step(static_cast<int>(k & 1u));
-            }
-        } catch (...) {
-            cudaStreamEndCapture(stream, &captured);
-            if (captured) cudaGraphDestroy(captured);
-            launches = before;
-            throw;
-        }
-        launches = before;
-        check(cudaStreamEndCapture(stream, &captured), "graph capture");
-        const cudaError_t e = cudaGraphInstantiate(&graph, captured, 0);
-        cudaGraphDestroy(captured);
-        check(e, "graph instantiate");
-    }
-
-    void run(uint64_t count) {
-        uint64_t left = count;
-        if (left >= kGraphSteps) {
-            if (cur != 0) {
-                launch_step(cur);
-                cur = 1 - cur;
-                --left;
-            }
-            if (!graph) {
-                build_graph();
-            }
-            while (left >= kGraphSteps) {
-                check(cudaGraphLaunch(graph, stream), "graph launch");
-                launches += kGraphSteps;
-                left -= kGraphSteps;
-            }
-        }
-        for (; left > 0; --left) {
-            launch_step(cur);
-            cur = 1 - cur;
-        }
-        steps += count;
-    }
-};
 
 namespace {
 
@@ -289,6 +97,8 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
                           h->stream),
           "population copy");
     check(h->ops->history(h->g, h->f[0], h->hist, h->stream), "history kernel");
+    check(cudaMemsetAsync(h->status(), 0, sizeof(uint32_t), h->stream), "status reset");
+    ++h->epoch;
     h->launches += 2;
     h->cur = 0;
     h->steps = 0;
@@ -377,6 +187,15 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         if (o.block_x < 0 || o.block_x > 256 || (o.block_x % 32) != 0) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: block_x must be 0 or a multiple of 32 up to 256"};
         }
+        if (o.kernel < ORR_KERNEL_AUTO || o.kernel > ORR_KERNEL_STAGED) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: unknown step kernel"};
+        }
+        if (o.kernel == ORR_KERNEL_STAGED && o.block_x != 0 && o.block_x != 128 && o.block_x != 256) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step takes block_x 128 or 256"};
+        }
+        if (o.stages < 0 || o.stages > static_cast<int32_t>(kMaxStages)) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: stages must be 0 (tuned) or 1 to 8"};
+        }
         require_device(o.device);
         auto h = std::make_unique<orr_lbm3d>();
         h->device = o.device;
@@ -434,9 +253,13 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
         const std::size_t cells = p.cells;
         for (int k = 0; k < 2; ++k) {
-            check(cudaMalloc(&h->f[k], d3::Q * cells * h->sbytes), "population buffer");
+            const std::size_t bytes = (d3::Q * cells + 2 * kPopPad) * h->sbytes;
+            check(cudaMalloc(&h->fbase[k], bytes), "population buffer");
+            check(cudaMemsetAsync(h->fbase[k], 0, bytes, h->stream), "population buffer");
+            h->f[k] = static_cast<char*>(h->fbase[k]) + kPopPad * h->sbytes;
         }
-        h->cls = device_alloc<uint8_t>(cells, "node class buffer");
+        h->cls = device_alloc<uint8_t>(cells + kClassPad, "node class buffer");
+        check(cudaMemsetAsync(h->cls + cells, 0, kClassPad, h->stream), "node class buffer");
         h->nmask = device_alloc<uint32_t>(cells, "bounce-back mask buffer");
         if (!p.nslot.empty()) {
             h->nslot = device_alloc<int32_t>(cells, "wall slot buffer");
@@ -449,7 +272,9 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         h->ldir = device_alloc<uint32_t>(p.link_cell.size(), "link buffer");
         h->lq = device_alloc<double>(p.link_cell.size(), "link buffer");
         check(cudaMalloc(&h->small, 256), "small buffer");
+        check(cudaMemsetAsync(h->small, 0, 256, h->stream), "small buffer");
         check(cudaMallocHost(reinterpret_cast<void**>(&h->host_small), 256), "pinned buffer");
+        check(cudaMalloc(&h->table, kTableBytes), "lattice table");
         // Uploads.
         cudaStream_t s = h->stream;
         check(cudaMemcpyAsync(h->cls, p.cls.data(), cells, cudaMemcpyHostToDevice, s), "class upload");
@@ -481,6 +306,31 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             check(cudaMemcpyAsync(h->ldir, p.link_dir.data(), n * 4, cudaMemcpyHostToDevice, s), "link upload");
             check(cudaMemcpyAsync(h->lq, p.link_q.data(), n * 8, cudaMemcpyHostToDevice, s), "link upload");
         }
+        // Step kernel: the persistent staged step when asked for, or
+        // automatically when the lattice's rows can be staged.
+        const bool want = o.kernel == ORR_KERNEL_STAGED ||
+                          (o.kernel == ORR_KERNEL_AUTO && stageable(g) &&
+                           (o.block_x == 0 || o.block_x == 128 || o.block_x == 256));
+        if (want) {
+            const uint32_t sblock = o.block_x == 128 ? 128u : 256u;
+            h->shape = staged_shape(*h->ops, h->smag, sblock, static_cast<uint32_t>(o.stages), o.device);
+            if (h->shape.per_sm <= 0) {
+                if (o.kernel == ORR_KERNEL_STAGED) {
+                    throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step cannot launch with " +
+                                                       std::to_string(h->shape.stages) + " stages"};
+                }
+            } else {
+                h->persistent = true;
+                if (binary32) {
+                    h->upload_table(h->phys32);
+                } else {
+                    h->upload_table(h->phys64);
+                }
+                // No more CTAs than items.
+                const uint64_t most = std::max<uint64_t>({h->items.staged, h->items.direct, 1});
+                h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
+            }
+        }
         initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
         check(cudaStreamSynchronize(s), "create");
         // The per-node tables are on the device now; keep the links.
@@ -496,6 +346,9 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
 }
 
 void orr_lbm3d_destroy(orr_lbm3d* solver) {
+    if (solver != nullptr && solver->batch != nullptr) {
+        orr_batch3d_forget(solver->batch, solver);
+    }
     delete solver;
 }
 
@@ -521,6 +374,9 @@ orr_status orr_lbm3d_initialize(orr_lbm3d* solver, const double* rho, const doub
 orr_status orr_lbm3d_step(orr_lbm3d* solver, uint64_t count) {
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
+        if (h->batch != nullptr) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d: the solver belongs to a batch; step the batch"};
+        }
         h->run(count);
         return ORR_OK;
     });
@@ -573,6 +429,7 @@ orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
                               h->stream),
               "force read-back");
         check(cudaStreamSynchronize(h->stream), "force read-back");
+        h->check_status();
         std::memcpy(force_moment, h->host_small + 8, 6 * sizeof(double));
         return ORR_OK;
     });
@@ -582,6 +439,7 @@ orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, dou
                                  double* uz) {
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
+        h->check_status();
         const std::size_t cells = h->plan.cells;
         check(h->ops->moments(h->g, h->phys(), h->cls, h->f[h->cur], h->moments, h->stream),
               "moments kernel");
@@ -617,6 +475,7 @@ orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
         if (f == nullptr) {
             throw Refusal{ORR_ERR_INVALID, "null output"};
         }
+        h->check_status();
         const std::size_t cells = h->plan.cells;
         const std::size_t n = d3::Q * cells;
         if (h->storage == ORR_STORAGE_F64) {
@@ -666,6 +525,7 @@ orr_status orr_lbm3d_mass(orr_lbm3d* solver, double* mass) {
                               h->stream),
               "mass read-back");
         check(cudaStreamSynchronize(h->stream), "mass read-back");
+        h->check_status();
         double m = h->host_small[16];
         if (h->storage != ORR_STORAGE_F64) {
             m += static_cast<double>(h->plan.fluid); // the weights of each fluid node add up to 1
@@ -711,6 +571,34 @@ orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream) {
     }
     *stream = solver->stream;
     return ORR_OK;
+}
+
+orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info) {
+    if (solver == nullptr || info == nullptr) {
+        return orr::fail(ORR_ERR_INVALID, "null argument");
+    }
+    return orr::guarded(nullptr, [&]() -> orr_status {
+        check(cudaSetDevice(solver->device), "cudaSetDevice");
+        orr_kernel_info k{};
+        if (solver->persistent) {
+            k.kernel = ORR_KERNEL_STAGED;
+            k.block = solver->shape.block;
+            k.stages = solver->shape.stages;
+            k.grid = solver->shape.grid;
+            k.ctas_per_sm = solver->shape.per_sm;
+            k.registers = solver->ops->staged_registers(solver->smag, solver->shape.block);
+            k.shared_bytes = solver->ops->staged_smem(solver->shape.block, solver->shape.stages);
+            k.staged_items = solver->items.staged;
+            k.direct_items = solver->items.direct;
+        } else {
+            k.kernel = ORR_KERNEL_ROWS;
+            k.block = solver->block;
+            k.grid = ((solver->g.nx + solver->block - 1) / solver->block) * solver->g.ny * solver->g.nz;
+            k.registers = solver->ops->step_registers(solver->smag);
+        }
+        *info = k;
+        return ORR_OK;
+    });
 }
 
 orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches) {

@@ -29,6 +29,7 @@ template <> struct Storage<float> {
     using A = float;
     static constexpr bool kShifted = true;
     __device__ __forceinline__ static A load(const float* p) { return __ldg(p); }
+    __device__ __forceinline__ static A value(float v) { return v; }
     __device__ __forceinline__ static void store(float* p, A v) { *p = v; }
     __host__ __device__ static float encode(double shifted) { return static_cast<float>(shifted); }
     __host__ __device__ static double decode(float s) { return static_cast<double>(s); }
@@ -40,6 +41,7 @@ template <> struct Storage<__half> {
     __device__ __forceinline__ static A load(const __half* p) {
         return __half2float(__ldg(p));
     }
+    __device__ __forceinline__ static A value(__half v) { return __half2float(v); }
     __device__ __forceinline__ static void store(__half* p, A v) {
         *p = __float2half_rn(v);
     }
@@ -57,6 +59,7 @@ template <> struct Storage<__nv_bfloat16> {
     __device__ __forceinline__ static A load(const __nv_bfloat16* p) {
         return __bfloat162float(__ldg(p));
     }
+    __device__ __forceinline__ static A value(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, A v) {
         *p = __float2bfloat16_rn(v);
     }
@@ -72,6 +75,7 @@ template <> struct Storage<double> {
     using A = double;
     static constexpr bool kShifted = false;
     __device__ __forceinline__ static A load(const double* p) { return __ldg(p); }
+    __device__ __forceinline__ static A value(double v) { return v; }
     __device__ __forceinline__ static void store(double* p, A v) { *p = v; }
     __host__ __device__ static double encode(double unshifted) { return unshifted; }
     __host__ __device__ static double decode(double s) { return s; }

@@ -184,34 +184,39 @@ def naca_wing_mask(nx: int, ny: int, nz: int, digits: str, leading_edge, chord: 
     the closed trailing edge, naca.h:21-29), chord along x, thickness along y,
     span along z centred on ``leading_edge[2]``, pitched nose-up by
     ``angle_of_attack`` radians about the leading edge for flow along +x.
+    The thickness is laid off normal to the chord line rather than to the
+    camber line (a difference of order t theta^2 for the cambered sections).
     The distance is an estimate (positive outside, negative inside) from the
-    local half-thickness; the flags are exact point-in-section tests.
+    local half-thickness; the flags are exact point-in-section tests.  The
+    section test depends on (x, y) only and the span test on z only, so both
+    are evaluated on their own axes and combined by broadcasting.
     """
+    if nx <= 0 or ny <= 0 or nz <= 0 or nx * ny * nz > MAX_GRID_CELLS:
+        raise ValueError("lbm3d: mask dimensions must be positive with at most "
+                         "geom::max_grid_cells nodes")
     m, p, t = naca4_profile(digits)
     lx, ly, lz = (float(v) for v in leading_edge)
     ca, sa = math.cos(angle_of_attack), math.sin(angle_of_attack)
-
-    def sdf(x, y, z):
-        dx, dy = x - lx, y - ly
-        # section coordinates (unit chord): undo the nose-up rotation
-        u = (ca * dx - sa * dy) / chord
-        v = (sa * dx + ca * dy) / chord
-        uc = np.clip(u, 0.0, 1.0)
-        yt = 5.0 * t * (0.2969 * np.sqrt(uc) - 0.1260 * uc - 0.3516 * uc ** 2 + 0.2843 * uc ** 3
-                        - 0.1036 * uc ** 4)
-        if m > 0.0:
-            yc = np.where(uc < p, m / p ** 2 * (2 * p * uc - uc ** 2),
-                          m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * uc - uc ** 2))
-        else:
-            yc = np.zeros_like(uc)
-        # chordwise and normal excess in lattice units
-        d_norm = (np.abs(v - yc) - yt) * chord
-        d_chord = np.maximum(-u, u - 1.0) * chord
-        d_span = np.abs(z - lz) - 0.5 * span
-        out = np.maximum(np.maximum(d_norm, d_chord), d_span)
-        return out
-
-    return mask_from_sdf_3d(nx, ny, nz, sdf)
+    y, x = np.meshgrid(np.arange(ny, dtype=np.float64), np.arange(nx, dtype=np.float64), indexing="ij")
+    dx, dy = x - lx, y - ly
+    # section coordinates (unit chord): undo the nose-up rotation
+    u = (ca * dx - sa * dy) / chord
+    v = (sa * dx + ca * dy) / chord
+    uc = np.clip(u, 0.0, 1.0)
+    yt = 5.0 * t * (0.2969 * np.sqrt(uc) - 0.1260 * uc - 0.3516 * uc ** 2 + 0.2843 * uc ** 3
+                    - 0.1036 * uc ** 4)
+    if m > 0.0:
+        yc = np.where(uc < p, m / p ** 2 * (2 * p * uc - uc ** 2),
+                      m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * uc - uc ** 2))
+    else:
+        yc = np.zeros_like(uc)
+    # chordwise and normal excess in lattice units
+    d_norm = (np.abs(v - yc) - yt) * chord
+    d_chord = np.maximum(-u, u - 1.0) * chord
+    d_section = np.maximum(d_norm, d_chord)                        # (ny, nx)
+    d_span = np.abs(np.arange(nz, dtype=np.float64) - lz) - 0.5 * span  # (nz,)
+    d = np.maximum(d_section[None, :, :], d_span[:, None, None]).reshape(-1)
+    return SolidMask3D(nx, ny, nz, (d <= 0.0).astype(np.uint8), d)
 
 
 def mask_from_sdf(nx: int, ny: int, sdf) -> SolidMask2D:

@@ -65,14 +65,19 @@ class Force2D:
     moment: float
 
 
-def _options(storage: str, allow_high_mach: bool, device: int, block_x: int) -> abi.CSolverOptions:
+def _options(storage: str, allow_high_mach: bool, device: int, block_x: int, kernel: str = "auto",
+             stages: int = 0) -> abi.CSolverOptions:
     if storage not in abi.STORAGE_NAMES:
         raise ValueError(f"unknown storage {storage!r}; one of {sorted(abi.STORAGE_NAMES)}")
+    if kernel not in abi.KERNEL_NAMES:
+        raise ValueError(f"unknown step kernel {kernel!r}; one of {sorted(abi.KERNEL_NAMES)}")
     o = abi.CSolverOptions()
     o.storage = abi.STORAGE_NAMES[storage]
     o.allow_high_mach = 1 if allow_high_mach else 0
     o.device = int(device)
     o.block_x = int(block_x)
+    o.kernel = abi.KERNEL_NAMES[kernel]
+    o.stages = int(stages)
     return o
 
 
@@ -128,7 +133,8 @@ class CudaLbm3D:
     q = 19
 
     def __init__(self, config: Lbm3DConfig, mask: SolidMask3D, storage: str = "f32",
-                 allow_high_mach: bool = False, device: int = 0, block_x: int = 0):
+                 allow_high_mach: bool = False, device: int = 0, block_x: int = 0,
+                 kernel: str = "auto", stages: int = 0):
         self._lib = lib()
         self._h = None
         self.config = config
@@ -140,7 +146,7 @@ class CudaLbm3D:
             raise LbmError(abi.ORR_ERR_INVALID, "lbm3d: the solid mask does not match the lattice size")
         dist = None if mask.distance is None else np.ascontiguousarray(mask.distance, np.float64).reshape(-1)
         self._solid = solid
-        opts = _options(storage, allow_high_mach, device, block_x)
+        opts = _options(storage, allow_high_mach, device, block_x, kernel, stages)
         c = config.to_c()
         h = ctypes.c_void_p()
         check(self._lib.orr_lbm3d_create(ctypes.byref(c), ptr(solid, _u8p), ptr(dist, _dp), ctypes.byref(opts),
@@ -242,6 +248,16 @@ class CudaLbm3D:
         self._check(self._lib.orr_lbm3d_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    def kernel_info(self) -> dict:
+        """The step kernel this solver runs and its launch shape."""
+        k = abi.CKernelInfo()
+        self._check(self._lib.orr_lbm3d_kernel_info(self._h, ctypes.byref(k)))
+        names = {v: n for n, v in abi.KERNEL_NAMES.items()}
+        return {"kernel": names.get(k.kernel, str(k.kernel)), "block": k.block, "stages": k.stages,
+                "grid": k.grid, "ctas_per_sm": k.ctas_per_sm, "registers": k.registers,
+                "shared_bytes": k.shared_bytes, "staged_items": k.staged_items,
+                "direct_items": k.direct_items}
+
 
 class CudaLbm2D:
     """A D2Q9 device solver (the reference's GpuLbm2D behind Lbm2DSolver)."""
@@ -338,10 +354,11 @@ class CudaLbm2D:
 
 
 def make_gpu_solver(config, mask, storage: str = "f32", allow_high_mach: bool = False,
-                    device: int = 0, block_x: int = 0):
-    """make_gpu_solver (lbm3d.h:246-247; lbm2d.h:211-212) on the CUDA path."""
+                    device: int = 0, block_x: int = 0, kernel: str = "auto", stages: int = 0):
+    """make_gpu_solver (lbm3d.h:246-247; lbm2d.h:211-212) on the CUDA path.
+    `kernel` and `stages` choose the D3Q19 step kernel (ignored in 2D)."""
     if isinstance(config, Lbm3DConfig):
-        return CudaLbm3D(config, mask, storage, allow_high_mach, device, block_x)
+        return CudaLbm3D(config, mask, storage, allow_high_mach, device, block_x, kernel, stages)
     if isinstance(config, Lbm2DConfig):
         return CudaLbm2D(config, mask, storage, allow_high_mach, device, block_x)
     raise TypeError("config must be an Lbm3DConfig or an Lbm2DConfig")

@@ -17,6 +17,20 @@ Workloads (sizes in lattice nodes):
                   rotated 10 degrees about z, u = 0.08, Re 1000 on the major
                   axis L = 96 (nu 0.00768), Smagorinsky C = 0.12 (the inlet
                   speed is above the lattice Mach guard: needs the opt-in).
+  naca_batch      64 D3Q19 lattices for the batched form: sizes drawn from the
+                  seed between 96^3 and 256 x 128 x 128 (nx a multiple of 16),
+                  each with a NACA 4-digit wing (0012, 2412 or 4415), chord
+                  0.4 nx, span 0.6 nz, angle of attack uniform in -4..12
+                  degrees, u = 0.05, Re uniform in 200..1000 on the chord,
+                  Smagorinsky C = 0.1, free-slip lateral walls, zero-gradient
+                  outflow.
+  sphere_cone_requests
+                  the serving form's request stream: Poisson arrivals (rate
+                  20/s), sphere-cone capsules (half-angle 20..35 degrees, nose
+                  radius 0.2..0.4 of the base radius, base radius ny / 8) on
+                  grids nx = 64 + 256 t, ny = nz = 64 + 96 t with t uniform in
+                  [0, 1] (nx rounded to a multiple of 16), Re uniform in
+                  100..2000 on the base diameter, u = 0.05, Smagorinsky C = 0.1.
 """
 from __future__ import annotations
 
@@ -161,3 +175,118 @@ def coefficients2d(fx: float, fy: float, u: float, diameter: float, rho: float =
     """force_coefficients (src/aero/lbm/force_history.cpp:9-13): per unit span."""
     q = 0.5 * rho * u * u
     return {"cd": fx / (q * diameter), "cl": fy / (q * diameter)}
+
+
+@dataclass
+class BatchMember:
+    """Parameters of one lattice of the batched form; ``build()`` makes the workload."""
+    index: int
+    seed: int
+    nx: int
+    ny: int
+    nz: int
+    digits: str
+    angle_deg: float
+    reynolds: float
+    u: float = 0.05
+    smagorinsky: float = 0.1
+    noise: float = 1e-3
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def chord(self) -> float:
+        return 0.4 * self.nx
+
+    @property
+    def span(self) -> float:
+        return 0.6 * self.nz
+
+    def build(self) -> Workload3D:
+        chord = self.chord
+        cfg = Lbm3DConfig(nx=self.nx, ny=self.ny, nz=self.nz,
+                          tau=tau_of_viscosity(self.u * chord / self.reynolds),
+                          x_boundary=XBoundary.inflow_outflow, outlet=Outlet.extrapolation,
+                          y_low=wall(WallKind.slip), y_high=wall(WallKind.slip),
+                          z_low=wall(WallKind.slip), z_high=wall(WallKind.slip), inlet_ux=self.u,
+                          smagorinsky=Smagorinsky(self.smagorinsky > 0.0, self.smagorinsky))
+        leading = (0.25 * self.nx, 0.5 * self.ny, 0.5 * self.nz)
+        mask = M.naca_wing_mask(self.nx, self.ny, self.nz, self.digits, leading, chord, self.span,
+                                math.radians(self.angle_deg))
+        rho, ux, uy, uz = noisy_state3d(cfg, mask, self.seed, self.noise)
+        return Workload3D(f"naca{self.digits}_{self.nx}x{self.ny}x{self.nz}", cfg, mask, rho, ux, uy, uz,
+                          chord, chord * self.span)
+
+
+def naca_batch(seed: int = 4, count: int = 64) -> list[BatchMember]:
+    """The batched form's lattices (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        nx = int(16 * round(rng.uniform(96.0, 256.0) / 16.0))
+        ny = int(round(rng.uniform(96.0, 128.0)))
+        nz = int(round(rng.uniform(96.0, 128.0)))
+        digits = str(rng.choice(["0012", "2412", "4415"]))
+        angle = float(rng.uniform(-4.0, 12.0))
+        reynolds = float(rng.uniform(200.0, 1000.0))
+        out.append(BatchMember(k, seed * 1000 + k, nx, ny, nz, digits, angle, reynolds))
+    return out
+
+
+@dataclass
+class SolveRequest:
+    """One request of the serving form: arrival time (seconds from the
+    start of the stream) and the body; ``build()`` makes the workload."""
+    index: int
+    seed: int
+    arrival: float
+    nx: int
+    ny: int
+    nz: int
+    half_angle_deg: float
+    nose_ratio: float
+    reynolds: float
+    u: float = 0.05
+    smagorinsky: float = 0.1
+    noise: float = 1e-3
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def base_radius(self) -> float:
+        return self.ny / 8.0
+
+    def build(self) -> Workload3D:
+        rb = self.base_radius
+        diameter = 2.0 * rb
+        cfg = Lbm3DConfig(nx=self.nx, ny=self.ny, nz=self.nz,
+                          tau=tau_of_viscosity(self.u * diameter / self.reynolds),
+                          x_boundary=XBoundary.inflow_outflow, outlet=Outlet.extrapolation,
+                          y_low=wall(WallKind.slip), y_high=wall(WallKind.slip),
+                          z_low=wall(WallKind.slip), z_high=wall(WallKind.slip), inlet_ux=self.u,
+                          smagorinsky=Smagorinsky(self.smagorinsky > 0.0, self.smagorinsky))
+        nose = (0.2 * self.nx, 0.5 * (self.ny - 1), 0.5 * (self.nz - 1))
+        mask = M.sphere_cone_mask(self.nx, self.ny, self.nz, nose, rb, math.radians(self.half_angle_deg),
+                                  self.nose_ratio * rb)
+        rho, ux, uy, uz = noisy_state3d(cfg, mask, self.seed, self.noise)
+        return Workload3D(f"sphere_cone_{self.nx}x{self.ny}x{self.nz}", cfg, mask, rho, ux, uy, uz,
+                          diameter, math.pi * rb * rb)
+
+
+def sphere_cone_requests(seed: int = 5, count: int = 48, rate: float = 20.0) -> list[SolveRequest]:
+    """The serving form's request stream (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        size = float(rng.uniform(0.0, 1.0))
+        nx = int(16 * round((64.0 + 256.0 * size) / 16.0))
+        ny = nz = int(round(64.0 + 96.0 * size))
+        out.append(SolveRequest(k, seed * 1000 + k, t, nx, ny, nz, float(rng.uniform(20.0, 35.0)),
+                                float(rng.uniform(0.2, 0.4)), float(rng.uniform(100.0, 2000.0))))
+    return out

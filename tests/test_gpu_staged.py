@@ -1,0 +1,119 @@
+"""The persistent staged D3Q19 step against the row-tile step.
+
+Both kernels finish every node with the same device code (the staged kernel
+only changes where the 19 plain pulls come from: a shared-memory stage
+instead of global loads), so for every storage form they must give the same
+populations bit for bit.  The cases cover each rule the staged kernel has to
+route correctly: inlet and extrapolation / convective outlets at the x edges
+of interior rows, halfway and interpolated bounce-back next to staged
+values, periodic x with moving no-slip walls and a body force, the absorbing
+layers, row tiles that end inside a row (nx not a multiple of the tile) and
+lattices whose rows cannot be staged (every row on the per-node path).
+"""
+import numpy as np
+import pytest
+
+from helpers import copy_config, duct_config, sphere_channel
+from orrery_b200 import masks as M
+from orrery_b200 import solver as S
+from orrery_b200.lbm3d import Outlet, Smagorinsky, SolidWall, Sponge, WallKind, wall
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 150
+
+
+def case(name):
+    if name == "sphere_les":
+        cfg, mask = sphere_channel(64, 32, 32, 8.0, 2.5, 0.05, 20.0)
+        cfg.smagorinsky = Smagorinsky(True, 0.1)
+        return cfg, mask
+    if name == "interpolated_convective_sponge":
+        cfg, mask = sphere_channel(64, 24, 20, 7.0, 3.0, 0.05, 40.0)
+        cfg.solid_wall = SolidWall.interpolated
+        cfg.outlet = Outlet.convective
+        cfg.sponge = Sponge(0.5, 6, 8, 4)
+        cfg.z_low = wall(WallKind.no_slip, 0.01)
+        cfg.z_high = wall(WallKind.no_slip, -0.02)
+        cfg.smagorinsky = Smagorinsky(True, 0.12)
+        return cfg, mask
+    if name == "periodic_duct_obstacle":
+        cfg = duct_config(48, 16, 12, 0.8, 1e-5)
+        mask = M.box_mask(48, 16, 12, (10, 4, 3), (16, 9, 8))
+        return cfg, mask
+    if name == "ragged_tile":
+        # 272 = 256 + 16: the second tile of a 256-node row holds 16 nodes.
+        cfg, mask = sphere_channel(272, 12, 10, 6.0, 4.0, 0.05, 30.0)
+        return cfg, mask
+    if name == "unaligned_rows":
+        # nx = 40 is not a multiple of 16: every row takes the per-node path.
+        cfg, mask = sphere_channel(40, 16, 16, 6.0, 2.5, 0.05, 30.0)
+        return cfg, mask
+    raise KeyError(name)
+
+
+CASES = ["sphere_les", "interpolated_convective_sponge", "periodic_duct_obstacle", "ragged_tile",
+         "unaligned_rows"]
+
+
+def run(cfg, mask, storage, kernel, block=0, stages=0, steps=STEPS, inlet=None):
+    s = S.make_gpu_solver(cfg, mask, storage=storage, kernel=kernel, block_x=block, stages=stages)
+    if inlet is not None:
+        s.set_inlet_velocity(inlet)
+    s.step(steps)
+    return s
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("name", CASES)
+def test_staged_equals_rows_bitwise(name, storage):
+    cfg, mask = case(name)
+    a = run(cfg, mask, storage, "rows")
+    b = run(cfg, mask, storage, "staged")
+    info = b.kernel_info()
+    assert info["kernel"] == "staged"
+    if name == "unaligned_rows":
+        assert info["staged_items"] == 0
+    else:
+        assert info["staged_items"] > 0
+    fa, fb = a.populations(), b.populations()
+    assert np.array_equal(fa, fb), f"max diff {np.max(np.abs(fa - fb))}"
+    # Equal populations; the binary64 link sum adds with atomics, so only its
+    # last bits may depend on the order.
+    ga, gb = a.force().force, b.force().force
+    assert np.allclose(ga, gb, rtol=0, atol=1e-12 * np.max(np.abs(ga)))
+
+
+@pytest.mark.parametrize("block,stages", [(128, 1), (128, 3), (256, 2), (256, 4)])
+def test_launch_shapes_agree(block, stages):
+    cfg, mask = case("sphere_les")
+    ref = run(cfg, mask, "f32", "rows")
+    s = run(cfg, mask, "f32", "staged", block=block, stages=stages)
+    info = s.kernel_info()
+    assert (info["block"], info["stages"]) == (block, stages)
+    assert np.array_equal(ref.populations(), s.populations())
+
+
+def test_skewed_inlet_bitwise():
+    cfg, mask = case("sphere_les")
+    cfg = copy_config(cfg)
+    a = run(cfg, mask, "f64", "rows", inlet=(0.04, 0.004, -0.003))
+    b = run(cfg, mask, "f64", "staged", inlet=(0.04, 0.004, -0.003))
+    assert np.array_equal(a.populations(), b.populations())
+
+
+def test_automatic_choice():
+    cfg, mask = case("sphere_les")
+    assert S.make_gpu_solver(cfg, mask).kernel_info()["kernel"] == "staged"
+    cfg, mask = case("unaligned_rows")
+    assert S.make_gpu_solver(cfg, mask).kernel_info()["kernel"] == "rows"
+    cfg, mask = case("sphere_les")
+    assert S.make_gpu_solver(cfg, mask, kernel="rows").kernel_info()["kernel"] == "rows"
+
+
+def test_refused_shapes():
+    cfg, mask = case("sphere_les")
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, kernel="staged", block_x=64)
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, kernel="staged", stages=9)
