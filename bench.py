@@ -7,6 +7,8 @@ collide-stream step over the whole lattice; MLUPS counts every node
 (steps * nx * ny * nz / s / 1e6).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {cuda,reference}]
+  python bench.py --form batched [--storage f16] [--steps 3000]   (64 NACA lattices, one batch)
+  python bench.py --form serve [--storage f16]                     (sphere-cone request stream)
 
 N > 1 runs under torchrun as N independent replicas (one lattice per GPU, no
 collective on the data path); the reported value is the whole-job MLUPS over
@@ -152,6 +154,36 @@ def run_reference_arm(args, rank: int):
     return 0
 
 
+def run_form(args, rank: int) -> int:
+    """The batched and served forms (one GPU; other ranks idle)."""
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(0)
+    from orrery_b200 import forms
+    clocks = ClockSampler(0)
+    clocks.start()
+    if args.form == "batched":
+        steps = args.steps if args.steps != 1000 else 3000
+        r = forms.run_batched(storage=args.storage, count=args.lattices, steps=steps, plain=not args.no_plain,
+                              warmup=max(args.warmup, 4))
+        metric, value, unit = "D3Q19 batched solves/s", r["solves_per_s"], "solves/s"
+    else:
+        r = forms.run_serve(storage=args.storage, count=args.requests, max_steps=args.max_steps,
+                            plain=not args.no_plain, oracle_check=args.oracle_check)
+        metric, value, unit = "D3Q19 served solves/s", r["served"]["solves_per_s"], "solves/s"
+    clock_info = clocks.stop()
+    peak, peak_kind = measured_peak()
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "f32", "f16": "f16-storage/f32-math", "bf16": "bf16-storage/f32-math",
+                      "f64": "f64"}[args.storage],
+            "data": "synthetic", "form": args.form, "result": r, "clocks": clock_info,
+            "hbm_peak_gbs": peak, "peak_source": peak_kind}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -162,6 +194,13 @@ def main(argv=None) -> int:
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
     ap.add_argument("--stages", type=int, default=0)
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"])
+    ap.add_argument("--lattices", type=int, default=64, help="batched form: lattices")
+    ap.add_argument("--requests", type=int, default=48, help="serve form: requests")
+    ap.add_argument("--max-steps", type=int, default=20000, help="serve form: step cap per solve")
+    ap.add_argument("--oracle-check", type=int, default=0,
+                    help="serve form: requests whose Cd is checked against the binary64 form")
+    ap.add_argument("--no-plain", action="store_true", help="batched/serve: skip the plain-form baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1000)
     args = ap.parse_args(argv)
@@ -171,6 +210,8 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.form != "plain":
+        return run_form(args, rank)
 
     import torch
     dist = None

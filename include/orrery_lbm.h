@@ -291,6 +291,102 @@ ORR_API orr_status orr_batch3d_synchronize(orr_batch3d* batch);
 ORR_API orr_status orr_batch3d_stream(const orr_batch3d* batch, void** stream);
 ORR_API orr_status orr_batch3d_launch_count(const orr_batch3d* batch, uint64_t* launches);
 
+/* ---- D3Q19 serving ------------------------------------------------------ */
+
+/* A server runs drag solves of any lattice size as they arrive, with
+ * continuous batching on one device: each round advances every admitted
+ * lattice by `chunk_steps` steps in one batch (orr_batch3d_*), admits queued
+ * requests in arrival order while a slot is free and the admitted lattices'
+ * device memory (orr_lbm3d_memory_bytes) stays within `memory_budget` - the
+ * planning, allocation and upload of new solves overlap the running chunk -
+ * and retires the solves that are done.  A solve samples its force every
+ * `sample_every` steps (the reference adapter's sampling,
+ * lbm_aero_solver3d.cpp:385-441) and is done when the mean Cd of its last
+ * window of `window` steps differs from the previous window's by less than
+ * `tolerance` (converged), at `max_steps` (capped), or when the force stops
+ * being finite (failed).  A solve's result is the same alone and in any mix.
+ * The reference has no counterpart: atmo::sample_cd_table
+ * (src/atmo/cd_sampling.cpp:98-120) runs its solves one after another.
+ * Entry points are thread-safe; results are kept until the server is
+ * destroyed. */
+typedef struct orr_server orr_server;
+
+typedef struct orr_serve_options {
+    int32_t storage;          /* ORR_STORAGE_* of every solve */
+    int32_t device;
+    uint64_t memory_budget;   /* bytes of device memory the admitted lattices may hold */
+    uint32_t max_active;      /* lattices on the device at once */
+    uint32_t chunk_steps;     /* steps per round (a multiple of sample_every) */
+    uint32_t sample_every;    /* force sampling interval, even */
+    int32_t kernel;           /* batch schedule: ORR_KERNEL_STAGED (default) or ORR_KERNEL_ROWS */
+    uint32_t block;           /* 0: the schedule's default */
+    uint32_t stages;          /* 0: tuned default */
+} orr_serve_options;
+
+typedef struct orr_solve_request {
+    const orr_lbm3d_config* config;   /* inflow / outflow x with a non-zero inlet speed */
+    const uint8_t* solid;             /* nx*ny*nz flags, copied */
+    const double* distance;           /* signed distances or NULL, copied */
+    const double* rho;                /* initial fields (all four or none), copied */
+    const double* ux;
+    const double* uy;
+    const double* uz;
+    int32_t allow_high_mach;
+    uint32_t sample_every;            /* 0 or the server's */
+    uint32_t window;                  /* steps per window, a multiple of chunk_steps */
+    uint32_t reserved;
+    double tolerance;                 /* on |delta Cd| between consecutive window means */
+    uint64_t max_steps;               /* step cap (0: none) */
+    double reference_area;            /* Cd = Fx / (1/2 rho U^2 A) */
+    double reference_length;          /* Cm = Mz / (1/2 rho U^2 A L) */
+    double moment_centre[3];
+} orr_solve_request;
+
+enum {
+    ORR_SOLVE_QUEUED = 0,
+    ORR_SOLVE_RUNNING = 1,
+    ORR_SOLVE_CONVERGED = 2,
+    ORR_SOLVE_CAPPED = 3,
+    ORR_SOLVE_FAILED = 4
+};
+
+typedef struct orr_solve_result {
+    int32_t state;                    /* ORR_SOLVE_* */
+    int32_t reserved;
+    uint64_t steps;
+    double cd, cl, cm;                /* means of the last window (lift along +y, moment about z) */
+    double delta_cd;                  /* |Cd difference| of the last two windows */
+    double force[3], moment[3];       /* window means, moment about the lattice origin */
+    double arrival_s, admitted_s, finished_s; /* seconds since the server started */
+    uint64_t device_bytes;
+    char message[160];
+} orr_solve_result;
+
+typedef struct orr_serve_statistics {
+    uint64_t submitted, completed, failed, queued, active;
+    double latency_p50_s, latency_p99_s, latency_mean_s; /* arrival to result, completed solves */
+    double solves_per_second;         /* completed / (last finish - first arrival) */
+    double lattice_updates;           /* sum over rounds of active nodes x steps */
+    double busy_seconds;              /* time with lattices on the device */
+    uint64_t peak_device_bytes;
+    double mean_active;               /* lattices per round */
+    uint64_t chunks;
+    int32_t worker_failed;
+    char message[160];
+} orr_serve_statistics;
+
+ORR_API orr_status orr_serve_create(const orr_serve_options* options, orr_server** out);
+/* Stops the worker (solves still queued or running are abandoned). */
+ORR_API void orr_serve_destroy(orr_server* server);
+ORR_API const char* orr_serve_last_error(const orr_server* server);
+ORR_API orr_status orr_serve_submit(orr_server* server, const orr_solve_request* request, uint64_t* id);
+ORR_API orr_status orr_serve_poll(orr_server* server, uint64_t id, orr_solve_result* result);
+/* Blocks until the solve is done or the timeout passes (ORR_ERR_TIMEOUT). */
+ORR_API orr_status orr_serve_wait(orr_server* server, uint64_t id, double timeout_s, orr_solve_result* result);
+/* Blocks until every submitted solve is done or the timeout passes. */
+ORR_API orr_status orr_serve_drain(orr_server* server, double timeout_s);
+ORR_API orr_status orr_serve_stats(orr_server* server, orr_serve_statistics* stats);
+
 /* Inputs of orr_lbm3d_force_static: device pointers the caller owns. */
 typedef struct orr_force_links {
     uint64_t nx, ny, nz;        /* lattice dimensions */

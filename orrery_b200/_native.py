@@ -83,6 +83,14 @@ SIGNATURES = {
     "orr_batch3d_synchronize": (_st, [_vp]),
     "orr_batch3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
     "orr_batch3d_launch_count": (_st, [_vp, _u64p]),
+    "orr_serve_create": (_st, [ctypes.POINTER(abi.CServeOptions), ctypes.POINTER(_vp)]),
+    "orr_serve_destroy": (None, [_vp]),
+    "orr_serve_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_serve_submit": (_st, [_vp, ctypes.POINTER(abi.CSolveRequest), _u64p]),
+    "orr_serve_poll": (_st, [_vp, ctypes.c_uint64, ctypes.POINTER(abi.CSolveResult)]),
+    "orr_serve_wait": (_st, [_vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(abi.CSolveResult)]),
+    "orr_serve_drain": (_st, [_vp, ctypes.c_double]),
+    "orr_serve_stats": (_st, [_vp, ctypes.POINTER(abi.CServeStatistics)]),
 }
 
 

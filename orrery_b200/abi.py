@@ -95,3 +95,47 @@ class CBatchSchedule(ctypes.Structure):
     """orr_batch_schedule."""
     _fields_ = [("kernel", ctypes.c_int32), ("block", ctypes.c_uint32), ("stages", ctypes.c_uint32),
                 ("grid", ctypes.c_uint32), ("ms_per_step", ctypes.c_double)]
+
+
+class CServeOptions(ctypes.Structure):
+    """orr_serve_options."""
+    _fields_ = [("storage", ctypes.c_int32), ("device", ctypes.c_int32), ("memory_budget", ctypes.c_uint64),
+                ("max_active", ctypes.c_uint32), ("chunk_steps", ctypes.c_uint32),
+                ("sample_every", ctypes.c_uint32), ("kernel", ctypes.c_int32), ("block", ctypes.c_uint32),
+                ("stages", ctypes.c_uint32)]
+
+
+class CSolveRequest(ctypes.Structure):
+    """orr_solve_request."""
+    _fields_ = [("config", ctypes.POINTER(CLbm3DConfig)), ("solid", ctypes.POINTER(ctypes.c_uint8)),
+                ("distance", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double)),
+                ("ux", ctypes.POINTER(ctypes.c_double)), ("uy", ctypes.POINTER(ctypes.c_double)),
+                ("uz", ctypes.POINTER(ctypes.c_double)), ("allow_high_mach", ctypes.c_int32),
+                ("sample_every", ctypes.c_uint32), ("window", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("tolerance", ctypes.c_double), ("max_steps", ctypes.c_uint64),
+                ("reference_area", ctypes.c_double), ("reference_length", ctypes.c_double),
+                ("moment_centre", ctypes.c_double * 3)]
+
+
+ORR_SOLVE_QUEUED, ORR_SOLVE_RUNNING, ORR_SOLVE_CONVERGED, ORR_SOLVE_CAPPED, ORR_SOLVE_FAILED = 0, 1, 2, 3, 4
+SOLVE_STATES = {0: "queued", 1: "running", 2: "converged", 3: "capped", 4: "failed"}
+
+
+class CSolveResult(ctypes.Structure):
+    """orr_solve_result."""
+    _fields_ = [("state", ctypes.c_int32), ("reserved", ctypes.c_int32), ("steps", ctypes.c_uint64),
+                ("cd", ctypes.c_double), ("cl", ctypes.c_double), ("cm", ctypes.c_double),
+                ("delta_cd", ctypes.c_double), ("force", ctypes.c_double * 3), ("moment", ctypes.c_double * 3),
+                ("arrival_s", ctypes.c_double), ("admitted_s", ctypes.c_double), ("finished_s", ctypes.c_double),
+                ("device_bytes", ctypes.c_uint64), ("message", ctypes.c_char * 160)]
+
+
+class CServeStatistics(ctypes.Structure):
+    """orr_serve_statistics."""
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("active", ctypes.c_uint64), ("latency_p50_s", ctypes.c_double),
+                ("latency_p99_s", ctypes.c_double), ("latency_mean_s", ctypes.c_double),
+                ("solves_per_second", ctypes.c_double), ("lattice_updates", ctypes.c_double),
+                ("busy_seconds", ctypes.c_double), ("peak_device_bytes", ctypes.c_uint64),
+                ("mean_active", ctypes.c_double), ("chunks", ctypes.c_uint64), ("worker_failed", ctypes.c_int32),
+                ("message", ctypes.c_char * 160)]

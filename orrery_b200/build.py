@@ -39,6 +39,7 @@ SOURCES = {
     "solver2d.cu": [],
     "force_static.cu": [],
     "batch3d.cu": [],
+    "serve3d.cu": [],
 }
 
 

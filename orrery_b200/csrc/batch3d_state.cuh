@@ -1,0 +1,393 @@
+// State of a batch of D3Q19 solvers (the handle behind orr_batch3d_*),
+// shared by the batch entry points and the serving loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "solver3d_state.cuh"
+
+namespace orr {
+
+// Candidate schedules of the autotuner (kernel, block, stages).
+struct Candidate {
+    int32_t kernel;
+    uint32_t block;
+    uint32_t stages;
+};
+inline constexpr Candidate kCandidates[] = {
+    {ORR_KERNEL_STAGED, 256, 2}, {ORR_KERNEL_STAGED, 256, 3}, {ORR_KERNEL_STAGED, 256, 4},
+    {ORR_KERNEL_STAGED, 128, 2}, {ORR_KERNEL_STAGED, 128, 4}, {ORR_KERNEL_ROWS, 128, 0},
+    {ORR_KERNEL_ROWS, 256, 0},
+};
+
+} // namespace orr
+
+struct orr_batch3d {
+    int device = 0;
+    int32_t storage = -1;
+    bool smag = false;
+    const Ops3D* ops = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::vector<orr_lbm3d*> members;
+    std::vector<cudaEvent_t> member_events;
+
+    // Schedule.
+    int32_t kernel = ORR_KERNEL_STAGED;
+    uint32_t block = 256;
+    uint32_t stages = 0;      // 0: the shape's default
+    StagedShape shape{};
+
+    // State of the current table: parities and epochs of the members when it
+    // was built, and the steps taken since (mod 2).
+    bool dirty = true;
+    std::vector<int> parity;
+    std::vector<uint64_t> epochs;
+    uint32_t flip = 0;
+    ItemCounts items{};
+    void* table = nullptr;
+    std::size_t table_bytes = 0;
+    std::vector<unsigned char> host_table; // host copy of the entries
+    uint32_t* status = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_sample = 0;    // sampling interval the graph was captured with (0: none)
+
+    // Batched forces.
+    void* jobs = nullptr;
+    std::size_t jobs_bytes = 0;
+    double* partial = nullptr;
+    std::size_t partial_count = 0;
+    double* sums = nullptr;       // 6 per member
+    std::size_t sums_count = 0;
+    uint64_t chunks = 0;
+    std::vector<ForceJob> host_jobs;
+
+    uint64_t launches = 0;
+    std::string error;
+
+    ~orr_batch3d() { release(); }
+
+    void release() noexcept {
+        cudaSetDevice(device);
+        for (orr_lbm3d* m : members) {
+            m->batch = nullptr;
+        }
+        members.clear();
+        if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : member_events) cudaEventDestroy(e);
+        member_events.clear();
+        for (void* p : {table, static_cast<void*>(status), jobs, static_cast<void*>(partial),
+                        static_cast<void*>(sums)}) {
+            if (p) cudaFree(p);
+        }
+        if (done) cudaEventDestroy(done);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        if (stream) cudaStreamDestroy(stream);
+        graph = nullptr;
+        table = jobs = nullptr;
+        status = nullptr;
+        partial = sums = nullptr;
+        done = t0 = t1 = nullptr;
+        stream = nullptr;
+    }
+
+    void drop_graph() {
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+    }
+
+    template <class T> static void grow(T*& p, std::size_t& have, std::size_t need, const char* what) {
+        if (need <= have && p != nullptr) {
+            return;
+        }
+        if (p) cudaFree(p);
+        p = nullptr;
+        have = 0;
+        check(cudaMalloc(reinterpret_cast<void**>(&p), std::max<std::size_t>(need, 1) * sizeof(T)), what);
+        have = need;
+    }
+    static void grow_bytes(void*& p, std::size_t& have, std::size_t need, const char* what) {
+        if (need <= have && p != nullptr) {
+            return;
+        }
+        if (p) cudaFree(p);
+        p = nullptr;
+        have = 0;
+        check(cudaMalloc(&p, std::max<std::size_t>(need, 1)), what);
+        have = need;
+    }
+
+    bool stale() const {
+        if (dirty) {
+            return true;
+        }
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            if (members[k]->epoch != epochs[k] || members[k]->cur != (parity[k] ^ static_cast<int>(flip))) {
+                return true;
+            }
+        }
+        return false;
+    }
+
+    template <class A> void fill_table(std::vector<Lattice3D<A>>& lats) {
+        lats.resize(members.size());
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            orr_lbm3d* m = members[k];
+            Lattice3D<A>& L = lats[k];
+            L = Lattice3D<A>{};
+            L.g = m->g;
+            if constexpr (sizeof(A) == 8) {
+                L.p = m->phys64;
+            } else {
+                L.p = m->phys32;
+            }
+            L.b = m->buffers();
+            L.f[0] = m->f[0];
+            L.f[1] = m->f[1];
+            L.parity = static_cast<uint32_t>(m->cur);
+            L.staged = stageable(m->g) ? 1u : 0u;
+        }
+        items = number_items(lats.data(), lats.size(), block);
+        host_table.resize(lats.size() * sizeof(Lattice3D<A>));
+        std::memcpy(host_table.data(), lats.data(), host_table.size());
+        grow_bytes(table, table_bytes, lats.size() * sizeof(Lattice3D<A>), "batch table");
+        check(cudaMemcpyAsync(table, lats.data(), lats.size() * sizeof(Lattice3D<A>), cudaMemcpyHostToDevice,
+                              stream),
+              "batch table upload");
+        check(cudaStreamSynchronize(stream), "batch table upload");
+    }
+
+    // Rebuilds the tables from the members' current state (flip restarts at 0).
+    void rebuild() {
+        drop_graph();
+        parity.resize(members.size());
+        epochs.resize(members.size());
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            parity[k] = members[k]->cur;
+            epochs[k] = members[k]->epoch;
+        }
+        flip = 0;
+        if (members.empty()) {
+            dirty = false;
+            return;
+        }
+        if (kernel == ORR_KERNEL_STAGED) {
+            shape = staged_shape(*ops, smag, block, stages, device);
+            if (shape.per_sm <= 0) {
+                throw Refusal{ORR_ERR_INVALID, "batch3d: the staged step cannot launch with this shape"};
+            }
+            if (storage == ORR_STORAGE_F64) {
+                std::vector<Lattice3D<double>> lats;
+                fill_table(lats);
+            } else {
+                std::vector<Lattice3D<float>> lats;
+                fill_table(lats);
+            }
+            const uint64_t most = std::max<uint64_t>({items.staged, items.direct, 1});
+            shape.grid = static_cast<uint32_t>(std::min<uint64_t>(shape.grid, most));
+        }
+        // Force jobs read the buffer that is current at flip 0 (sampling at
+        // even step counts only).
+        host_jobs.resize(members.size());
+        chunks = 0;
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            orr_lbm3d* m = members[k];
+            ForceJob& J = host_jobs[k];
+            J.f = m->f[parity[k]];
+            J.lcell = m->lcell;
+            J.ldir = m->ldir;
+            J.lq = m->lq;
+            J.links = m->plan.link_cell.size();
+            J.chunk_begin = chunks;
+            J.nx = m->g.nx;
+            J.plane = m->g.plane;
+            J.cells = m->g.cells;
+            chunks += (J.links + kForceChunk - 1) / kForceChunk;
+        }
+        grow_bytes(jobs, jobs_bytes, host_jobs.size() * sizeof(ForceJob), "batch force table");
+        check(cudaMemcpyAsync(jobs, host_jobs.data(), host_jobs.size() * sizeof(ForceJob),
+                              cudaMemcpyHostToDevice, stream),
+              "batch force table upload");
+        grow(partial, partial_count, std::max<uint64_t>(chunks, 1) * 6, "batch force partials");
+        grow(sums, sums_count, members.size() * 6, "batch force sums");
+        check(cudaStreamSynchronize(stream), "batch force table upload");
+        dirty = false;
+    }
+
+    // One step of every member (flip = steps since the table, mod 2).
+    void launch_step() {
+        if (kernel == ORR_KERNEL_STAGED) {
+            check(ops->staged(members.size() == 1 ? host_table.data() : nullptr, table,
+                              static_cast<uint32_t>(members.size()), items.staged, items.direct, flip,
+                              shape.stages, smag, shape.block, shape.grid, status, stream),
+                  "batch step kernel");
+            ++launches;
+        } else {
+            for (std::size_t k = 0; k < members.size(); ++k) {
+                orr_lbm3d* m = members[k];
+                const int from = parity[k] ^ static_cast<int>(flip);
+                check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block,
+                                stream),
+                      "batch step kernel");
+                ++launches;
+            }
+        }
+        flip ^= 1u;
+    }
+
+    // Sum of the members' force and moment into sums[6 k ..] (flip must be 0).
+    void launch_sample(bool accumulate) {
+        check(ops->force_batch(jobs, static_cast<uint32_t>(members.size()), chunks, partial, sums, accumulate,
+                               stream),
+              "batch force kernels");
+        launches += chunks > 0 ? 2 : 1;
+    }
+
+    // kGraphSteps steps, with a force sample after every `sample` steps
+    // when sample > 0 (kGraphSteps is then a multiple of it).
+    void build_graph(uint32_t sample, uint32_t steps) {
+        drop_graph();
+        cudaGraph_t captured = nullptr;
+        const uint64_t before = launches;
+        const uint32_t flip_before = flip;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "batch graph capture");
+        try {
+            for (uint32_t k = 0; k < steps; ++k) {
+                launch_step();
+                if (sample > 0 && (k + 1) % sample == 0) {
+                    launch_sample(true);
+                }
+            }
+        } catch (...) {
+            cudaStreamEndCapture(stream, &captured);
+            if (captured) cudaGraphDestroy(captured);
+            launches = before;
+            flip = flip_before;
+            throw;
+        }
+        launches = before;
+        flip = flip_before;
+        check(cudaStreamEndCapture(stream, &captured), "batch graph capture");
+        const cudaError_t e = cudaGraphInstantiate(&graph, captured, 0);
+        cudaGraphDestroy(captured);
+        check(e, "batch graph instantiate");
+        graph_sample = sample;
+        graph_steps = steps;
+        graph_launches = launches_per_step() * steps + (sample > 0 ? (steps / sample) * (chunks > 0 ? 2 : 1) : 0);
+    }
+    uint32_t graph_steps = 0;
+    uint64_t graph_launches = 0;
+
+    uint64_t launches_per_step() const {
+        return kernel == ORR_KERNEL_STAGED ? 1 : members.size();
+    }
+
+    void wait_members() {
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            check(cudaEventRecord(member_events[k], members[k]->stream), "batch event");
+            check(cudaStreamWaitEvent(stream, member_events[k], 0), "batch event");
+        }
+    }
+
+    void release_members(uint64_t count) {
+        check(cudaEventRecord(done, stream), "batch event");
+        for (std::size_t k = 0; k < members.size(); ++k) {
+            orr_lbm3d* m = members[k];
+            check(cudaStreamWaitEvent(m->stream, done, 0), "batch event");
+            m->cur = parity[k] ^ static_cast<int>(flip);
+            m->steps += count;
+        }
+    }
+
+    // `count` steps of every member; with sample > 0 the force is summed into
+    // the device sums after every `sample` steps (count a multiple of it,
+    // sample even).
+    void run(uint64_t count, uint32_t sample) {
+        if (members.empty() || count == 0) {
+            return;
+        }
+        if (stale() || (sample > 0 && flip != 0)) {
+            rebuild();
+        }
+        wait_members();
+        if (sample > 0) {
+            check(cudaMemsetAsync(sums, 0, members.size() * 6 * sizeof(double), stream), "batch sums");
+        }
+        // Graphs cover whole sampling periods: the largest multiple of
+        // `sample` up to kGraphSteps (at least one period).
+        const uint32_t period = sample > 0 ? std::max<uint32_t>(1u, kGraphSteps / sample) * sample
+                                           : kGraphSteps;
+        uint64_t done_steps = 0;
+        const auto single = [&]() {
+            launch_step();
+            ++done_steps;
+            if (sample > 0 && done_steps % sample == 0) {
+                launch_sample(true);
+            }
+        };
+        if (flip != 0) {
+            single();
+        }
+        if (count - done_steps >= period) {
+            if (!graph || graph_sample != sample || graph_steps != period) {
+                build_graph(sample, period);
+            }
+            while (count - done_steps >= period) {
+                check(cudaGraphLaunch(graph, stream), "batch graph launch");
+                launches += graph_launches;
+                done_steps += period;
+            }
+        }
+        while (done_steps < count) {
+            single();
+        }
+        release_members(count);
+    }
+
+    void check_status() {
+        uint32_t word = 0;
+        check(cudaMemcpyAsync(&word, status, sizeof(word), cudaMemcpyDeviceToHost, stream), "batch status");
+        check(cudaStreamSynchronize(stream), "batch status");
+        if (word != 0u) {
+            throw Refusal{ORR_ERR_TIMEOUT, "batch3d: a staged step gave up waiting for its row copies; the "
+                                        "members' populations are invalid until they are initialised"};
+        }
+    }
+
+    // Milliseconds per step of the current schedule over `graphs` graphs of
+    // kGraphSteps steps (after one untimed graph).
+    double time_schedule(uint32_t graphs) {
+        run(kGraphSteps, 0);
+        wait_members();
+        check(cudaEventRecord(t0, stream), "tune event");
+        for (uint32_t k = 0; k < graphs; ++k) {
+            run_graph_only();
+        }
+        check(cudaEventRecord(t1, stream), "tune event");
+        release_members(static_cast<uint64_t>(graphs) * kGraphSteps);
+        check(cudaEventSynchronize(t1), "tune event");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, t0, t1), "tune event");
+        return static_cast<double>(ms) / (static_cast<double>(graphs) * kGraphSteps);
+    }
+
+    void run_graph_only() {
+        if (!graph || graph_sample != 0 || graph_steps != kGraphSteps) {
+            build_graph(0, kGraphSteps);
+        }
+        check(cudaGraphLaunch(graph, stream), "batch graph launch");
+        launches += graph_launches;
+    }
+};
+

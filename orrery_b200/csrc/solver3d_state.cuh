@@ -214,7 +214,7 @@ struct orr_lbm3d {
               "status read-back");
         check(cudaStreamSynchronize(stream), "status read-back");
         if (*word != 0u) {
-            throw Refusal{ORR_ERR_CUDA, "lbm3d gpu: a staged step gave up waiting for its row copies; "
+            throw Refusal{ORR_ERR_TIMEOUT, "lbm3d gpu: a staged step gave up waiting for its row copies; "
                                         "the populations are invalid until initialize"};
         }
     }

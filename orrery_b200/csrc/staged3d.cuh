@@ -94,14 +94,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
                  : "memory");
 }
 
+// One poll of the phase of `parity`; if it has not completed, the thread may
+// sleep until it completes or about kSuspendNs nanoseconds pass (the hint of
+// mbarrier.try_wait), instead of spinning on the barrier.
+constexpr uint32_t kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "n"(kSuspendNs)
         : "memory");
     return done != 0;
 }
@@ -111,17 +115,20 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // Waits for the phase of `parity` to complete, giving up after a bounded
-// number of polls (each poll may suspend the thread for a short while) or
+// number of polls (each sleeps at most kSuspendNs: about 1.3 s in all) or
 // when another warp has raised the CTA's abort word.
-constexpr uint32_t kWaitPolls = 1u << 20;
+constexpr uint32_t kWaitPolls = 1u << 16;
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
                                                   const volatile uint32_t* abort_word) {
+    if (mbar_try_wait(bar, parity)) {
+        return true;
+    }
     for (uint32_t k = 0; k < kWaitPolls; ++k) {
-        if (mbar_try_wait(bar, parity)) {
-            return true;
-        }
         if (*abort_word != 0u) {
             return false;
+        }
+        if (mbar_try_wait(bar, parity)) {
+            return true;
         }
     }
     return false;
@@ -280,13 +287,9 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
 
-    const auto lattice = [&](uint32_t l) -> const Lattice3D<A>& {
-        if constexpr (kSingle) {
-            return one;
-        } else {
-            return lats[l];
-        }
-    };
+    // Entries: the by-value parameter (its address is in the constant
+    // bank) or the device table.
+    const Lattice3D<A>* const table = kSingle ? &one : lats;
 
     if (tid == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             }
             const uint32_t k = blockIdx.x + j * G;
             const uint32_t l = kSingle ? 0u : find_lattice<A, true>(lats, n, k);
-            const Lattice3D<A>& L = lattice(l);
+            const Lattice3D<A>& L = table[kSingle ? 0u : l];
             const uint32_t tiles = L.g.tiles_x;
             const uint32_t local = k - static_cast<uint32_t>(L.staged_begin);
             const uint32_t t = local % tiles;
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
         // ---- consumer warps: direct items first, while the first stages load
         for (uint32_t d = blockIdx.x; d < direct_total; d += G) {
             const uint32_t l = kSingle ? 0u : find_lattice<A, false>(lats, n, d);
-            const Lattice3D<A>& L = lattice(l);
+            const Lattice3D<A>& L = table[kSingle ? 0u : l];
             const uint32_t tiles = L.g.tiles_x;
             const uint32_t local = d - static_cast<uint32_t>(L.direct_begin);
             const uint32_t x = (local % tiles) * B + tid;
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             if (lane == 0) {
                 mbar_arrive(smem_u32(empty + s));
             }
-            const Lattice3D<A>& L = lattice(it.x);
+            const Lattice3D<A>& L = table[kSingle ? 0u : it.x];
             const uint32_t x = it.y * B + tid;
             if (x < L.g.nx) {
                 const uint32_t from = L.parity ^ flip;

@@ -1,0 +1,124 @@
+"""Serving of drag solves with continuous batching (orr_serve_*).
+
+A solve's result must be the same served alone and served in a mix of
+requests that arrive while it runs (bit for bit: members of a batch do not
+interact and the force sums have a fixed order), the convergence rule must
+be the window-mean rule the reference adapter's sampling gives, admission
+must respect the device-memory budget, and bad requests are refused.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from orrery_b200 import solver as S
+from orrery_b200 import workloads as W
+from orrery_b200.lbm3d import XBoundary
+from orrery_b200.serve import Server
+
+pytestmark = pytest.mark.gpu
+
+CHUNK = 100
+WINDOW = 200
+TOL = 2e-3
+CAP = 3000
+
+
+def small(seed, nx=64, ny=32, nz=32, reynolds=60.0, diameter=8.0):
+    return W.sphere3d(seed=seed, nx=nx, ny=ny, nz=nz, diameter=diameter, reynolds=reynolds)
+
+
+def serve(workloads, storage="f32", delays=None, **opts):
+    with Server(storage=storage, chunk_steps=CHUNK, sample_every=10, **opts) as srv:
+        ids = []
+        for k, w in enumerate(workloads):
+            if delays is not None:
+                time.sleep(delays[k])
+            ids.append(srv.submit(w, window=WINDOW, tolerance=TOL, max_steps=CAP))
+        srv.drain(timeout=600)
+        return [srv.poll(i) for i in ids], srv.stats()
+
+
+def test_results_alone_and_in_mix_are_identical():
+    target = small(7)
+    alone, _ = serve([target])
+    others = [small(11, nx=96, ny=40, nz=40, reynolds=80.0), small(12, nx=48, ny=24, nz=24),
+              small(13, nx=80, ny=32, nz=48, reynolds=100.0)]
+    # The target arrives between the others, some while they already run.
+    mixed, stats = serve([others[0], others[1], target, others[2]], delays=[0.0, 0.0, 0.05, 0.02])
+    a, b = alone[0], mixed[2]
+    assert a["state"] in ("converged", "capped")
+    for key in ("state", "steps", "cd", "cl", "cm", "delta_cd"):
+        assert a[key] == b[key], (key, a[key], b[key])
+    assert a["force"] == b["force"] and a["moment"] == b["moment"]
+    assert stats["completed"] == 4 and stats["failed"] == 0
+    assert stats["mean_active"] > 1.0          # the requests overlapped on the device
+    assert 0 < stats["latency_p50_s"] <= stats["latency_p99_s"]
+    assert stats["solves_per_second"] > 0
+
+
+def test_window_rule_matches_a_plain_solver_loop():
+    """The served steps and window-mean Cd follow the rule run by hand on a
+    plain solver (force every 10 steps, window means, |delta Cd| < tol)."""
+    w = small(21)
+    served, _ = serve([w])
+    r = served[0]
+    s = S.make_gpu_solver(w.config, w.mask)
+    s.initialize(w.rho, w.ux, w.uy, w.uz)
+    q = 0.5 * w.config.inlet_ux ** 2 * w.reference_area
+    steps, prev, cd, state = 0, None, None, None
+    while state is None:
+        acc = np.zeros(6)
+        for _ in range(WINDOW // 10):
+            s.step(10)
+            f = s.force()
+            acc += np.concatenate([f.force, f.moment])
+        steps += WINDOW
+        cd = acc[0] / (WINDOW // 10) / q
+        if prev is not None and abs(cd - prev) < TOL:
+            state = "converged"
+        elif steps >= CAP:
+            state = "capped"
+        prev = cd
+    assert r["state"] == state
+    assert r["steps"] == steps
+    assert r["cd"] == pytest.approx(cd, rel=1e-10)
+
+
+def test_memory_budget_admission():
+    ws = [small(31), small(32), small(33)]
+    need = max(S.memory_bytes(w.config, 40000, 0, "f32") for w in ws)
+    # Room for one lattice at a time.
+    results, stats = serve(ws, memory_budget=int(need * 1.5))
+    assert all(r["state"] in ("converged", "capped") for r in results)
+    assert stats["peak_device_bytes"] <= int(need * 1.5)
+    assert stats["mean_active"] == pytest.approx(1.0)
+    # Admitted one after another: each starts after the previous finished.
+    assert results[1]["admitted_s"] >= results[0]["finished_s"] - 1e-3
+    big = small(34, nx=128, ny=64, nz=64)
+    res, _ = serve([big], memory_budget=int(need * 1.5))
+    assert res[0]["state"] == "failed" and "budget" in res[0]["message"]
+
+
+def test_fp16_served_close_to_fp32():
+    w = small(41)
+    r32, _ = serve([w], storage="f32")
+    r16, _ = serve([w], storage="f16")
+    assert r16[0]["state"] != "failed"
+    if r16[0]["steps"] == r32[0]["steps"]:
+        assert abs(r16[0]["cd"] - r32[0]["cd"]) / abs(r32[0]["cd"]) < 5e-3
+
+
+def test_refusals():
+    w = small(51)
+    with Server(chunk_steps=CHUNK, sample_every=10) as srv:
+        with pytest.raises(S.LbmError):
+            srv.submit(w, window=150)            # not a multiple of the chunk
+        with pytest.raises(S.LbmError):
+            srv.submit(w, tolerance=0.0)
+        bad = small(52)
+        bad.config.x_boundary = XBoundary.periodic
+        with pytest.raises(S.LbmError):
+            srv.submit(bad)
+    with pytest.raises(S.LbmError):
+        Server(chunk_steps=105, sample_every=10)
