@@ -194,6 +194,7 @@ def main(argv=None) -> int:
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
     ap.add_argument("--stages", type=int, default=0)
+    ap.add_argument("--npt", type=int, default=0, help="staged kernel: nodes per thread of a span")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"])
     ap.add_argument("--lattices", type=int, default=64, help="batched form: lattices")
     ap.add_argument("--requests", type=int, default=48, help="serve form: requests")
@@ -230,7 +231,8 @@ def main(argv=None) -> int:
 
     w = W.sphere3d(seed=1 + rank)
     solver = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank,
-                               block_x=args.block, kernel=args.kernel, stages=args.stages)
+                               block_x=args.block, kernel=args.kernel, stages=args.stages,
+                               nodes_per_thread=args.npt)
     kinfo = solver.kernel_info()
     solver.initialize(w.rho, w.ux, w.uy, w.uz)
     stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local_rank))
@@ -286,7 +288,7 @@ def main(argv=None) -> int:
         barrier()
         t0 = time.perf_counter()
         s2 = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank, block_x=args.block,
-                               kernel=args.kernel, stages=args.stages)
+                               kernel=args.kernel, stages=args.stages, nodes_per_thread=args.npt)
         s2.initialize(w.rho, w.ux, w.uy, w.uz)
         samples = 0
         for _ in range(args.e2e_steps // 10):

@@ -111,6 +111,7 @@ typedef struct orr_solver_options {
     int32_t block_x;          /* threads per block of the step kernel; 0 = tuned default */
     int32_t kernel;           /* ORR_KERNEL_*: the D3Q19 step kernel (0 = automatic) */
     int32_t stages;           /* pipeline stages of ORR_KERNEL_STAGED; 0 = tuned default */
+    int32_t nodes_per_thread; /* ORR_KERNEL_STAGED: 1 or 2 nodes per thread of a span; 0 = default */
 } orr_solver_options;
 
 /* D3Q19 step kernels.  ROWS: one block per row tile, every population read
@@ -158,7 +159,8 @@ ORR_API const char* orr_lbm3d_last_error(const orr_lbm3d* solver);
  * reference, whose GL backend has one dispatch shape): kernel ORR_KERNEL_ROWS
  * or ORR_KERNEL_STAGED, threads per CTA, pipeline stages and shared bytes
  * per CTA (staged), CTAs per launch, resident CTAs per SM (staged),
- * registers per thread, and the staged / per-node work items. */
+ * registers per thread, nodes per consumer thread of a staged span, and the
+ * staged / per-node work items. */
 typedef struct orr_kernel_info {
     int32_t kernel;
     uint32_t block;
@@ -167,7 +169,7 @@ typedef struct orr_kernel_info {
     int32_t ctas_per_sm;
     int32_t registers;
     uint32_t shared_bytes;
-    uint32_t reserved;
+    uint32_t nodes_per_thread;
     uint64_t staged_items;
     uint64_t direct_items;
 } orr_kernel_info;
@@ -255,6 +257,10 @@ typedef struct orr_batch_schedule {
     uint32_t block;
     uint32_t stages;
     uint32_t grid;
+    uint32_t nodes_per_thread;   /* staged: 1 or 2 (0 = default) */
+    uint32_t branches;           /* 0: as above; n > 0: each member runs its own single-lattice
+                                    launches (staged: a grid proportional to its nodes), the
+                                    members spread over n parallel graph branches */
     double ms_per_step;
 } orr_batch_schedule;
 

@@ -81,20 +81,22 @@ KERNEL_NAMES = {"auto": ORR_KERNEL_AUTO, "rows": ORR_KERNEL_ROWS, "staged": ORR_
 class CKernelInfo(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("block", ctypes.c_uint32), ("stages", ctypes.c_uint32),
                 ("grid", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_int32), ("registers", ctypes.c_int32),
-                ("shared_bytes", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("shared_bytes", ctypes.c_uint32), ("nodes_per_thread", ctypes.c_uint32),
                 ("staged_items", ctypes.c_uint64), ("direct_items", ctypes.c_uint64)]
 
 
 class CSolverOptions(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int32), ("allow_high_mach", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("block_x", ctypes.c_int32),
-                ("kernel", ctypes.c_int32), ("stages", ctypes.c_int32)]
+                ("kernel", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("nodes_per_thread", ctypes.c_int32)]
 
 
 class CBatchSchedule(ctypes.Structure):
     """orr_batch_schedule."""
     _fields_ = [("kernel", ctypes.c_int32), ("block", ctypes.c_uint32), ("stages", ctypes.c_uint32),
-                ("grid", ctypes.c_uint32), ("ms_per_step", ctypes.c_double)]
+                ("grid", ctypes.c_uint32), ("nodes_per_thread", ctypes.c_uint32), ("branches", ctypes.c_uint32),
+                ("ms_per_step", ctypes.c_double)]
 
 
 class CServeOptions(ctypes.Structure):

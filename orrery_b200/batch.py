@@ -23,7 +23,8 @@ _KERNELS = {v: n for n, v in abi.KERNEL_NAMES.items()}
 
 def _schedule_dict(s: abi.CBatchSchedule) -> dict:
     return {"kernel": _KERNELS.get(s.kernel, str(s.kernel)), "block": s.block, "stages": s.stages,
-            "grid": s.grid, "ms_per_step": s.ms_per_step}
+            "nodes_per_thread": s.nodes_per_thread, "branches": s.branches, "grid": s.grid,
+            "ms_per_step": s.ms_per_step}
 
 
 class CudaBatch3D:
@@ -69,11 +70,14 @@ class CudaBatch3D:
         self._check(self._lib.orr_batch3d_size(self._h, ctypes.byref(n), ctypes.byref(cells)))
         return n.value, cells.value
 
-    def set_schedule(self, kernel: str = "staged", block: int = 256, stages: int = 0) -> None:
+    def set_schedule(self, kernel: str = "staged", block: int = 256, stages: int = 0,
+                     nodes_per_thread: int = 0, branches: int = 0) -> None:
         s = abi.CBatchSchedule()
         s.kernel = abi.KERNEL_NAMES[kernel]
         s.block = int(block)
         s.stages = int(stages)
+        s.nodes_per_thread = int(nodes_per_thread)
+        s.branches = int(branches)
         self._check(self._lib.orr_batch3d_set_schedule(self._h, ctypes.byref(s)))
 
     def schedule(self) -> dict:

@@ -173,6 +173,9 @@ orr_status orr_batch3d_set_schedule(orr_batch3d* batch, const orr_batch_schedule
             if (s.stages > kMaxStages) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: stages must be 0 (tuned) or 1 to 8"};
             }
+            if (s.nodes_per_thread > 2) {
+                throw Refusal{ORR_ERR_INVALID, "batch3d: nodes_per_thread must be 0 (default), 1 or 2"};
+            }
         } else if (s.kernel == ORR_KERNEL_ROWS) {
             if (s.block == 0 || s.block > 256 || s.block % 32 != 0) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the row step takes a block of 32 to 256 threads"};
@@ -183,6 +186,8 @@ orr_status orr_batch3d_set_schedule(orr_batch3d* batch, const orr_batch_schedule
         b->kernel = s.kernel;
         b->block = s.block;
         b->stages = s.kernel == ORR_KERNEL_STAGED ? s.stages : 0;
+        b->npt = s.kernel == ORR_KERNEL_STAGED ? s.nodes_per_thread : 0;
+        b->branches = s.branches;
         b->dirty = true;
         return ORR_OK;
     });
@@ -197,6 +202,10 @@ orr_status orr_batch3d_schedule(const orr_batch3d* batch, orr_batch_schedule* sc
     s.block = batch->block;
     s.stages = batch->kernel == ORR_KERNEL_STAGED ? (batch->shape.stages ? batch->shape.stages : batch->stages) : 0;
     s.grid = batch->kernel == ORR_KERNEL_STAGED ? batch->shape.grid : 0;
+    s.nodes_per_thread = batch->kernel == ORR_KERNEL_STAGED
+                             ? (batch->shape.npt && !batch->dirty ? batch->shape.npt : batch->npt)
+                             : 0;
+    s.branches = batch->branches;
     s.ms_per_step = 0.0;
     *schedule = s;
     return ORR_OK;
@@ -276,12 +285,14 @@ orr_status orr_batch3d_tune(orr_batch3d* batch, uint32_t graphs_per_trial, orr_b
         uint32_t n = 0;
         for (const Candidate& c : kCandidates) {
             if (c.kernel == ORR_KERNEL_STAGED &&
-                b->ops->staged_occupancy(b->smag, c.block, c.stages) <= 0) {
+                b->ops->staged_occupancy(b->smag, c.block, c.npt, c.stages) <= 0) {
                 continue;
             }
             b->kernel = c.kernel;
             b->block = c.block;
             b->stages = c.stages;
+            b->npt = c.npt;
+            b->branches = c.branches;
             b->dirty = true;
             const double ms = b->time_schedule(graphs);
             if (trials != nullptr && n < capacity) {
@@ -289,6 +300,8 @@ orr_status orr_batch3d_tune(orr_batch3d* batch, uint32_t graphs_per_trial, orr_b
                 t.kernel = c.kernel;
                 t.block = c.block;
                 t.stages = c.stages;
+                t.nodes_per_thread = c.npt;
+                t.branches = c.branches;
                 t.grid = c.kernel == ORR_KERNEL_STAGED ? b->shape.grid : 0;
                 t.ms_per_step = ms;
             }
@@ -301,6 +314,8 @@ orr_status orr_batch3d_tune(orr_batch3d* batch, uint32_t graphs_per_trial, orr_b
         b->kernel = pick.kernel;
         b->block = pick.block;
         b->stages = pick.stages;
+        b->npt = pick.npt;
+        b->branches = pick.branches;
         b->dirty = true;
         if (count) *count = n;
         return ORR_OK;

@@ -15,16 +15,21 @@
 
 namespace orr {
 
-// Candidate schedules of the autotuner (kernel, block, stages).
+// Candidate schedules of the autotuner (kernel, block, stages, nodes per
+// thread of a staged span, graph branches; 64 branches means one per member
+// up to 64).
 struct Candidate {
     int32_t kernel;
     uint32_t block;
     uint32_t stages;
+    uint32_t npt;
+    uint32_t branches;
 };
 inline constexpr Candidate kCandidates[] = {
-    {ORR_KERNEL_STAGED, 256, 2}, {ORR_KERNEL_STAGED, 256, 3}, {ORR_KERNEL_STAGED, 256, 4},
-    {ORR_KERNEL_STAGED, 128, 2}, {ORR_KERNEL_STAGED, 128, 4}, {ORR_KERNEL_ROWS, 128, 0},
-    {ORR_KERNEL_ROWS, 256, 0},
+    {ORR_KERNEL_STAGED, 256, 3, 2, 0},  {ORR_KERNEL_STAGED, 256, 2, 1, 0},
+    {ORR_KERNEL_STAGED, 256, 2, 2, 64}, {ORR_KERNEL_STAGED, 256, 3, 2, 64},
+    {ORR_KERNEL_STAGED, 256, 4, 1, 64}, {ORR_KERNEL_STAGED, 128, 3, 2, 64},
+    {ORR_KERNEL_ROWS, 128, 0, 0, 0},    {ORR_KERNEL_ROWS, 128, 0, 0, 64},
 };
 
 } // namespace orr
@@ -44,7 +49,22 @@ struct orr_batch3d {
     int32_t kernel = ORR_KERNEL_STAGED;
     uint32_t block = 256;
     uint32_t stages = 0;      // 0: the shape's default
+    uint32_t npt = 0;         // nodes per thread of a staged span, 0: the storage's default
+    uint32_t branches = 0;    // 0: one stream; else members spread over this many graph branches
     StagedShape shape{};
+
+    // Branched schedule: member k runs its own single-lattice launches (its
+    // entry solo[k], items solo_items[k], grid solo_grid[k]) on branch
+    // stream lane_of[k]; a fork event starts the branches, join events end
+    // them.
+    std::vector<cudaStream_t> branch_streams;
+    std::vector<cudaEvent_t> join_events;
+    cudaEvent_t fork_event = nullptr;
+    std::vector<unsigned char> solo;
+    std::size_t solo_stride = 0;
+    std::vector<ItemCounts> solo_items;
+    std::vector<uint32_t> solo_grid;
+    std::vector<uint32_t> lane_of;
 
     // State of the current table: parities and epochs of the members when it
     // was built, and the steps taken since (mod 2).
@@ -84,6 +104,12 @@ struct orr_batch3d {
         if (graph) cudaGraphExecDestroy(graph);
         for (cudaEvent_t e : member_events) cudaEventDestroy(e);
         member_events.clear();
+        for (cudaEvent_t e : join_events) cudaEventDestroy(e);
+        join_events.clear();
+        for (cudaStream_t s : branch_streams) cudaStreamDestroy(s);
+        branch_streams.clear();
+        if (fork_event) cudaEventDestroy(fork_event);
+        fork_event = nullptr;
         for (void* p : {table, static_cast<void*>(status), jobs, static_cast<void*>(partial),
                         static_cast<void*>(sums)}) {
             if (p) cudaFree(p);
@@ -158,7 +184,7 @@ struct orr_batch3d {
             L.parity = static_cast<uint32_t>(m->cur);
             L.staged = stageable(m->g) ? 1u : 0u;
         }
-        items = number_items(lats.data(), lats.size(), block);
+        items = number_items(lats.data(), lats.size(), block, shape.npt);
         host_table.resize(lats.size() * sizeof(Lattice3D<A>));
         std::memcpy(host_table.data(), lats.data(), host_table.size());
         grow_bytes(table, table_bytes, lats.size() * sizeof(Lattice3D<A>), "batch table");
@@ -183,7 +209,7 @@ struct orr_batch3d {
             return;
         }
         if (kernel == ORR_KERNEL_STAGED) {
-            shape = staged_shape(*ops, smag, block, stages, device);
+            shape = staged_shape(*ops, smag, block, npt ? npt : default_npt(storage), stages, device);
             if (shape.per_sm <= 0) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the staged step cannot launch with this shape"};
             }
@@ -195,7 +221,17 @@ struct orr_batch3d {
                 fill_table(lats);
             }
             const uint64_t most = std::max<uint64_t>({items.staged, items.direct, 1});
+            if (branches > 0) {
+                if (storage == ORR_STORAGE_F64) {
+                    fill_solo<double>();
+                } else {
+                    fill_solo<float>();
+                }
+            }
             shape.grid = static_cast<uint32_t>(std::min<uint64_t>(shape.grid, most));
+        }
+        if (branches > 0) {
+            assign_lanes();
         }
         // Force jobs read the buffer that is current at flip 0 (sampling at
         // even step counts only).
@@ -225,12 +261,108 @@ struct orr_batch3d {
         dirty = false;
     }
 
+    bool branched() const { return branches > 0; }
+
+    // Per-member single-lattice entries of the branched staged schedule; each
+    // member's grid is its share of the whole launch's CTAs by node count.
+    template <class A> void fill_solo() {
+        const std::size_t n = members.size();
+        solo_stride = sizeof(Lattice3D<A>);
+        solo.assign(n * solo_stride, 0);
+        solo_items.assign(n, ItemCounts{});
+        solo_grid.assign(n, 1);
+        const auto* all = reinterpret_cast<const Lattice3D<A>*>(host_table.data());
+        double total = 0.0;
+        for (const orr_lbm3d* m : members) total += static_cast<double>(m->g.cells);
+        for (std::size_t k = 0; k < n; ++k) {
+            Lattice3D<A> L = all[k];
+            solo_items[k] = number_items(&L, 1, shape.block, shape.npt);
+            std::memcpy(solo.data() + k * solo_stride, &L, sizeof(L));
+            const double share = static_cast<double>(members[k]->g.cells) / total;
+            const uint64_t g = static_cast<uint64_t>(std::lround(share * shape.grid));
+            const uint64_t most = std::max<uint64_t>({solo_items[k].staged, solo_items[k].direct, 1});
+            solo_grid[k] = static_cast<uint32_t>(std::clamp<uint64_t>(g, 1, most));
+        }
+    }
+
+    // Members to branches: largest first, each to the least-loaded branch.
+    void assign_lanes() {
+        const std::size_t n = members.size();
+        const std::size_t lanes = std::min<std::size_t>(branches, n);
+        while (branch_streams.size() < lanes) {
+            cudaStream_t s = nullptr;
+            check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "batch branch stream");
+            branch_streams.push_back(s);
+            cudaEvent_t e = nullptr;
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch branch event");
+            join_events.push_back(e);
+        }
+        if (fork_event == nullptr) {
+            check(cudaEventCreateWithFlags(&fork_event, cudaEventDisableTiming), "batch branch event");
+        }
+        std::vector<std::size_t> order(n);
+        for (std::size_t k = 0; k < n; ++k) order[k] = k;
+        std::sort(order.begin(), order.end(),
+                  [&](std::size_t a, std::size_t b) { return members[a]->g.cells > members[b]->g.cells; });
+        std::vector<double> load(lanes, 0.0);
+        lane_of.assign(n, 0);
+        for (std::size_t k : order) {
+            const std::size_t lane =
+                static_cast<std::size_t>(std::min_element(load.begin(), load.end()) - load.begin());
+            lane_of[k] = static_cast<uint32_t>(lane);
+            load[lane] += static_cast<double>(members[k]->g.cells);
+        }
+    }
+
+    // `count` steps of every member on the branches: fork from the batch
+    // stream, each member's steps in order on its branch, join back.
+    void launch_branched(uint32_t count) {
+        const std::size_t lanes = std::min<std::size_t>(branches, members.size());
+        check(cudaEventRecord(fork_event, stream), "batch fork");
+        for (std::size_t b = 0; b < lanes; ++b) {
+            check(cudaStreamWaitEvent(branch_streams[b], fork_event, 0), "batch fork");
+        }
+        for (uint32_t step = 0; step < count; ++step) {
+            for (std::size_t k = 0; k < members.size(); ++k) {
+                orr_lbm3d* m = members[k];
+                cudaStream_t s = branch_streams[lane_of[k]];
+                const uint32_t from = static_cast<uint32_t>(parity[k]) ^ flip;
+                if (kernel == ORR_KERNEL_STAGED) {
+                    // The entry's parity is the member's at the rebuild:
+                    // its source is f[parity ^ flip].
+                    check(ops->staged(solo.data() + k * solo_stride, nullptr, 1, solo_items[k].staged,
+                                      solo_items[k].direct, flip, shape.stages, smag, shape.block, shape.npt,
+                                      solo_grid[k], status, s),
+                          "batch step kernel");
+                } else {
+                    check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
+                          "batch step kernel");
+                }
+                ++launches;
+            }
+            flip ^= 1u;
+        }
+        for (std::size_t b = 0; b < lanes; ++b) {
+            check(cudaEventRecord(join_events[b], branch_streams[b]), "batch join");
+            check(cudaStreamWaitEvent(stream, join_events[b], 0), "batch join");
+        }
+    }
+
+    // `count` steps of every member with the current schedule.
+    void launch_steps(uint32_t count) {
+        if (branched()) {
+            launch_branched(count);
+        } else {
+            for (uint32_t k = 0; k < count; ++k) launch_step();
+        }
+    }
+
     // One step of every member (flip = steps since the table, mod 2).
     void launch_step() {
         if (kernel == ORR_KERNEL_STAGED) {
             check(ops->staged(members.size() == 1 ? host_table.data() : nullptr, table,
                               static_cast<uint32_t>(members.size()), items.staged, items.direct, flip,
-                              shape.stages, smag, shape.block, shape.grid, status, stream),
+                              shape.stages, smag, shape.block, shape.npt, shape.grid, status, stream),
                   "batch step kernel");
             ++launches;
         } else {
@@ -263,11 +395,13 @@ struct orr_batch3d {
         const uint32_t flip_before = flip;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "batch graph capture");
         try {
-            for (uint32_t k = 0; k < steps; ++k) {
-                launch_step();
-                if (sample > 0 && (k + 1) % sample == 0) {
+            if (sample > 0) {
+                for (uint32_t k = 0; k < steps; k += sample) {
+                    launch_steps(sample);
                     launch_sample(true);
                 }
+            } else {
+                launch_steps(steps);
             }
         } catch (...) {
             cudaStreamEndCapture(stream, &captured);
@@ -290,7 +424,7 @@ struct orr_batch3d {
     uint64_t graph_launches = 0;
 
     uint64_t launches_per_step() const {
-        return kernel == ORR_KERNEL_STAGED ? 1 : members.size();
+        return kernel == ORR_KERNEL_STAGED && !branched() ? 1 : members.size();
     }
 
     void wait_members() {
@@ -330,7 +464,7 @@ struct orr_batch3d {
                                            : kGraphSteps;
         uint64_t done_steps = 0;
         const auto single = [&]() {
-            launch_step();
+            launch_steps(1);
             ++done_steps;
             if (sample > 0 && done_steps % sample == 0) {
                 launch_sample(true);

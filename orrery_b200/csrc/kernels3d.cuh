@@ -110,6 +110,28 @@ __device__ __forceinline__ double fast_sqrt(double x) {
 
 // ---------------------------------------------------------------- collide --
 
+// BGK relaxation of two opposite pairs of the shifted binary32 form in
+// packed lanes (FMUL2 / FFMA2 / FADD2 of sm_100, each lane rounded like the
+// scalar instruction): plus members (fa, fb) with c.u = cu, minus members
+// (fa1, fb1) with -cu; f += omega (f_eq - f) with f_eq - w = even +- odd,
+// even = w (base + 4.5 rho (c.u)^2), odd = 3 w rho c.u.
+__device__ __forceinline__ void relax_pairs2(float& fa, float& fb, float& fa1, float& fb1, float2 cu,
+                                             float2 w, float2 w3rho, float2 base2, float2 rho45_2,
+                                             float2 omega2) {
+    const float2 neg = make_float2(-1.0f, -1.0f);
+    const float2 even = __fmul2_rn(w, __ffma2_rn(rho45_2, __fmul2_rn(cu, cu), base2));
+    const float2 odd = __fmul2_rn(w3rho, cu);
+    const float2 eqp = __fadd2_rn(even, odd);
+    const float2 eqm = __ffma2_rn(odd, neg, even);
+    float2 P = make_float2(fa, fb), M = make_float2(fa1, fb1);
+    P = __ffma2_rn(omega2, __ffma2_rn(P, neg, eqp), P);
+    M = __ffma2_rn(omega2, __ffma2_rn(M, neg, eqm), M);
+    fa = P.x;
+    fb = P.y;
+    fa1 = M.x;
+    fb1 = M.y;
+}
+
 // BGK collision with Guo forcing and the optional Smagorinsky closure.
 // Shifted form: lbm3_collide (lbm_d3q19_common.glsl:261-326).
 // Unshifted binary64 form: collide (lbm3d_cpu.cpp:32-93), same operation order.
@@ -169,14 +191,27 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
         const A base = drho - A(1.5) * rho * uu;
         const A rho45 = A(4.5) * rho;
         f[0] += omega * (A(d3::w(0)) * base - f[0]);
-#pragma unroll
-        for (int i = 1; i < d3::Q; i += 2) {
-            const A w = A(d3::w(i));
-            const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
-            const A even = w * (base + rho45 * cu * cu);
-            const A odd = (A(3) * w * rho) * cu;
-            f[i] += omega * (even + odd - f[i]);
-            f[i + 1] += omega * (even - odd - f[i + 1]);
+        // Two opposite pairs at a time in packed binary32 lanes: plus
+        // members (f_a, f_b), minus members (f_a+1, f_b+1).  c.u is written
+        // out per direction (c components are 0 or +-1).
+        const float2 base2 = make_float2(base, base), rho45_2 = make_float2(rho45, rho45);
+        const float2 omega2 = make_float2(omega, omega);
+        constexpr float w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+        const float r3a = (3.0f * w1) * rho, r3b = (3.0f * w2) * rho;
+        relax_pairs2(f[1], f[3], f[2], f[4], make_float2(ux, uy), make_float2(w1, w1),
+                     make_float2(r3a, r3a), base2, rho45_2, omega2);
+        relax_pairs2(f[5], f[7], f[6], f[8], make_float2(uz, ux + uy), make_float2(w1, w2),
+                     make_float2(r3a, r3b), base2, rho45_2, omega2);
+        relax_pairs2(f[9], f[11], f[10], f[12], make_float2(ux - uy, ux + uz), make_float2(w2, w2),
+                     make_float2(r3b, r3b), base2, rho45_2, omega2);
+        relax_pairs2(f[13], f[15], f[14], f[16], make_float2(ux - uz, uy + uz), make_float2(w2, w2),
+                     make_float2(r3b, r3b), base2, rho45_2, omega2);
+        {
+            const A cu = uy - uz; // direction 17 (0, 1, -1)
+            const A even = A(w2) * (base + rho45 * cu * cu);
+            const A odd = r3b * cu;
+            f[17] += omega * (even + odd - f[17]);
+            f[18] += omega * (even - odd - f[18]);
         }
         if (forced) {
             const A scale = A(1) - A(0.5) * omega;
@@ -546,6 +581,32 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
     }
 }
 
+// Convective outlet at x = nx - 1 (outlet_value, lbm3d_cpu.cpp:239-250): the
+// zero-gradient copies in f (c_x < 0) are blended with the node's history;
+// nothing for the extrapolation outlet.
+template <class S>
+__device__ __forceinline__ void convective_blend3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                                  const StepBuffers3D& b, uint32_t y, uint32_t z,
+                                                  typename Storage<S>::A (&f)[d3::Q]) {
+    using A = typename Storage<S>::A;
+    if (g.outlet_mode != ORR_OUTLET_CONVECTIVE) {
+        return;
+    }
+    A* hist = static_cast<A*>(b.hist);
+    const A u = p.outlet_speed;
+    const uint64_t at = static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
+    const uint64_t face = static_cast<uint64_t>(g.ny) * g.nz;
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        if (d3::cx(i) < 0) {
+            const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
+            const A v = (hist[k] + u * f[i]) / (A(1) + u);
+            hist[k] = v;
+            f[i] = v;
+        }
+    }
+}
+
 // Fix-ups of a bulk node after its 19 plain pulls f_i = f*_i(x - c_i).  The
 // x-edge lanes of an interior row (two per row) read their c_x != 0 sources
 // again: x = -1 wraps to nx - 1 (periodic) or is an inlet unknown, rebuilt by
@@ -583,21 +644,8 @@ __device__ __forceinline__ void bulk_edges3(const Geom3D& g, const Phys3D<typena
             }
         }
     }
-    if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW && g.outlet_mode == ORR_OUTLET_CONVECTIVE) {
-        // Convective outlet (outlet_value, lbm3d_cpu.cpp:239-250).
-        A* hist = static_cast<A*>(b.hist);
-        const A u = p.outlet_speed;
-        const uint64_t at = static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
-        const uint64_t face = static_cast<uint64_t>(g.ny) * g.nz;
-#pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
-            if (d3::cx(i) < 0) {
-                const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
-                const A v = (hist[k] + u * f[i]) / (A(1) + u);
-                hist[k] = v;
-                f[i] = v;
-            }
-        }
+    if (xhi && g.x_mode == ORR_X_INFLOW_OUTFLOW) {
+        convective_blend3<S>(g, p, b, y, z, f);
     }
 }
 

@@ -24,18 +24,25 @@ struct ItemCounts {
     uint64_t direct = 0;
 };
 
-// Numbers the items of lattices[0, n) for tiles of `block` nodes: sets each
-// tiles_x and the prefix offsets, returns the totals.
-template <class A> ItemCounts number_items(Lattice3D<A>* lats, std::size_t n, uint32_t block) {
+// Numbers the items of lattices[0, n) for direct tiles of `block` nodes and
+// staged spans of block * npt nodes: sets each tiles_x, spans, magic and the
+// prefix offsets, returns the totals.
+template <class A>
+ItemCounts number_items(Lattice3D<A>* lats, std::size_t n, uint32_t block, uint32_t npt) {
     ItemCounts c;
+    const uint64_t span = static_cast<uint64_t>(block) * npt;
     for (std::size_t k = 0; k < n; ++k) {
         Lattice3D<A>& L = lats[k];
         L.g.tiles_x = (L.g.nx + block - 1) / block;
         const uint64_t tiles = L.g.tiles_x;
         L.staged_begin = c.staged;
         L.direct_begin = c.direct;
+        L.spans = 0;
+        L.magic = L.g.nx <= kMagicMaxNx ? static_cast<uint32_t>(((uint64_t{1} << 32) + L.g.nx - 1) / L.g.nx) : 0u;
         if (L.staged) {
-            c.staged += tiles * (L.g.ny - 2ull) * (L.g.nz - 2ull);
+            const uint64_t interior = static_cast<uint64_t>(L.g.nx) * (L.g.ny - 2ull);
+            L.spans = static_cast<uint32_t>((interior + span - 1) / span);
+            c.staged += static_cast<uint64_t>(L.spans) * (L.g.nz - 2ull);
             c.direct += tiles * (2ull * L.g.ny + 2ull * (L.g.nz - 2ull));
         } else {
             c.direct += tiles * L.g.ny * static_cast<uint64_t>(L.g.nz);
@@ -47,18 +54,20 @@ template <class A> ItemCounts number_items(Lattice3D<A>* lats, std::size_t n, ui
 // Launch shape of the persistent step.
 struct StagedShape {
     uint32_t block = 256;
+    uint32_t npt = 1;      // nodes per consumer thread of a span
     uint32_t stages = 0;
     uint32_t grid = 0;     // CTAs (resident CTAs per SM x SMs)
     int per_sm = 0;
 };
 
 // Picks the stages (the most, up to 4, that keep the register-limited
-// residency, unless `stages` is given) and the grid for `block`.  A shape
-// with per_sm == 0 cannot launch.
-inline StagedShape staged_shape(const Ops3D& ops, bool smag, uint32_t block, uint32_t stages,
+// residency, unless `stages` is given) and the grid for (block, npt).  A
+// shape with per_sm == 0 cannot launch.
+inline StagedShape staged_shape(const Ops3D& ops, bool smag, uint32_t block, uint32_t npt, uint32_t stages,
                                 int device) {
     StagedShape s;
     s.block = block;
+    s.npt = npt;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
@@ -66,13 +75,13 @@ inline StagedShape staged_shape(const Ops3D& ops, bool smag, uint32_t block, uin
     }
     if (stages != 0) {
         s.stages = stages;
-        s.per_sm = ops.staged_occupancy(smag, block, stages);
+        s.per_sm = ops.staged_occupancy(smag, block, npt, stages);
     } else {
-        const int best = ops.staged_occupancy(smag, block, 1);
+        const int best = ops.staged_occupancy(smag, block, npt, 1);
         s.stages = 2;
-        s.per_sm = ops.staged_occupancy(smag, block, 2);
+        s.per_sm = ops.staged_occupancy(smag, block, npt, 2);
         for (uint32_t k = 4; k > 2; --k) {
-            const int o = ops.staged_occupancy(smag, block, k);
+            const int o = ops.staged_occupancy(smag, block, npt, k);
             if (o == best && o > 0) {
                 s.stages = k;
                 s.per_sm = o;

@@ -36,20 +36,21 @@ struct Ops3D {
     int (*step_registers)(bool smag);
     // Persistent step over a device table of n Lattice3D entries of the
     // storage's arithmetic type (staged3d.cuh): `grid` CTAs of `block`
-    // consumer threads (128 or 256) plus a producer warp, `stages` pipeline
-    // stages, source buffer f[parity ^ flip] of every lattice.  With n == 1
-    // and `host_one` (a host copy of the entry) the entry is passed by value.
+    // consumer threads (128 or 256) plus a producer warp, spans of
+    // block * npt nodes (npt 1 or 2), `stages` pipeline stages, source buffer
+    // f[parity ^ flip] of every lattice.  With n == 1 and `host_one` (a host
+    // copy of the entry) the entry is passed by value.
     cudaError_t (*staged)(const void* host_one, const void* table, uint32_t n, uint64_t staged_items,
                           uint64_t direct_items, uint32_t flip, uint32_t stages, bool smag,
-                          uint32_t block, uint32_t grid, uint32_t* status, cudaStream_t s);
-    // Resident CTAs per SM of the persistent step for (smag, block, stages),
-    // after raising the kernel's dynamic shared-memory limit; 0 if it cannot
-    // launch.
-    int (*staged_occupancy)(bool smag, uint32_t block, uint32_t stages);
+                          uint32_t block, uint32_t npt, uint32_t grid, uint32_t* status, cudaStream_t s);
+    // Resident CTAs per SM of the persistent step for (smag, block, npt,
+    // stages), after raising the kernel's dynamic shared-memory limit; 0 if
+    // it cannot launch.
+    int (*staged_occupancy)(bool smag, uint32_t block, uint32_t npt, uint32_t stages);
     // Dynamic shared memory of the persistent step, bytes.
-    uint32_t (*staged_smem)(uint32_t block, uint32_t stages);
+    uint32_t (*staged_smem)(uint32_t block, uint32_t npt, uint32_t stages);
     // Registers per thread of the persistent step.
-    int (*staged_registers)(bool smag, uint32_t block);
+    int (*staged_registers)(bool smag, uint32_t block, uint32_t npt);
     // Momentum exchange of n lattices (device table of ForceJob, kernels3d.cuh)
     // summed in a fixed order: pass 1 over `chunks` link chunks into
     // `partial` (6 doubles per chunk), pass 2 into out[6 l ..] (added to it

@@ -84,56 +84,52 @@ template <class S> struct Launch3D {
         return e == cudaSuccess ? a.numRegs : -1;
     }
 
-    template <bool kSmag, int B, bool kSingle> static constexpr auto staged_kernel() {
-        return &step3d_staged_kernel<S, kSmag, B, kSingle>;
+    template <bool kSmag, int B, int NPT, bool kSingle> static constexpr auto staged_kernel() {
+        return &step3d_staged_kernel<S, kSmag, B, NPT, kSingle>;
+    }
+
+    // Calls f.template operator()<kSmag, B, NPT>() for a supported runtime
+    // shape (B 128 or 256, NPT 1 or 2); false otherwise.
+    template <class F> static bool with_shape(bool smag, uint32_t block, uint32_t npt, F&& f) {
+        const auto go = [&]<bool K>() {
+            if (block == 256 && npt == 1) { f.template operator()<K, 256, 1>(); return true; }
+            if (block == 256 && npt == 2) { f.template operator()<K, 256, 2>(); return true; }
+            if (block == 128 && npt == 1) { f.template operator()<K, 128, 1>(); return true; }
+            if (block == 128 && npt == 2) { f.template operator()<K, 128, 2>(); return true; }
+            return false;
+        };
+        return smag ? go.template operator()<true>() : go.template operator()<false>();
     }
 
     // One lattice (host_one non-null, n == 1) travels by value, so its fields
     // are constant-bank operands; otherwise the kernel reads the device table.
-    template <bool kSmag, int B>
-    static void launch_staged(const Lattice3D<A>* host_one, const Lattice3D<A>* lats, uint32_t n,
-                              uint32_t staged_items, uint32_t direct_items, uint32_t flip, uint32_t stages,
-                              uint32_t grid, uint32_t smem, uint32_t* status, cudaStream_t s) {
-        if (host_one != nullptr && n == 1) {
-            staged_kernel<kSmag, B, true>()<<<grid, kStagedThreads<B>, smem, s>>>(
-                *host_one, lats, n, staged_items, direct_items, flip, stages, status);
-        } else {
-            staged_kernel<kSmag, B, false>()<<<grid, kStagedThreads<B>, smem, s>>>(
-                Lattice3D<A>{}, lats, n, staged_items, direct_items, flip, stages, status);
-        }
-    }
-
     static cudaError_t staged(const void* host_one, const void* table, uint32_t n, uint64_t staged_items,
                               uint64_t direct_items, uint32_t flip, uint32_t stages, bool smag,
-                              uint32_t block, uint32_t grid, uint32_t* status, cudaStream_t s) {
+                              uint32_t block, uint32_t npt, uint32_t grid, uint32_t* status, cudaStream_t s) {
         if (stages == 0 || stages > kMaxStages || grid == 0 || staged_items >= (1ull << 31) ||
             direct_items >= (1ull << 31)) {
             return cudaErrorInvalidValue;
         }
         const auto* one = static_cast<const Lattice3D<A>*>(host_one);
         const auto* lats = static_cast<const Lattice3D<A>*>(table);
-        const uint32_t smem = staged_smem(block, stages);
         const auto si = static_cast<uint32_t>(staged_items), di = static_cast<uint32_t>(direct_items);
-        if (block == 256) {
-            if (smag) {
-                launch_staged<true, 256>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+        const bool ok = with_shape(smag, block, npt, [&]<bool K, int B, int NPT>() {
+            const uint32_t smem = staged_smem_bytes<S, B * NPT>(stages);
+            if (one != nullptr && n == 1) {
+                staged_kernel<K, B, NPT, true>()<<<grid, kStagedThreads<B>, smem, s>>>(
+                    *one, lats, n, si, di, flip, stages, status);
             } else {
-                launch_staged<false, 256>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
+                staged_kernel<K, B, NPT, false>()<<<grid, kStagedThreads<B>, smem, s>>>(
+                    Lattice3D<A>{}, lats, n, si, di, flip, stages, status);
             }
-        } else if (block == 128) {
-            if (smag) {
-                launch_staged<true, 128>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
-            } else {
-                launch_staged<false, 128>(one, lats, n, si, di, flip, stages, grid, smem, status, s);
-            }
-        } else {
-            return cudaErrorInvalidValue;
-        }
-        return cudaGetLastError();
+        });
+        return ok ? cudaGetLastError() : cudaErrorInvalidValue;
     }
 
-    static uint32_t staged_smem(uint32_t block, uint32_t stages) {
-        return block == 256 ? staged_smem_bytes<S, 256>(stages) : staged_smem_bytes<S, 128>(stages);
+    static uint32_t staged_smem(uint32_t block, uint32_t npt, uint32_t stages) {
+        uint32_t bytes = 0;
+        with_shape(false, block, npt, [&]<bool K, int B, int NPT>() { bytes = staged_smem_bytes<S, B * NPT>(stages); });
+        return bytes;
     }
 
     // The kernel's dynamic shared-memory limit is raised to the device's
@@ -164,37 +160,29 @@ template <class S> struct Launch3D {
 
     // Both variants (single and table) get the attribute; the occupancy is
     // the smaller of the two.
-    template <bool kSmag, int B> static int occupancy_both(uint32_t stages) {
-        const uint32_t smem = staged_smem_bytes<S, B>(stages);
-        const int a = occupancy_of(staged_kernel<kSmag, B, true>(), kStagedThreads<B>, smem);
-        const int b = occupancy_of(staged_kernel<kSmag, B, false>(), kStagedThreads<B>, smem);
-        return a < b ? a : b;
-    }
-
-    static int staged_occupancy(bool smag, uint32_t block, uint32_t stages) {
+    static int staged_occupancy(bool smag, uint32_t block, uint32_t npt, uint32_t stages) {
         if (stages == 0 || stages > kMaxStages) {
             return 0;
         }
-        if (block == 256) {
-            return smag ? occupancy_both<true, 256>(stages) : occupancy_both<false, 256>(stages);
-        }
-        if (block == 128) {
-            return smag ? occupancy_both<true, 128>(stages) : occupancy_both<false, 128>(stages);
-        }
-        return 0;
+        int result = 0;
+        with_shape(smag, block, npt, [&]<bool K, int B, int NPT>() {
+            const uint32_t smem = staged_smem_bytes<S, B * NPT>(stages);
+            const int a = occupancy_of(staged_kernel<K, B, NPT, true>(), kStagedThreads<B>, smem);
+            const int b = occupancy_of(staged_kernel<K, B, NPT, false>(), kStagedThreads<B>, smem);
+            result = a < b ? a : b;
+        });
+        return result;
     }
 
-    static int staged_registers(bool smag, uint32_t block) {
-        cudaFuncAttributes a{};
-        cudaError_t e = cudaErrorInvalidValue;
-        if (block == 256) {
-            e = smag ? cudaFuncGetAttributes(&a, staged_kernel<true, 256, true>())
-                     : cudaFuncGetAttributes(&a, staged_kernel<false, 256, true>());
-        } else if (block == 128) {
-            e = smag ? cudaFuncGetAttributes(&a, staged_kernel<true, 128, true>())
-                     : cudaFuncGetAttributes(&a, staged_kernel<false, 128, true>());
-        }
-        return e == cudaSuccess ? a.numRegs : -1;
+    static int staged_registers(bool smag, uint32_t block, uint32_t npt) {
+        int regs = -1;
+        with_shape(smag, block, npt, [&]<bool K, int B, int NPT>() {
+            cudaFuncAttributes a{};
+            if (cudaFuncGetAttributes(&a, staged_kernel<K, B, NPT, true>()) == cudaSuccess) {
+                regs = a.numRegs;
+            }
+        });
+        return regs;
     }
 
     static cudaError_t force_batch(const void* jobs, uint32_t n, uint64_t chunks, double* partial,

@@ -196,6 +196,9 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         if (o.stages < 0 || o.stages > static_cast<int32_t>(kMaxStages)) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: stages must be 0 (tuned) or 1 to 8"};
         }
+        if (o.nodes_per_thread < 0 || o.nodes_per_thread > 2) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: nodes_per_thread must be 0 (default), 1 or 2"};
+        }
         require_device(o.device);
         auto h = std::make_unique<orr_lbm3d>();
         h->device = o.device;
@@ -313,7 +316,9 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
                            (o.block_x == 0 || o.block_x == 128 || o.block_x == 256));
         if (want) {
             const uint32_t sblock = o.block_x == 128 ? 128u : 256u;
-            h->shape = staged_shape(*h->ops, h->smag, sblock, static_cast<uint32_t>(o.stages), o.device);
+            const uint32_t npt = o.nodes_per_thread > 0 ? static_cast<uint32_t>(o.nodes_per_thread)
+                                                        : default_npt(o.storage);
+            h->shape = staged_shape(*h->ops, h->smag, sblock, npt, static_cast<uint32_t>(o.stages), o.device);
             if (h->shape.per_sm <= 0) {
                 if (o.kernel == ORR_KERNEL_STAGED) {
                     throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step cannot launch with " +
@@ -586,8 +591,9 @@ orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info)
             k.stages = solver->shape.stages;
             k.grid = solver->shape.grid;
             k.ctas_per_sm = solver->shape.per_sm;
-            k.registers = solver->ops->staged_registers(solver->smag, solver->shape.block);
-            k.shared_bytes = solver->ops->staged_smem(solver->shape.block, solver->shape.stages);
+            k.registers = solver->ops->staged_registers(solver->smag, solver->shape.block, solver->shape.npt);
+            k.shared_bytes = solver->ops->staged_smem(solver->shape.block, solver->shape.npt, solver->shape.stages);
+            k.nodes_per_thread = solver->shape.npt;
             k.staged_items = solver->items.staged;
             k.direct_items = solver->items.direct;
         } else {

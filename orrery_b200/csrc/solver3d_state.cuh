@@ -65,6 +65,12 @@ inline const Ops3D& ops_for(int32_t storage) {
     }
 }
 
+// Nodes per consumer thread of a staged span when the caller leaves it open.
+inline uint32_t default_npt(int32_t storage) {
+    (void)storage;
+    return 1u;
+}
+
 inline float to_f32(double v) {
     return static_cast<float>(v);
 }
@@ -194,7 +200,7 @@ struct orr_lbm3d {
     void launch_step(int from) {
         if (persistent) {
             check(ops->staged(host_table, table, 1, items.staged, items.direct, static_cast<uint32_t>(from),
-                              shape.stages, smag, shape.block, shape.grid, status(), stream),
+                              shape.stages, smag, shape.block, shape.npt, shape.grid, status(), stream),
                   "step kernel");
         } else {
             check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream),
@@ -229,7 +235,7 @@ struct orr_lbm3d {
         L.f[1] = f[1];
         L.parity = 0;
         L.staged = stageable(g) ? 1u : 0u;
-        items = number_items(&L, 1, shape.block);
+        items = number_items(&L, 1, shape.block, shape.npt);
         static_assert(sizeof(Lattice3D<A>) <= kTableBytes, "table entry");
         std::memcpy(host_table, &L, sizeof(L));
         check(cudaMemcpyAsync(table, &L, sizeof(L), cudaMemcpyHostToDevice, stream), "table upload");

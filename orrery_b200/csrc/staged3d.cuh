@@ -2,27 +2,34 @@
 // every interior row tile staged in shared memory by bulk asynchronous
 // copies (cp.async.bulk, completion on an mbarrier).
 //
-// Work items.  A lattice's rows are cut into tiles of B nodes along x.
-//   staged items   tiles of interior rows (1 <= y <= ny-2, 1 <= z <= nz-2)
-//                  of a lattice whose rows are 16-node aligned: the 19 source
-//                  row segments f*_i(y - cy_i, z - cz_i, [x0 - H, x0 + B + H))
-//                  and the tile's class bytes arrive in one pipeline stage;
-//   direct items   every other tile (y or z face rows, and all rows of a
-//                  lattice that cannot be staged): the per-node gather of
-//                  step_node3 from global memory.
+// Work items.
+//   staged items   spans of N = NPT * B consecutive nodes (flattened order) of
+//                  the interior rows (1 <= y <= ny-2) of an interior z-plane
+//                  (1 <= z <= nz-2), for lattices whose rows are 16-node
+//                  aligned.  The pull sources of a span are contiguous in
+//                  every population plane: plane i needs
+//                  f*_i([c0 - o_i - H, c0 - o_i + N + H)), o_i = cx_i + nx cy_i +
+//                  nx ny cz_i, so one bulk copy per plane (the halo H covers
+//                  cx = +-1) and one for the span's class bytes fill a
+//                  pipeline stage.  A span may cover several short rows or
+//                  part of a long one; x-edge nodes take their fix-ups.
+//   direct items   every other row, in tiles of B nodes (the y and z face
+//                  rows, and all rows of a lattice that cannot be staged):
+//                  the per-node gather of step_node3 from global memory.
 // Items of all lattices are numbered globally (prefix offsets in the lattice
 // table) and CTA b takes items b, b + G, b + 2G, ... so that the CTAs in
-// flight work on neighbouring rows, as a one-shot grid would.
+// flight work on neighbouring spans, as a one-shot grid would.
 //
 // Pipeline.  A CTA has B consumer threads and one producer warp.  The
 // producer keeps up to `stages` items in flight: for each it waits until
 // every consumer warp has released the stage (the stage's empty mbarrier),
 // records the item, arms the stage's full mbarrier with the byte count, and
 // its lanes 0-18 copy one population plane's segment each, lane 19 the
-// class bytes.  Each consumer warp waits for the full barrier, reads its
-// nodes' 19 values and classes into registers, releases the stage (one
-// arrive per warp on the empty barrier) and finishes its nodes; consumer
-// warps never wait for each other.  The finish is the one of step_node3
+// class bytes.  Each consumer thread owns NPT nodes of the span (k = tid +
+// p B): it waits for the full barrier, and for each node reads the 19 values
+// and the class into registers and finishes the node; after its last
+// node's reads its warp releases the stage (one arrive per warp on the empty
+// barrier).  Consumer warps never wait for each other.  The finish is the one of step_node3
 // (x-edge fix-ups, bounce-back overrides from global memory for the rare
 // boundary nodes, inlet, collision, 19 stores), so a node's arithmetic does
 // not depend on which item or lattice mix carried it.
@@ -57,22 +64,28 @@ template <class A> struct Lattice3D {
     uint32_t staged;       // interior rows go through shared memory
     uint64_t staged_begin; // first global staged item of this lattice
     uint64_t direct_begin; // first global direct item of this lattice
+    uint32_t spans;        // staged spans per interior z-plane
+    uint32_t magic;        // ceil(2^32 / nx) when nx <= kMagicMaxNx (exact quotients n / nx, n < 2^16), else 0
 };
 
-// Shared memory of one pipeline stage: 19 segments of B + 2H values, then B
-// class bytes (every piece starts on a 16-byte boundary).
+// Shared memory of one pipeline stage: 19 segments of N + 2H values, then N
+// class bytes (every piece starts on a 16-byte boundary), N = NPT * B.
 template <class S> constexpr int kHalo = 16 / static_cast<int>(sizeof(S));
-template <class S, int B> constexpr uint32_t kSegment = B + 2 * kHalo<S>;
-template <class S, int B> constexpr uint32_t kPopBytes = d3::Q * kSegment<S, B> * sizeof(S);
-template <class S, int B> constexpr uint32_t kStageBytes = kPopBytes<S, B> + B;
+template <class S, int N> constexpr uint32_t kSegment = N + 2 * kHalo<S>;
+template <class S, int N> constexpr uint32_t kPopBytes = d3::Q * kSegment<S, N> * sizeof(S);
+template <class S, int N> constexpr uint32_t kStageBytes = kPopBytes<S, N> + N;
 
-template <class S, int B> constexpr uint32_t staged_smem_bytes(uint32_t stages) {
-    return kStagedHeader + stages * kStageBytes<S, B>;
+template <class S, int N> constexpr uint32_t staged_smem_bytes(uint32_t stages) {
+    return kStagedHeader + stages * kStageBytes<S, N>;
 }
 
-// Threads of a staged CTA: B consumers (one node of the tile each) and one
-// producer warp.
+// Threads of a staged CTA: B consumers and one producer warp.
 template <int B> constexpr int kStagedThreads = B + 32;
+
+// The largest nx with exact multiply-high quotients of span offsets: for
+// n < 2^16 and nx < 2^16, floor(n / nx) = umulhi(n, ceil(2^32 / nx)); span
+// offsets reach nx + N with N <= 1024.
+constexpr uint32_t kMagicMaxNx = 65536u - 1024u;
 
 // ----------------------------------------------------------- PTX helpers --
 
@@ -214,7 +227,10 @@ __device__ __forceinline__ void reflect_masked3(const Geom3D& g, const StepBuffe
     }
 }
 
-// Finish of a staged node: f holds the 19 plain pulls of the node.
+// Finish of a staged node: f holds the 19 plain pulls of the node, and for a
+// bulk node at the outlet (x = nx - 1, inflow / outflow) already the
+// zero-gradient copies of its c_x < 0 directions (the consumer loop takes
+// them from the stage).
 template <class S, bool kSmag>
 __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
                                              const StepBuffers3D& b, const S* __restrict__ src,
@@ -240,6 +256,8 @@ __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typen
         } else {
             reflect_masked3<S, 0>(g, b, src, mask, slot, here, f);
         }
+    } else if (x + 1u == g.nx && g.x_mode == ORR_X_INFLOW_OUTFLOW) {
+        convective_blend3<S>(g, p, b, y, z, f);
     } else {
         bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
     }
@@ -256,14 +274,11 @@ template <class S, int B> constexpr int kStagedMinBlocks =
 
 // The staged step.  kSingle: the one lattice is the by-value parameter `one`
 // (its fields are constant-bank operands); otherwise lattices come from the
-// device table `lats` of n entries.
-//
-// Warps 0 .. B/32-1 consume: each thread owns node x0 + tid of a tile.
-// Warp B/32 produces: for item j it waits until every consumer warp has
-// released stage j % stages (its empty barrier), records the item, arms the
-// full barrier with the stage's bytes and issues the 20 bulk copies.  There
-// is no block-wide barrier in the loop: consumer warps advance on their own.
-template <class S, bool kSmag, int B, bool kSingle>
+// device table `lats` of n entries.  B consumer threads, NPT nodes each per
+// span; warp B/32 produces (waits until every consumer warp has released
+// stage j % stages, records span j, arms the full barrier with the stage's
+// bytes and issues its 20 bulk copies).  No block-wide barrier in the loop.
+template <class S, bool kSmag, int B, int NPT, bool kSingle>
 __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
     step3d_staged_kernel(const __grid_constant__ Lattice3D<typename Storage<S>::A> one,
                          const Lattice3D<typename Storage<S>::A>* __restrict__ lats, uint32_t n,
@@ -272,9 +287,10 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
     using A = typename Storage<S>::A;
     using T = Storage<S>;
     constexpr int H = kHalo<S>;
-    constexpr uint32_t SEG = kSegment<S, B>;
-    constexpr uint32_t POP = kPopBytes<S, B>;
-    constexpr uint32_t STAGE = kStageBytes<S, B>;
+    constexpr uint32_t N = static_cast<uint32_t>(B * NPT);
+    constexpr uint32_t SEG = kSegment<S, N>;
+    constexpr uint32_t POP = kPopBytes<S, N>;
+    constexpr uint32_t STAGE = kStageBytes<S, N>;
     constexpr uint32_t kConsumerWarps = B / 32;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -286,7 +302,6 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
-
     // Entries: the by-value parameter (its address is in the constant
     // bank) or the device table.
     const Lattice3D<A>* const table = kSingle ? &one : lats;
@@ -310,7 +325,7 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
         uint32_t s = 0, phase = 0;
         for (uint32_t j = 0; j < count; ++j) {
             if (j >= stages) {
-                // Stage s last held item j - stages (use phase ^ 1 of the ring).
+                // Stage s last held span j - stages (phase ^ 1 of the ring).
                 if (!mbar_wait_bounded(smem_u32(empty + s), phase ^ 1u, abort_word)) {
                     if (lane == 0) {
                         *abort_word = 1u;
@@ -322,32 +337,30 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             const uint32_t k = blockIdx.x + j * G;
             const uint32_t l = kSingle ? 0u : find_lattice<A, true>(lats, n, k);
             const Lattice3D<A>& L = table[kSingle ? 0u : l];
-            const uint32_t tiles = L.g.tiles_x;
             const uint32_t local = k - static_cast<uint32_t>(L.staged_begin);
-            const uint32_t t = local % tiles;
-            const uint32_t r = local / tiles;
-            const uint32_t inner = L.g.ny - 2u;
-            const uint32_t y = 1u + r % inner;
-            const uint32_t z = 1u + r / inner;
+            const uint32_t zi = local / L.spans;
+            const uint32_t off = (local - zi * L.spans) * N;   // node offset in the plane's interior rows
+            const uint32_t nx = L.g.nx;
+            const uint32_t dy = off / nx;
+            const uint32_t x0 = off - dy * nx, y0 = 1u + dy, z = 1u + zi;
+            const uint64_t c0 = static_cast<uint64_t>(z) * L.g.plane + static_cast<uint64_t>(nx) * y0 + x0;
             const uint32_t bar = smem_u32(full + s);
             unsigned char* stage = ring + s * STAGE;
             if (lane == 0) {
-                info[s] = make_uint4(l, t, y, z);
+                info[s] = make_uint4(l, x0, y0, z);
                 mbar_expect_tx(bar, STAGE);
             }
             __syncwarp();
-            const uint64_t x0 = static_cast<uint64_t>(t) * B;
-            const uint64_t nx = L.g.nx, ny = L.g.ny;
             if (lane < static_cast<uint32_t>(d3::Q)) {
                 int cx, cy, cz;
                 c_rt(static_cast<int>(lane), cx, cy, cz);
                 const S* src = static_cast<const S*>(L.f[L.parity ^ flip]);
-                const uint64_t row = static_cast<uint64_t>(static_cast<int64_t>(y) - cy) +
-                                     ny * static_cast<uint64_t>(static_cast<int64_t>(z) - cz);
-                const S* from = src + static_cast<uint64_t>(lane) * L.g.cells + row * nx + x0 - H;
+                const int64_t shift = static_cast<int64_t>(nx) * cy + static_cast<int64_t>(L.g.plane) * cz + H;
+                const S* from = src + static_cast<uint64_t>(lane) * L.g.cells +
+                                static_cast<uint64_t>(static_cast<int64_t>(c0) - shift);
                 bulk_load(smem_u32(stage + lane * SEG * sizeof(S)), from, SEG * sizeof(S), bar);
             } else if (lane == static_cast<uint32_t>(d3::Q)) {
-                bulk_load(smem_u32(stage + POP), L.b.cls + (x0 + nx * (y + ny * z)), B, bar);
+                bulk_load(smem_u32(stage + POP), L.b.cls + c0, N, bar);
             }
             if (lane == 0) {
                 *issued_word = j + 1u;
@@ -385,22 +398,41 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             const unsigned char* stage = ring + s * STAGE;
             const uint4 it = info[s];
             const S* seg = reinterpret_cast<const S*>(stage);
-            A f[d3::Q];
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                f[i] = T::value(seg[i * SEG + (H - d3::cx(i)) + tid]);
-            }
-            const uint8_t cls = stage[POP + tid];
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(smem_u32(empty + s));
-            }
             const Lattice3D<A>& L = table[kSingle ? 0u : it.x];
-            const uint32_t x = it.y * B + tid;
-            if (x < L.g.nx) {
-                const uint32_t from = L.parity ^ flip;
-                staged_node3<S, kSmag>(L.g, L.p, L.b, static_cast<const S*>(L.f[from]),
-                                       static_cast<S*>(L.f[from ^ 1u]), f, cls, x, it.z, it.w);
+            const uint32_t from = L.parity ^ flip;
+#pragma unroll
+            for (int p = 0; p < NPT; ++p) {
+                const uint32_t k = tid + static_cast<uint32_t>(p) * B;
+                A f[d3::Q];
+#pragma unroll
+                for (int i = 0; i < d3::Q; ++i) {
+                    f[i] = T::value(seg[i * SEG + (H - d3::cx(i)) + k]);
+                }
+                const uint8_t cls = stage[POP + k];
+                // Node coordinates: x0 + k = dy nx + x, in row y0 + dy.
+                const uint32_t m = it.y + k;
+                const uint32_t dy = L.magic != 0u ? __umulhi(m, L.magic) : m / L.g.nx;
+                const uint32_t x = m - dy * L.g.nx, y = it.z + dy;
+                if (cls == kBulk && x + 1u == L.g.nx && L.g.x_mode == ORR_X_INFLOW_OUTFLOW) {
+                    // Outlet: the zero-gradient copy f*_i(nx - 1) of the
+                    // c_x < 0 directions is the node's own staged value.
+#pragma unroll
+                    for (int i = 0; i < d3::Q; ++i) {
+                        if (d3::cx(i) < 0) {
+                            f[i] = T::value(seg[i * SEG + H + k]);
+                        }
+                    }
+                }
+                if (p == NPT - 1) {
+                    __syncwarp();
+                    if (lane == 0) {
+                        mbar_arrive(smem_u32(empty + s));
+                    }
+                }
+                if (y + 1u < L.g.ny) {
+                    staged_node3<S, kSmag>(L.g, L.p, L.b, static_cast<const S*>(L.f[from]),
+                                           static_cast<S*>(L.f[from ^ 1u]), f, cls, x, y, it.w);
+                }
             }
             if (++s == stages) {
                 s = 0;
@@ -411,7 +443,7 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
     __syncthreads();
     if (*abort_word != 0u && tid == 0) {
         // Let the copies still in flight land before the CTA's shared memory
-        // goes away: the last `stages` issued items (bounded waits).
+        // goes away: the last `stages` issued spans (bounded waits).
         const uint32_t issued = *issued_word;
         const uint32_t first = issued > stages ? issued - stages : 0u;
         for (uint32_t j = first; j < issued; ++j) {

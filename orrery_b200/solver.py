@@ -66,7 +66,7 @@ class Force2D:
 
 
 def _options(storage: str, allow_high_mach: bool, device: int, block_x: int, kernel: str = "auto",
-             stages: int = 0) -> abi.CSolverOptions:
+             stages: int = 0, nodes_per_thread: int = 0) -> abi.CSolverOptions:
     if storage not in abi.STORAGE_NAMES:
         raise ValueError(f"unknown storage {storage!r}; one of {sorted(abi.STORAGE_NAMES)}")
     if kernel not in abi.KERNEL_NAMES:
@@ -78,6 +78,7 @@ def _options(storage: str, allow_high_mach: bool, device: int, block_x: int, ker
     o.block_x = int(block_x)
     o.kernel = abi.KERNEL_NAMES[kernel]
     o.stages = int(stages)
+    o.nodes_per_thread = int(nodes_per_thread)
     return o
 
 
@@ -134,7 +135,7 @@ class CudaLbm3D:
 
     def __init__(self, config: Lbm3DConfig, mask: SolidMask3D, storage: str = "f32",
                  allow_high_mach: bool = False, device: int = 0, block_x: int = 0,
-                 kernel: str = "auto", stages: int = 0):
+                 kernel: str = "auto", stages: int = 0, nodes_per_thread: int = 0):
         self._lib = lib()
         self._h = None
         self.config = config
@@ -146,7 +147,7 @@ class CudaLbm3D:
             raise LbmError(abi.ORR_ERR_INVALID, "lbm3d: the solid mask does not match the lattice size")
         dist = None if mask.distance is None else np.ascontiguousarray(mask.distance, np.float64).reshape(-1)
         self._solid = solid
-        opts = _options(storage, allow_high_mach, device, block_x, kernel, stages)
+        opts = _options(storage, allow_high_mach, device, block_x, kernel, stages, nodes_per_thread)
         c = config.to_c()
         h = ctypes.c_void_p()
         check(self._lib.orr_lbm3d_create(ctypes.byref(c), ptr(solid, _u8p), ptr(dist, _dp), ctypes.byref(opts),
@@ -255,7 +256,8 @@ class CudaLbm3D:
         names = {v: n for n, v in abi.KERNEL_NAMES.items()}
         return {"kernel": names.get(k.kernel, str(k.kernel)), "block": k.block, "stages": k.stages,
                 "grid": k.grid, "ctas_per_sm": k.ctas_per_sm, "registers": k.registers,
-                "shared_bytes": k.shared_bytes, "staged_items": k.staged_items,
+                "shared_bytes": k.shared_bytes, "nodes_per_thread": k.nodes_per_thread,
+                "staged_items": k.staged_items,
                 "direct_items": k.direct_items}
 
 
@@ -354,11 +356,13 @@ class CudaLbm2D:
 
 
 def make_gpu_solver(config, mask, storage: str = "f32", allow_high_mach: bool = False,
-                    device: int = 0, block_x: int = 0, kernel: str = "auto", stages: int = 0):
+                    device: int = 0, block_x: int = 0, kernel: str = "auto", stages: int = 0,
+                    nodes_per_thread: int = 0):
     """make_gpu_solver (lbm3d.h:246-247; lbm2d.h:211-212) on the CUDA path.
     `kernel` and `stages` choose the D3Q19 step kernel (ignored in 2D)."""
     if isinstance(config, Lbm3DConfig):
-        return CudaLbm3D(config, mask, storage, allow_high_mach, device, block_x, kernel, stages)
+        return CudaLbm3D(config, mask, storage, allow_high_mach, device, block_x, kernel, stages,
+                         nodes_per_thread)
     if isinstance(config, Lbm2DConfig):
         return CudaLbm2D(config, mask, storage, allow_high_mach, device, block_x)
     raise TypeError("config must be an Lbm3DConfig or an Lbm2DConfig")

@@ -41,11 +41,14 @@ def solvers(storage):
     return [S.make_gpu_solver(c, m, storage=storage) for c, m in lattices()]
 
 
-SCHEDULES = [("staged", 256, 2), ("staged", 128, 4), ("rows", 128, 0), ("rows", 256, 0)]
+# (kernel, block, stages, nodes per thread, graph branches)
+SCHEDULES = [("staged", 256, 2, 2, 0), ("staged", 256, 3, 1, 0), ("staged", 128, 4, 2, 0),
+             ("staged", 256, 3, 2, 64), ("staged", 256, 2, 1, 3), ("rows", 128, 0, 0, 0),
+             ("rows", 256, 0, 0, 2)]
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
-@pytest.mark.parametrize("schedule", SCHEDULES, ids=lambda s: f"{s[0]}{s[1]}s{s[2]}")
+@pytest.mark.parametrize("schedule", SCHEDULES, ids=lambda s: f"{s[0]}{s[1]}s{s[2]}n{s[3]}b{s[4]}")
 def test_members_equal_alone(storage, schedule):
     alone = solvers(storage)
     for s in alone:

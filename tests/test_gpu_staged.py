@@ -56,8 +56,9 @@ CASES = ["sphere_les", "interpolated_convective_sponge", "periodic_duct_obstacle
          "unaligned_rows"]
 
 
-def run(cfg, mask, storage, kernel, block=0, stages=0, steps=STEPS, inlet=None):
-    s = S.make_gpu_solver(cfg, mask, storage=storage, kernel=kernel, block_x=block, stages=stages)
+def run(cfg, mask, storage, kernel, block=0, stages=0, steps=STEPS, inlet=None, npt=0):
+    s = S.make_gpu_solver(cfg, mask, storage=storage, kernel=kernel, block_x=block, stages=stages,
+                          nodes_per_thread=npt)
     if inlet is not None:
         s.set_inlet_velocity(inlet)
     s.step(steps)
@@ -84,13 +85,17 @@ def test_staged_equals_rows_bitwise(name, storage):
     assert np.allclose(ga, gb, rtol=0, atol=1e-12 * np.max(np.abs(ga)))
 
 
-@pytest.mark.parametrize("block,stages", [(128, 1), (128, 3), (256, 2), (256, 4)])
-def test_launch_shapes_agree(block, stages):
-    cfg, mask = case("sphere_les")
+@pytest.mark.parametrize("block,stages,npt", [(128, 1, 1), (128, 3, 2), (256, 2, 1), (256, 4, 1), (256, 2, 2),
+                                              (256, 3, 2)])
+@pytest.mark.parametrize("name", ["sphere_les", "ragged_tile", "interpolated_convective_sponge"])
+def test_launch_shapes_agree(name, block, stages, npt):
+    """Spans of one or two nodes per thread, across rows (64 and 272 nodes
+    wide: spans hold several rows, or end inside one)."""
+    cfg, mask = case(name)
     ref = run(cfg, mask, "f32", "rows")
-    s = run(cfg, mask, "f32", "staged", block=block, stages=stages)
+    s = run(cfg, mask, "f32", "staged", block=block, stages=stages, npt=npt)
     info = s.kernel_info()
-    assert (info["block"], info["stages"]) == (block, stages)
+    assert (info["block"], info["stages"], info["nodes_per_thread"]) == (block, stages, npt)
     assert np.array_equal(ref.populations(), s.populations())
 
 
@@ -117,3 +122,5 @@ def test_refused_shapes():
         S.make_gpu_solver(cfg, mask, kernel="staged", block_x=64)
     with pytest.raises(S.LbmError):
         S.make_gpu_solver(cfg, mask, kernel="staged", stages=9)
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, kernel="staged", nodes_per_thread=3)
