@@ -30,6 +30,7 @@ inline constexpr Candidate kCandidates[] = {
     {ORR_KERNEL_STAGED, 256, 2, 2, 64}, {ORR_KERNEL_STAGED, 256, 3, 2, 64},
     {ORR_KERNEL_STAGED, 256, 4, 1, 64}, {ORR_KERNEL_STAGED, 128, 3, 2, 64},
     {ORR_KERNEL_ROWS, 128, 0, 0, 0},    {ORR_KERNEL_ROWS, 128, 0, 0, 64},
+    {ORR_KERNEL_PAIRS, 128, 0, 0, 0},   {ORR_KERNEL_PAIRS, 128, 0, 0, 64},
 };
 
 } // namespace orr
@@ -263,6 +264,14 @@ struct orr_batch3d {
 
     bool branched() const { return branches > 0; }
 
+    // One row-tile step of member m from buffer `from` on stream s: the
+    // two-node kernel for PAIRS when its nx is even, else the one-node one.
+    void member_step(orr_lbm3d* m, uint32_t from, cudaStream_t s) {
+        const auto step = kernel == ORR_KERNEL_PAIRS && m->g.nx % 2 == 0 ? ops->step_pairs : ops->step;
+        check(step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
+              "batch step kernel");
+    }
+
     // Per-member single-lattice entries of the branched staged schedule; each
     // member's grid is its share of the whole launch's CTAs by node count.
     template <class A> void fill_solo() {
@@ -335,8 +344,7 @@ struct orr_batch3d {
                                       solo_grid[k], status, s),
                           "batch step kernel");
                 } else {
-                    check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
-                          "batch step kernel");
+                    member_step(m, from, s);
                 }
                 ++launches;
             }
@@ -367,11 +375,7 @@ struct orr_batch3d {
             ++launches;
         } else {
             for (std::size_t k = 0; k < members.size(); ++k) {
-                orr_lbm3d* m = members[k];
-                const int from = parity[k] ^ static_cast<int>(flip);
-                check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block,
-                                stream),
-                      "batch step kernel");
+                member_step(members[k], static_cast<uint32_t>(parity[k]) ^ flip, stream);
                 ++launches;
             }
         }

@@ -721,6 +721,58 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
     step_node3<S, kSmag>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
 }
 
+// Row tiles with two neighbouring nodes (x, x + 1) per thread, for lattices
+// with even nx.  When both nodes are bulk, all 38 pulls are issued before
+// either node is finished (twice the bytes in flight per thread of
+// step3d_kernel); the 7 directions with c_x = 0 fetch both nodes with one
+// aligned two-value load.  Any other pair takes step_node3 node by node.
+// The finish of every node is the one of step_node3, so the result equals
+// step3d_kernel's bit for bit.
+template <class S> constexpr int kPairMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 6;
+
+template <class S, bool kSmag>
+__global__ void __launch_bounds__(128, kPairMinBlocks<S>) step3d_pairs_kernel(Geom3D g,
+                                                                             Phys3D<typename Storage<S>::A> p,
+                                                                             const S* __restrict__ src,
+                                                                             S* __restrict__ dst,
+                                                                             StepBuffers3D b) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint32_t x = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (x >= g.nx) {
+        return;
+    }
+    const uint32_t y = blockIdx.y, z = blockIdx.z;
+    const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
+    const uint8_t ca = b.cls[here], cb = b.cls[here + 1];
+    if (ca != kBulk || cb != kBulk) {
+        step_node3<S, kSmag>(g, p, src, dst, b, x, y, z);
+        step_node3<S, kSmag>(g, p, src, dst, b, x + 1u, y, z);
+        return;
+    }
+    const uint64_t cells = g.cells;
+    const int64_t nx = g.nx, plane = g.plane;
+    A fa[d3::Q], fb[d3::Q];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const int64_t source = static_cast<int64_t>(here) - (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+        const S* at = src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source);
+        if (d3::cx(i) == 0) {
+            T::load2(at, fa[i], fb[i]);
+        } else {
+            fa[i] = T::load(at);
+            fb[i] = T::load(at + 1);
+        }
+    }
+    bulk_edges3<S>(g, p, src, b, x, y, z, here, fa);
+    bulk_edges3<S>(g, p, src, b, x + 1u, y, z, here + 1, fb);
+    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
+        inlet_west3<A, T::kShifted>(fa, static_cast<const A*>(b.inlet));
+    }
+    finish3<S, kSmag>(g, p, b, fa, x, y, z, here, dst);
+    finish3<S, kSmag>(g, p, b, fb, x + 1u, y, z, here + 1, dst);
+}
+
 // ------------------------------------------------------------ init / misc --
 
 // Equilibrium of (rho, u) at every node, solids at rest (initial_populations,
