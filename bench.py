@@ -192,7 +192,7 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged", "pairs"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
     ap.add_argument("--stages", type=int, default=0)
     ap.add_argument("--npt", type=int, default=0, help="staged kernel: nodes per thread of a span")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"])

@@ -119,11 +119,9 @@ typedef struct orr_solver_options {
  * row tiles receive their 19 source row segments through a shared-memory
  * pipeline of bulk asynchronous copies (lattices whose nx is a multiple of 16;
  * other rows take the per-node path).  AUTO picks STAGED for the binary16
- * and bfloat16 forms when the lattice qualifies, ROWS otherwise.  PAIRS:
- * the row tiles with two neighbouring nodes per thread, all pulls of both in
- * flight before either is finished (lattices with even nx).  All kernels
- * give the same result bit for bit. */
-enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2, ORR_KERNEL_PAIRS = 3 };
+ * and bfloat16 forms when the lattice qualifies, ROWS otherwise.  Both give
+ * the same result bit for bit. */
+enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2 };
 
 typedef struct orr_lbm3d orr_lbm3d;
 typedef struct orr_lbm2d orr_lbm2d;

@@ -74,9 +74,8 @@ class CForceLinks(ctypes.Structure):
 ORR_FORCE_STATIC_MAX_LINKS = 8388608
 
 
-ORR_KERNEL_AUTO, ORR_KERNEL_ROWS, ORR_KERNEL_STAGED, ORR_KERNEL_PAIRS = 0, 1, 2, 3
-KERNEL_NAMES = {"auto": ORR_KERNEL_AUTO, "rows": ORR_KERNEL_ROWS, "staged": ORR_KERNEL_STAGED,
-                "pairs": ORR_KERNEL_PAIRS}
+ORR_KERNEL_AUTO, ORR_KERNEL_ROWS, ORR_KERNEL_STAGED = 0, 1, 2
+KERNEL_NAMES = {"auto": ORR_KERNEL_AUTO, "rows": ORR_KERNEL_ROWS, "staged": ORR_KERNEL_STAGED}
 
 
 class CKernelInfo(ctypes.Structure):

@@ -176,7 +176,7 @@ orr_status orr_batch3d_set_schedule(orr_batch3d* batch, const orr_batch_schedule
             if (s.nodes_per_thread > 2) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: nodes_per_thread must be 0 (default), 1 or 2"};
             }
-        } else if (s.kernel == ORR_KERNEL_ROWS || s.kernel == ORR_KERNEL_PAIRS) {
+        } else if (s.kernel == ORR_KERNEL_ROWS) {
             if (s.block == 0 || s.block > 256 || s.block % 32 != 0) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the row step takes a block of 32 to 256 threads"};
             }

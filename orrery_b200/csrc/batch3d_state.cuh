@@ -30,7 +30,6 @@ inline constexpr Candidate kCandidates[] = {
     {ORR_KERNEL_STAGED, 256, 2, 2, 64}, {ORR_KERNEL_STAGED, 256, 3, 2, 64},
     {ORR_KERNEL_STAGED, 256, 4, 1, 64}, {ORR_KERNEL_STAGED, 128, 3, 2, 64},
     {ORR_KERNEL_ROWS, 128, 0, 0, 0},    {ORR_KERNEL_ROWS, 128, 0, 0, 64},
-    {ORR_KERNEL_PAIRS, 128, 0, 0, 0},   {ORR_KERNEL_PAIRS, 128, 0, 0, 64},
 };
 
 } // namespace orr
@@ -264,11 +263,9 @@ struct orr_batch3d {
 
     bool branched() const { return branches > 0; }
 
-    // One row-tile step of member m from buffer `from` on stream s: the
-    // two-node kernel for PAIRS when its nx is even, else the one-node one.
+    // One row-tile step of member m from buffer `from` on stream s.
     void member_step(orr_lbm3d* m, uint32_t from, cudaStream_t s) {
-        const auto step = kernel == ORR_KERNEL_PAIRS && m->g.nx % 2 == 0 ? ops->step_pairs : ops->step;
-        check(step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
+        check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
               "batch step kernel");
     }
 

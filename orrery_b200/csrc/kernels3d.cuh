@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <initializer_list>
 
 #include "lattice.h"
 #include "orrery_lbm.h"
@@ -85,6 +86,24 @@ __device__ __forceinline__ double w_rt(int j) {
     return j == 0 ? 1.0 / 3.0 : (j <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
 }
 
+// Arithmetic with explicit rounding.  The binary32 step is written with
+// these: each operation rounds on its own or is an explicit fused
+// multiply-add, so the compiler cannot contract differently in the kernels
+// that inline the same node code (row, staged, batched), and all of
+// them give the same bits.  The binary64 overloads are the plain operators:
+// their unit is built without contraction and keeps the reference CPU
+// solver's order (r_fma is an unfused a * b + c there).
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float r_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double r_add(double a, double b) { return a + b; }
+__device__ __forceinline__ double r_sub(double a, double b) { return a - b; }
+__device__ __forceinline__ double r_mul(double a, double b) { return a * b; }
+__device__ __forceinline__ double r_div(double a, double b) { return a / b; }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return a * b + c; }
+
 // Reciprocal and square root of the binary32 collision: the hardware
 // approximations refined by one Newton-Raphson step, r' = r + r (1 - x r)
 // and s' = s + (y / 2)(x - s^2) with s = x y, y ~ 1/sqrt(x), which lands
@@ -94,15 +113,15 @@ __device__ __forceinline__ double w_rt(int j) {
 // the reference CPU solver's rounding).
 __device__ __forceinline__ float fast_rcp(float x) {
     const float r = __fdividef(1.0f, x);
-    return fmaf(r, fmaf(-x, r, 1.0f), r);
+    return __fmaf_rn(r, __fmaf_rn(-x, r, 1.0f), r);
 }
 __device__ __forceinline__ double fast_rcp(double x) {
     return 1.0 / x;
 }
 __device__ __forceinline__ float fast_sqrt(float x) {
     const float y = rsqrtf(x);
-    const float s = x * y;
-    return x == 0.0f ? 0.0f : fmaf(0.5f * y, fmaf(-s, s, x), s);
+    const float s = __fmul_rn(x, y);
+    return x == 0.0f ? 0.0f : __fmaf_rn(__fmul_rn(0.5f, y), __fmaf_rn(-s, s, x), s);
 }
 __device__ __forceinline__ double fast_sqrt(double x) {
     return sqrt(x);
@@ -141,24 +160,34 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
     if constexpr (kShifted) {
         // Pairwise sums: the density deviation (about 1e-3) is a sum of
         // terms about ten times larger, so a balanced tree keeps more digits
-        // than a running sum.
-        const A p1 = f[1] + f[2], p3 = f[3] + f[4], p5 = f[5] + f[6], p7 = f[7] + f[8],
-                p9 = f[9] + f[10], p11 = f[11] + f[12], p13 = f[13] + f[14], p15 = f[15] + f[16],
-                p17 = f[17] + f[18];
-        const A drho = f[0] + (((p1 + p3) + (p5 + p7)) + ((p9 + p11) + ((p13 + p15) + p17)));
-        const A m1 = f[1] - f[2], m3 = f[3] - f[4], m5 = f[5] - f[6], m7 = f[7] - f[8],
-                m9 = f[9] - f[10], m11 = f[11] - f[12], m13 = f[13] - f[14], m15 = f[15] - f[16],
-                m17 = f[17] - f[18];
-        const A jx = (m1 + m7) + (m9 + (m11 + m13));
-        const A jy = (m3 + m7) + ((m15 + m17) - m9);
-        const A jz = (m5 + m11) + ((m15 - m13) - m17);
-        const A rho = A(1) + drho;
-        const A inv = fast_rcp(rho);
-        const A ux = (jx + A(0.5) * p.fx) * inv;
-        const A uy = (jy + A(0.5) * p.fy) * inv;
-        const A uz = (jz + A(0.5) * p.fz) * inv;
-        const A uu = ux * ux + uy * uy + uz * uz;
-        A tau = p.tau;
+        // than a running sum.  Opposite pairs are summed and differenced two
+        // at a time in packed lanes: (f1, f3) with (f2, f4), (f5, f7) with
+        // (f6, f8), (f9, f11) with (f10, f12), (f13, f15) with (f14, f16).
+        const float2 neg = make_float2(-1.0f, -1.0f);
+        const float2 a1 = make_float2(f[1], f[3]), b1 = make_float2(f[2], f[4]);
+        const float2 a2 = make_float2(f[5], f[7]), b2 = make_float2(f[6], f[8]);
+        const float2 a3 = make_float2(f[9], f[11]), b3 = make_float2(f[10], f[12]);
+        const float2 a4 = make_float2(f[13], f[15]), b4 = make_float2(f[14], f[16]);
+        const float2 s1 = __fadd2_rn(a1, b1), d1 = __ffma2_rn(b1, neg, a1);
+        const float2 s2 = __fadd2_rn(a2, b2), d2 = __ffma2_rn(b2, neg, a2);
+        const float2 s3 = __fadd2_rn(a3, b3), d3v = __ffma2_rn(b3, neg, a3);
+        const float2 s4 = __fadd2_rn(a4, b4), d4 = __ffma2_rn(b4, neg, a4);
+        const float p1 = s1.x, p3 = s1.y, p5 = s2.x, p7 = s2.y, p9 = s3.x, p11 = s3.y, p13 = s4.x,
+                    p15 = s4.y, p17 = r_add(f[17], f[18]);
+        const float m1 = d1.x, m3 = d1.y, m5 = d2.x, m7 = d2.y, m9 = d3v.x, m11 = d3v.y, m13 = d4.x,
+                    m15 = d4.y, m17 = r_sub(f[17], f[18]);
+        const float drho = r_add(f[0], r_add(r_add(r_add(p1, p3), r_add(p5, p7)),
+                                             r_add(r_add(p9, p11), r_add(r_add(p13, p15), p17))));
+        const float jx = r_add(r_add(m1, m7), r_add(m9, r_add(m11, m13)));
+        const float jy = r_add(r_add(m3, m7), r_sub(r_add(m15, m17), m9));
+        const float jz = r_add(r_add(m5, m11), r_sub(r_sub(m15, m13), m17));
+        const float rho = r_add(1.0f, drho);
+        const float inv = fast_rcp(rho);
+        const float ux = r_mul(r_fma(0.5f, p.fx, jx), inv);
+        const float uy = r_mul(r_fma(0.5f, p.fy, jy), inv);
+        const float uz = r_mul(r_fma(0.5f, p.fz, jz), inv);
+        const float uu = r_fma(uz, uz, r_fma(uy, uy, r_mul(ux, ux)));
+        float tau = p.tau;
         if constexpr (kSmag) {
             // Pi_neq = sum c c (f - f_eq).  For the second-order D3Q19
             // equilibrium sum c_a c_b f_eq = rho (c_s^2 delta_ab + u_a u_b)
@@ -166,62 +195,66 @@ __device__ __forceinline__ void collide3(A (&f)[d3::Q], const Phys3D<A>& p, int 
             // Pi_neq = sum c c f_s - drho c_s^2 delta - rho u u; f_eq is then
             // formed on the fly in the relaxation below.  The second moments
             // reuse the opposite-pair sums of the density.
-            const A sxx = (p1 + p7) + (p9 + (p11 + p13));
-            const A syy = (p3 + p7) + (p9 + (p15 + p17));
-            const A szz = (p5 + p11) + (p13 + (p15 + p17));
-            const A sxy = p7 - p9;
-            const A sxz = p11 - p13;
-            const A syz = p15 - p17;
-            const A iso = drho * A(1.0 / 3.0);
-            const A pxx = sxx - iso - rho * ux * ux;
-            const A pyy = syy - iso - rho * uy * uy;
-            const A pzz = szz - iso - rho * uz * uz;
-            const A pxy = sxy - rho * ux * uy;
-            const A pxz = sxz - rho * ux * uz;
-            const A pyz = syz - rho * uy * uz;
-            const A strain =
-                fast_sqrt(pxx * pxx + pyy * pyy + pzz * pzz + A(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
-            tau = A(0.5) * (tau + fast_sqrt(tau * tau + A(kSmagFactor) * p.smag_c2 * strain * inv));
+            const float sxx = r_add(r_add(p1, p7), r_add(p9, r_add(p11, p13)));
+            const float syy = r_add(r_add(p3, p7), r_add(p9, r_add(p15, p17)));
+            const float szz = r_add(r_add(p5, p11), r_add(p13, r_add(p15, p17)));
+            const float sxy = r_sub(p7, p9);
+            const float sxz = r_sub(p11, p13);
+            const float syz = r_sub(p15, p17);
+            const float iso = r_mul(drho, 1.0f / 3.0f);
+            const float rux = r_mul(rho, ux), ruy = r_mul(rho, uy), ruz = r_mul(rho, uz);
+            const float pxx = r_fma(-rux, ux, r_sub(sxx, iso));
+            const float pyy = r_fma(-ruy, uy, r_sub(syy, iso));
+            const float pzz = r_fma(-ruz, uz, r_sub(szz, iso));
+            const float pxy = r_fma(-rux, uy, sxy);
+            const float pxz = r_fma(-rux, uz, sxz);
+            const float pyz = r_fma(-ruy, uz, syz);
+            const float diag = r_fma(pzz, pzz, r_fma(pyy, pyy, r_mul(pxx, pxx)));
+            const float off = r_fma(pyz, pyz, r_fma(pxz, pxz, r_mul(pxy, pxy)));
+            const float strain = fast_sqrt(r_fma(2.0f, off, diag));
+            const float k = r_mul(r_mul(r_mul(static_cast<float>(kSmagFactor), p.smag_c2), strain), inv);
+            tau = r_mul(0.5f, r_add(tau, fast_sqrt(r_fma(tau, tau, k))));
         }
-        const A omega = fast_rcp(tau);
+        const float omega = fast_rcp(tau);
         // Relaxation towards f_eq,i - w_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2
         // - 1.5 u.u)), by opposite pairs (c_{i+1} = -c_i for odd i): the even
         // part w (drho - 1.5 rho u.u + 4.5 rho (c.u)^2) is shared and the odd
-        // part 3 w rho c.u changes sign.
-        const A base = drho - A(1.5) * rho * uu;
-        const A rho45 = A(4.5) * rho;
-        f[0] += omega * (A(d3::w(0)) * base - f[0]);
-        // Two opposite pairs at a time in packed binary32 lanes: plus
-        // members (f_a, f_b), minus members (f_a+1, f_b+1).  c.u is written
-        // out per direction (c components are 0 or +-1).
+        // part 3 w rho c.u changes sign.  Two opposite pairs at a time in
+        // packed lanes; c.u is written out per direction (components 0, +-1).
+        const float base = r_fma(r_mul(-1.5f, rho), uu, drho);
+        const float rho45 = r_mul(4.5f, rho);
+        constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+        f[0] = r_fma(omega, r_fma(w0, base, -f[0]), f[0]);
         const float2 base2 = make_float2(base, base), rho45_2 = make_float2(rho45, rho45);
         const float2 omega2 = make_float2(omega, omega);
-        constexpr float w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
-        const float r3a = (3.0f * w1) * rho, r3b = (3.0f * w2) * rho;
+        const float r3a = r_mul(3.0f * w1, rho), r3b = r_mul(3.0f * w2, rho);
         relax_pairs2(f[1], f[3], f[2], f[4], make_float2(ux, uy), make_float2(w1, w1),
                      make_float2(r3a, r3a), base2, rho45_2, omega2);
-        relax_pairs2(f[5], f[7], f[6], f[8], make_float2(uz, ux + uy), make_float2(w1, w2),
+        relax_pairs2(f[5], f[7], f[6], f[8], make_float2(uz, r_add(ux, uy)), make_float2(w1, w2),
                      make_float2(r3a, r3b), base2, rho45_2, omega2);
-        relax_pairs2(f[9], f[11], f[10], f[12], make_float2(ux - uy, ux + uz), make_float2(w2, w2),
+        relax_pairs2(f[9], f[11], f[10], f[12], make_float2(r_sub(ux, uy), r_add(ux, uz)), make_float2(w2, w2),
                      make_float2(r3b, r3b), base2, rho45_2, omega2);
-        relax_pairs2(f[13], f[15], f[14], f[16], make_float2(ux - uz, uy + uz), make_float2(w2, w2),
+        relax_pairs2(f[13], f[15], f[14], f[16], make_float2(r_sub(ux, uz), r_add(uy, uz)), make_float2(w2, w2),
                      make_float2(r3b, r3b), base2, rho45_2, omega2);
         {
-            const A cu = uy - uz; // direction 17 (0, 1, -1)
-            const A even = A(w2) * (base + rho45 * cu * cu);
-            const A odd = r3b * cu;
-            f[17] += omega * (even + odd - f[17]);
-            f[18] += omega * (even - odd - f[18]);
+            const float cu = r_sub(uy, uz); // direction 17 (0, 1, -1)
+            const float even = r_mul(w2, r_fma(rho45, r_mul(cu, cu), base));
+            const float odd = r_mul(r3b, cu);
+            f[17] = r_fma(omega, r_sub(r_add(even, odd), f[17]), f[17]);
+            f[18] = r_fma(omega, r_sub(r_sub(even, odd), f[18]), f[18]);
         }
         if (forced) {
-            const A scale = A(1) - A(0.5) * omega;
+            // Guo forcing: w (1 - omega / 2) (3 (c - u).F + 9 (c.u)(c.F)).
+            const float scale = r_fma(-0.5f, omega, 1.0f);
 #pragma unroll
             for (int i = 0; i < d3::Q; ++i) {
-                const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
-                const A cu = ex * ux + ey * uy + ez * uz;
-                f[i] += scale * A(d3::w(i)) *
-                        (A(3) * ((ex - ux) * p.fx + (ey - uy) * p.fy + (ez - uz) * p.fz) +
-                         A(9) * cu * (ex * p.fx + ey * p.fy + ez * p.fz));
+                const float ex = static_cast<float>(d3::cx(i)), ey = static_cast<float>(d3::cy(i)),
+                            ez = static_cast<float>(d3::cz(i));
+                const float cu = r_fma(ez, uz, r_fma(ey, uy, r_mul(ex, ux)));
+                const float cf = r_fma(ez, p.fz, r_fma(ey, p.fy, r_mul(ex, p.fx)));
+                const float uf = r_fma(r_sub(ez, uz), p.fz, r_fma(r_sub(ey, uy), p.fy, r_mul(r_sub(ex, ux), p.fx)));
+                const float term = r_fma(3.0f, uf, r_mul(r_mul(9.0f, cu), cf));
+                f[i] = r_fma(r_mul(scale, static_cast<float>(d3::w(i))), term, f[i]);
             }
         }
         out_ux = ux;
@@ -293,8 +326,8 @@ __device__ __forceinline__ A sponge_rate3(const Geom3D& g, const Phys3D<A>& p, u
     A best = 0;
     const auto layer = [&best](uint32_t d, uint32_t t) {
         if (d < t) {
-            const A r = A(t - d) / A(t);
-            const A v = r * r;
+            const A r = r_div(A(t - d), A(t));
+            const A v = r_mul(r, r);
             best = best < v ? v : best;
         }
     };
@@ -308,7 +341,7 @@ __device__ __forceinline__ A sponge_rate3(const Geom3D& g, const Phys3D<A>& p, u
         layer(z, g.sponge_sides);
         layer(g.nz - 1u - z, g.sponge_sides);
     }
-    return p.sponge_strength * best;
+    return r_mul(p.sponge_strength, best);
 }
 
 // Absorbing-layer relaxation towards f_eq(1, u_inlet)
@@ -318,15 +351,18 @@ __device__ __forceinline__ void absorb3(A (&f)[d3::Q], A s, const A* inlet) {
     const A ux = inlet[0], uy = inlet[1], uz = inlet[2];
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
-        const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
-        const A uu = ux * ux + uy * uy + uz * uz;
+        const A cu = r_add(r_add(r_mul(A(d3::cx(i)), ux), r_mul(A(d3::cy(i)), uy)), r_mul(A(d3::cz(i)), uz));
+        const A uu = r_add(r_add(r_mul(ux, ux), r_mul(uy, uy)), r_mul(uz, uz));
+        const A quad = r_add(r_mul(A(3), cu), r_mul(r_mul(A(4.5), cu), cu));
         A target;
         if constexpr (kShifted) {
-            target = A(d3::w(i)) * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu);
+            target = r_mul(A(d3::w(i)), r_sub(quad, r_mul(A(1.5), uu)));
         } else {
-            target = A(d3::w(i)) * A(1) * (A(1) + A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu);
+            target = r_mul(r_mul(A(d3::w(i)), A(1)),
+                           r_sub(r_add(r_add(A(1), r_mul(A(3), cu)), r_mul(r_mul(A(4.5), cu), cu)),
+                                 r_mul(A(1.5), uu)));
         }
-        f[i] -= s * (f[i] - target);
+        f[i] = r_sub(f[i], r_mul(s, r_sub(f[i], target)));
     }
 }
 
@@ -340,50 +376,62 @@ __device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
         if (d3::cx(i) == 0) {
-            known += f[i];
+            known = r_add(known, f[i]);
         } else if (d3::cx(i) < 0) {
-            known += A(2) * f[i];
+            known = r_add(known, r_mul(A(2), f[i]));
         }
     }
     A rho, drho;
     if constexpr (kShifted) {
-        drho = (known + ux) / (A(1) - ux);
-        rho = A(1) + drho;
+        drho = r_div(r_add(known, ux), r_sub(A(1), ux));
+        rho = r_add(A(1), drho);
     } else {
-        rho = known / (1.0 - ux);
+        rho = r_div(known, r_sub(A(1), ux));
         drho = 0;
     }
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
         if (d3::cx(i) > 0) {
-            const A cu = A(d3::cx(i)) * ux + A(d3::cy(i)) * uy + A(d3::cz(i)) * uz;
-            f[i] = f[d3::opposite(i)] + A(6) * A(d3::w(i)) * rho * cu;
+            const A cu = r_add(r_add(r_mul(A(d3::cx(i)), ux), r_mul(A(d3::cy(i)), uy)), r_mul(A(d3::cz(i)), uz));
+            f[i] = r_add(f[d3::opposite(i)], r_mul(r_mul(A(6) * A(d3::w(i)), rho), cu));
         }
     }
-    const A uu = ux * ux + uy * uy + uz * uz;
+    const A uu = r_add(r_add(r_mul(ux, ux), r_mul(uy, uy)), r_mul(uz, uz));
     if constexpr (kShifted) {
         // Pi_neq from the second moments of the reconstructed set (sum c c f_eq
         // = rho (c_s^2 I + u u); shifted: drho c_s^2 I + rho u u), then
         // f = f_eq + 4.5 w (c c - c_s^2 I) : Pi_neq with f_eq formed on the fly.
-        const A iso = drho * A(1.0 / 3.0);
-        const A pxx = f[1] + f[2] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] + f[14] -
-                      iso - rho * ux * ux;
-        const A pyy = f[3] + f[4] + f[7] + f[8] + f[9] + f[10] + f[15] + f[16] + f[17] + f[18] -
-                      iso - rho * uy * uy;
-        const A pzz = f[5] + f[6] + f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18] -
-                      iso - rho * uz * uz;
-        const A pxy = f[7] + f[8] - f[9] - f[10] - rho * ux * uy;
-        const A pxz = f[11] + f[12] - f[13] - f[14] - rho * ux * uz;
-        const A pyz = f[15] + f[16] - f[17] - f[18] - rho * uy * uz;
+        const auto sum = [](std::initializer_list<A> v) {
+            A t = 0;
+            bool first = true;
+            for (A x : v) {
+                t = first ? x : r_add(t, x);
+                first = false;
+            }
+            return t;
+        };
+        const A iso = r_mul(drho, A(1.0 / 3.0));
+        const A pxx = r_sub(r_sub(sum({f[1], f[2], f[7], f[8], f[9], f[10], f[11], f[12], f[13], f[14]}), iso),
+                            r_mul(r_mul(rho, ux), ux));
+        const A pyy = r_sub(r_sub(sum({f[3], f[4], f[7], f[8], f[9], f[10], f[15], f[16], f[17], f[18]}), iso),
+                            r_mul(r_mul(rho, uy), uy));
+        const A pzz = r_sub(r_sub(sum({f[5], f[6], f[11], f[12], f[13], f[14], f[15], f[16], f[17], f[18]}), iso),
+                            r_mul(r_mul(rho, uz), uz));
+        const A pxy = r_sub(r_sub(r_sub(r_add(f[7], f[8]), f[9]), f[10]), r_mul(r_mul(rho, ux), uy));
+        const A pxz = r_sub(r_sub(r_sub(r_add(f[11], f[12]), f[13]), f[14]), r_mul(r_mul(rho, ux), uz));
+        const A pyz = r_sub(r_sub(r_sub(r_add(f[15], f[16]), f[17]), f[18]), r_mul(r_mul(rho, uy), uz));
         const A cs2 = A(1.0 / 3.0);
 #pragma unroll
         for (int i = 0; i < d3::Q; ++i) {
             const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
-            const A cu = ex * ux + ey * uy + ez * uz;
-            const A feq = A(d3::w(i)) * (drho + rho * (A(3) * cu + A(4.5) * cu * cu - A(1.5) * uu));
-            f[i] = feq + A(4.5) * A(d3::w(i)) *
-                             ((ex * ex - cs2) * pxx + (ey * ey - cs2) * pyy + (ez * ez - cs2) * pzz +
-                              A(2) * (ex * ey * pxy + ex * ez * pxz + ey * ez * pyz));
+            const A cu = r_add(r_add(r_mul(ex, ux), r_mul(ey, uy)), r_mul(ez, uz));
+            const A quad = r_sub(r_add(r_mul(A(3), cu), r_mul(r_mul(A(4.5), cu), cu)), r_mul(A(1.5), uu));
+            const A feq = r_mul(A(d3::w(i)), r_add(drho, r_mul(rho, quad)));
+            const A t = r_add(r_add(r_add(r_mul(ex * ex - cs2, pxx), r_mul(ey * ey - cs2, pyy)),
+                                    r_mul(ez * ez - cs2, pzz)),
+                              r_mul(A(2), r_add(r_add(r_mul(ex * ey, pxy), r_mul(ex * ez, pxz)),
+                                                r_mul(ey * ez, pyz))));
+            f[i] = r_add(feq, r_mul(A(4.5) * A(d3::w(i)), t));
         }
         return;
     }
@@ -441,12 +489,13 @@ __device__ __forceinline__ typename Storage<S>::A reflected3(const S* __restrict
     if (q == A(0.5)) {
         return leaving;
     }
+    const A q2 = r_mul(A(2), q);
     if (q < A(0.5)) {
         const uint64_t farther = static_cast<uint64_t>(static_cast<int64_t>(here) + farther_off);
-        return A(2) * q * leaving + (A(1) - A(2) * q) * T::load(src + O * cells + farther);
+        return r_add(r_mul(q2, leaving), r_mul(r_sub(A(1), q2), T::load(src + O * cells + farther)));
     }
-    return (leaving + (A(2) * q - A(1)) * T::load(src + static_cast<uint64_t>(I) * cells + here)) /
-           (A(2) * q);
+    return r_div(r_add(leaving, r_mul(r_sub(q2, A(1)), T::load(src + static_cast<uint64_t>(I) * cells + here))),
+                 q2);
 }
 
 // General gather of direction I at node (x, y, z) (resolve_source,
@@ -502,8 +551,8 @@ __device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typena
             for (int k = 0; k < d3::Q; ++k) r += T::load(src + static_cast<uint64_t>(k) * cells + here);
             wall_rho = T::kShifted ? A(1) + r : r;
         }
-        out = T::load(src + static_cast<uint64_t>(d3::opposite(I)) * cells + here) +
-              A(6) * A(d3::w(I)) * wall_rho * A(CX) * p.wall_ux[wall_side];
+        out = r_add(T::load(src + static_cast<uint64_t>(d3::opposite(I)) * cells + here),
+                    r_mul(r_mul(r_mul(A(6) * A(d3::w(I)), wall_rho), A(CX)), p.wall_ux[wall_side]));
         return;
     }
     const int dir = zmir ? (ymir ? MZY : MZ) : (ymir ? MY : I);
@@ -526,7 +575,7 @@ __device__ __forceinline__ void gather_one3(const Geom3D& g, const Phys3D<typena
                 const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(I)) * g.ny * g.nz +
                                    static_cast<uint64_t>(y) + static_cast<uint64_t>(g.ny) * z;
                 const A u = p.outlet_speed;
-                const A v = (hist[k] + u * up) / (A(1) + u);
+                const A v = r_div(r_add(hist[k], r_mul(u, up)), r_add(A(1), u));
                 hist[k] = v;
                 out = v;
             }
@@ -600,7 +649,7 @@ __device__ __forceinline__ void convective_blend3(const Geom3D& g, const Phys3D<
     for (int i = 0; i < d3::Q; ++i) {
         if (d3::cx(i) < 0) {
             const uint64_t k = static_cast<uint64_t>(d3::outlet_slot(i)) * face + at;
-            const A v = (hist[k] + u * f[i]) / (A(1) + u);
+            const A v = r_div(r_add(hist[k], r_mul(u, f[i])), r_add(A(1), u));
             hist[k] = v;
             f[i] = v;
         }
@@ -719,58 +768,6 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
         return;
     }
     step_node3<S, kSmag>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
-}
-
-// Row tiles with two neighbouring nodes (x, x + 1) per thread, for lattices
-// with even nx.  When both nodes are bulk, all 38 pulls are issued before
-// either node is finished (twice the bytes in flight per thread of
-// step3d_kernel); the 7 directions with c_x = 0 fetch both nodes with one
-// aligned two-value load.  Any other pair takes step_node3 node by node.
-// The finish of every node is the one of step_node3, so the result equals
-// step3d_kernel's bit for bit.
-template <class S> constexpr int kPairMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 6;
-
-template <class S, bool kSmag>
-__global__ void __launch_bounds__(128, kPairMinBlocks<S>) step3d_pairs_kernel(Geom3D g,
-                                                                             Phys3D<typename Storage<S>::A> p,
-                                                                             const S* __restrict__ src,
-                                                                             S* __restrict__ dst,
-                                                                             StepBuffers3D b) {
-    using A = typename Storage<S>::A;
-    using T = Storage<S>;
-    const uint32_t x = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (x >= g.nx) {
-        return;
-    }
-    const uint32_t y = blockIdx.y, z = blockIdx.z;
-    const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
-    const uint8_t ca = b.cls[here], cb = b.cls[here + 1];
-    if (ca != kBulk || cb != kBulk) {
-        step_node3<S, kSmag>(g, p, src, dst, b, x, y, z);
-        step_node3<S, kSmag>(g, p, src, dst, b, x + 1u, y, z);
-        return;
-    }
-    const uint64_t cells = g.cells;
-    const int64_t nx = g.nx, plane = g.plane;
-    A fa[d3::Q], fb[d3::Q];
-#pragma unroll
-    for (int i = 0; i < d3::Q; ++i) {
-        const int64_t source = static_cast<int64_t>(here) - (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-        const S* at = src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source);
-        if (d3::cx(i) == 0) {
-            T::load2(at, fa[i], fb[i]);
-        } else {
-            fa[i] = T::load(at);
-            fb[i] = T::load(at + 1);
-        }
-    }
-    bulk_edges3<S>(g, p, src, b, x, y, z, here, fa);
-    bulk_edges3<S>(g, p, src, b, x + 1u, y, z, here + 1, fb);
-    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
-        inlet_west3<A, T::kShifted>(fa, static_cast<const A*>(b.inlet));
-    }
-    finish3<S, kSmag>(g, p, b, fa, x, y, z, here, dst);
-    finish3<S, kSmag>(g, p, b, fb, x + 1u, y, z, here + 1, dst);
 }
 
 // ------------------------------------------------------------ init / misc --

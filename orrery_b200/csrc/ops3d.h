@@ -34,11 +34,6 @@ struct Ops3D {
                         cudaStream_t s);
     // Registers per thread of the step kernel (for the tuner and the docs).
     int (*step_registers)(bool smag);
-    // One fused step with two neighbouring nodes per thread (nx even):
-    // `block` threads cover 2 * block nodes of a row.
-    cudaError_t (*step_pairs)(const Geom3D& g, const void* phys, const void* src, void* dst,
-                              const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s);
-    int (*pairs_registers)(bool smag);
     // Persistent step over a device table of n Lattice3D entries of the
     // storage's arithmetic type (staged3d.cuh): `grid` CTAs of `block`
     // consumer threads (128 or 256) plus a producer warp, spans of

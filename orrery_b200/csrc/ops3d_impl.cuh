@@ -29,32 +29,6 @@ template <class S> struct Launch3D {
         return cudaGetLastError();
     }
 
-    static cudaError_t step_pairs(const Geom3D& g, const void* phys, const void* src, void* dst,
-                                  const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s) {
-        if (g.nx % 2 != 0 || block == 0) {
-            return cudaErrorInvalidValue;
-        }
-        Geom3D gg = g;
-        gg.tiles_x = (g.nx / 2 + block - 1) / block;
-        const dim3 grid(gg.tiles_x, g.ny, g.nz);
-        const auto& p = *static_cast<const Phys3D<A>*>(phys);
-        if (smag) {
-            step3d_pairs_kernel<S, true><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
-                                                                static_cast<S*>(dst), b);
-        } else {
-            step3d_pairs_kernel<S, false><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
-                                                                 static_cast<S*>(dst), b);
-        }
-        return cudaGetLastError();
-    }
-
-    static int pairs_registers(bool smag) {
-        cudaFuncAttributes a{};
-        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, step3d_pairs_kernel<S, true>)
-                                   : cudaFuncGetAttributes(&a, step3d_pairs_kernel<S, false>);
-        return e == cudaSuccess ? a.numRegs : -1;
-    }
-
     static cudaError_t init(const Geom3D& g, const uint8_t* cls, const double* rho,
                             const double* ux, const double* uy, const double* uz, double r0,
                             double u0x, double u0y, double u0z, void* f0, cudaStream_t s) {
@@ -225,9 +199,8 @@ template <class S> struct Launch3D {
     }
 
     static const Ops3D& table() {
-        static const Ops3D ops{&step,        &init,        &history,          &moments,
-                               &force,       &mass,        &step_registers,   &step_pairs,
-                               &pairs_registers, &staged,  &staged_occupancy, &staged_smem,
+        static const Ops3D ops{&step,   &init,   &history,        &moments,          &force,
+                               &mass,   &step_registers, &staged, &staged_occupancy, &staged_smem,
                                &staged_registers, &force_batch};
         return ops;
     }

@@ -187,11 +187,8 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         if (o.block_x < 0 || o.block_x > 256 || (o.block_x % 32) != 0) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: block_x must be 0 or a multiple of 32 up to 256"};
         }
-        if (o.kernel < ORR_KERNEL_AUTO || o.kernel > ORR_KERNEL_PAIRS) {
+        if (o.kernel < ORR_KERNEL_AUTO || o.kernel > ORR_KERNEL_STAGED) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: unknown step kernel"};
-        }
-        if (o.kernel == ORR_KERNEL_PAIRS && config->nx % 2 != 0) {
-            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the two-node row step needs an even nx"};
         }
         if (o.kernel == ORR_KERNEL_STAGED && o.block_x != 0 && o.block_x != 128 && o.block_x != 256) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step takes block_x 128 or 256"};
@@ -341,7 +338,6 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
                 h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
             }
         }
-        h->pairs = !h->persistent && o.kernel == ORR_KERNEL_PAIRS;
         initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
         check(cudaStreamSynchronize(s), "create");
         // The per-node tables are on the device now; keep the links.
@@ -602,12 +598,6 @@ orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info)
             k.nodes_per_thread = solver->shape.npt;
             k.staged_items = solver->items.staged;
             k.direct_items = solver->items.direct;
-        } else if (solver->pairs) {
-            k.kernel = ORR_KERNEL_PAIRS;
-            k.block = solver->block;
-            k.nodes_per_thread = 2;
-            k.grid = ((solver->g.nx / 2 + solver->block - 1) / solver->block) * solver->g.ny * solver->g.nz;
-            k.registers = solver->ops->pairs_registers(solver->smag);
         } else {
             k.kernel = ORR_KERNEL_ROWS;
             k.block = solver->block;

@@ -106,7 +106,6 @@ struct orr_lbm3d {
     void* f[2] = {nullptr, nullptr};
     int cur = 0;
     bool persistent = false;  // the staged persistent step runs the steps
-    bool pairs = false;       // the two-node row step runs the steps
     StagedShape shape{};
     ItemCounts items{};
     void* table = nullptr;
@@ -202,9 +201,6 @@ struct orr_lbm3d {
         if (persistent) {
             check(ops->staged(host_table, table, 1, items.staged, items.direct, static_cast<uint32_t>(from),
                               shape.stages, smag, shape.block, shape.npt, shape.grid, status(), stream),
-                  "step kernel");
-        } else if (pairs) {
-            check(ops->step_pairs(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream),
                   "step kernel");
         } else {
             check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream),

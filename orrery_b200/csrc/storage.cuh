@@ -30,12 +30,6 @@ template <> struct Storage<float> {
     static constexpr bool kShifted = true;
     __device__ __forceinline__ static A load(const float* p) { return __ldg(p); }
     __device__ __forceinline__ static A value(float v) { return v; }
-    // Two neighbouring values p[0], p[1] (p aligned to 2 values).
-    __device__ __forceinline__ static void load2(const float* p, A& a, A& b) {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-        a = v.x;
-        b = v.y;
-    }
     __device__ __forceinline__ static void store(float* p, A v) { *p = v; }
     __host__ __device__ static float encode(double shifted) { return static_cast<float>(shifted); }
     __host__ __device__ static double decode(float s) { return static_cast<double>(s); }
@@ -48,11 +42,6 @@ template <> struct Storage<__half> {
         return __half2float(__ldg(p));
     }
     __device__ __forceinline__ static A value(__half v) { return __half2float(v); }
-    __device__ __forceinline__ static void load2(const __half* p, A& a, A& b) {
-        const __half2 v = __ldg(reinterpret_cast<const __half2*>(p));
-        a = __low2float(v);
-        b = __high2float(v);
-    }
     __device__ __forceinline__ static void store(__half* p, A v) {
         *p = __float2half_rn(v);
     }
@@ -71,11 +60,6 @@ template <> struct Storage<__nv_bfloat16> {
         return __bfloat162float(__ldg(p));
     }
     __device__ __forceinline__ static A value(__nv_bfloat16 v) { return __bfloat162float(v); }
-    __device__ __forceinline__ static void load2(const __nv_bfloat16* p, A& a, A& b) {
-        const __nv_bfloat162 v = __ldg(reinterpret_cast<const __nv_bfloat162*>(p));
-        a = __low2float(v);
-        b = __high2float(v);
-    }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, A v) {
         *p = __float2bfloat16_rn(v);
     }
@@ -92,11 +76,6 @@ template <> struct Storage<double> {
     static constexpr bool kShifted = false;
     __device__ __forceinline__ static A load(const double* p) { return __ldg(p); }
     __device__ __forceinline__ static A value(double v) { return v; }
-    __device__ __forceinline__ static void load2(const double* p, A& a, A& b) {
-        const double2 v = __ldg(reinterpret_cast<const double2*>(p));
-        a = v.x;
-        b = v.y;
-    }
     __device__ __forceinline__ static void store(double* p, A v) { *p = v; }
     __host__ __device__ static double encode(double unshifted) { return unshifted; }
     __host__ __device__ static double decode(double s) { return s; }

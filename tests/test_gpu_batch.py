@@ -44,7 +44,7 @@ def solvers(storage):
 # (kernel, block, stages, nodes per thread, graph branches)
 SCHEDULES = [("staged", 256, 2, 2, 0), ("staged", 256, 3, 1, 0), ("staged", 128, 4, 2, 0),
              ("staged", 256, 2, 2, 64), ("staged", 256, 2, 1, 3), ("rows", 128, 0, 0, 0),
-             ("rows", 256, 0, 0, 2), ("pairs", 128, 0, 0, 0), ("pairs", 128, 0, 0, 64)]
+             ("rows", 256, 0, 0, 2)]
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])

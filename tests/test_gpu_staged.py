@@ -85,23 +85,6 @@ def test_staged_equals_rows_bitwise(name, storage):
     assert np.allclose(ga, gb, rtol=0, atol=1e-12 * np.max(np.abs(ga)))
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
-@pytest.mark.parametrize("name", CASES)
-def test_pairs_equals_rows_bitwise(name, storage):
-    """The two-node row kernel finishes each node like the one-node one."""
-    cfg, mask = case(name)
-    a = run(cfg, mask, storage, "rows")
-    b = run(cfg, mask, storage, "pairs")
-    assert b.kernel_info()["kernel"] == "pairs"
-    assert np.array_equal(a.populations(), b.populations())
-
-
-def test_pairs_refuses_odd_nx():
-    cfg, mask = sphere_channel(41, 16, 16, 6.0, 2.5, 0.05, 30.0)
-    with pytest.raises(S.LbmError):
-        S.make_gpu_solver(cfg, mask, kernel="pairs")
-
-
 @pytest.mark.parametrize("block,stages,npt", [(128, 1, 1), (128, 3, 2), (256, 2, 1), (256, 4, 1), (256, 2, 2),
                                               (256, 3, 2)])
 @pytest.mark.parametrize("name", ["sphere_les", "ragged_tile", "interpolated_convective_sponge"])
