@@ -43,17 +43,18 @@ def measured_peak():
 
 def dram_traffic(workload: str, storage: str):
     """Per-launch DRAM bytes (read + write) of the step kernel from the
-    committed ncu summary of this workload (the profiles/ line
-    'traffic_bytes_per_step <storage> <bytes>')."""
-    path = os.path.join(ROOT, "profiles", f"step3d_{workload}.md")
-    try:
-        with open(path) as fh:
-            for line in fh:
-                parts = line.split()
-                if len(parts) == 3 and parts[0] == "traffic_bytes_per_step" and parts[1] == storage:
-                    return float(parts[2])
-    except OSError:
-        pass
+    committed ncu summaries of this workload (a profiles/step3d_*<workload>.md
+    line 'traffic_bytes_per_step <storage> <bytes>')."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"step3d_*{workload}.md"))):
+        try:
+            with open(path) as fh:
+                for line in fh:
+                    parts = line.split()
+                    if len(parts) == 3 and parts[0] == "traffic_bytes_per_step" and parts[1] == storage:
+                        return float(parts[2])
+        except OSError:
+            pass
     return None
 
 
