@@ -36,6 +36,10 @@ struct Geom3D {
     int32_t forced;           // a body force is set (Guo forcing)
     int32_t sponge;           // absorbing layers active
     uint32_t sponge_inlet, sponge_outlet, sponge_sides;
+    // Every source resolves to one stored value or an inlet unknown: y and z
+    // sides periodic or free-slip, halfway solid walls, zero-gradient outlet
+    // (gather_flat3 then serves face and boundary nodes).
+    int32_t flat;
 };
 
 // Real parameters in the arithmetic type (binary32 parameters are the
@@ -630,6 +634,56 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
     }
 }
 
+// General gather of a lattice with g.flat set: the rules of gather_one3 for
+// periodic / free-slip sides, the inlet unknowns, the zero-gradient outlet
+// and halfway bounce-back, in which every direction's value is one stored
+// population (or 0 for an inlet unknown).  The source of each direction is
+// resolved with integer selects first and the 19 loads are then independent,
+// so a face or boundary node waits for one round trip instead of a chain.
+template <class S>
+__device__ __forceinline__ void gather_flat3(const Geom3D& g, const S* __restrict__ src, uint32_t mask,
+                                             int x, int y, int z, uint64_t here,
+                                             typename Storage<S>::A (&f)[d3::Q]) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const int nx = static_cast<int>(g.nx), ny = static_cast<int>(g.ny), nz = static_cast<int>(g.nz);
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        int sx = x - d3::cx(i), sy = y - d3::cy(i), sz = z - d3::cz(i);
+        int dir = i;
+        if (d3::cy(i) != 0 && (sy < 0 || sy >= ny)) {
+            const bool periodic = (sy < 0 ? g.y_lo : g.y_hi) == ORR_WALL_PERIODIC;
+            sy = periodic ? (sy < 0 ? ny - 1 : 0) : y;
+            dir = periodic ? dir : d3::mirror_y(i);
+        }
+        if (d3::cz(i) != 0 && (sz < 0 || sz >= nz)) {
+            const bool periodic = (sz < 0 ? g.z_lo : g.z_hi) == ORR_WALL_PERIODIC;
+            sz = periodic ? (sz < 0 ? nz - 1 : 0) : z;
+            // Mirror of the (possibly already mirrored) direction.
+            const int mz = dir == i ? d3::mirror_z(i) : d3::mirror_z(d3::mirror_y(i));
+            dir = periodic ? dir : mz;
+        }
+        bool unknown = false, xside = false;
+        if (d3::cx(i) != 0 && (sx < 0 || sx >= nx)) {
+            if (g.x_mode == ORR_X_PERIODIC) {
+                sx = sx < 0 ? nx - 1 : 0;
+            } else {
+                // Inlet unknown (reconstructed by the inlet) or the
+                // zero-gradient outlet copy; neither takes the solid test.
+                xside = true;
+                unknown = sx < 0;
+                sx = sx < 0 ? 0 : nx - 1;
+            }
+        }
+        uint64_t at = static_cast<uint64_t>(dir) * g.cells + static_cast<uint64_t>(sx) +
+                      static_cast<uint64_t>(nx) * (static_cast<uint64_t>(sy) + static_cast<uint64_t>(ny) * sz);
+        if (!xside && ((mask >> i) & 1u) != 0u) {
+            at = static_cast<uint64_t>(d3::opposite(i)) * g.cells + here; // halfway: f*_opp(x)
+        }
+        f[i] = unknown ? A(0) : T::load(src + at);
+    }
+}
+
 // Convective outlet at x = nx - 1 (outlet_value, lbm3d_cpu.cpp:239-250): the
 // zero-gradient copies in f (c_x < 0) are blended with the node's history;
 // nothing for the extrapolation outlet.
@@ -742,6 +796,9 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
             f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
         }
         bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
+    } else if (g.flat) {
+        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+        gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
     } else {
         const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
         const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;

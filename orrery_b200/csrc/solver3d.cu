@@ -243,6 +243,12 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         g.sponge_inlet = static_cast<uint32_t>(config->sponge_inlet);
         g.sponge_outlet = static_cast<uint32_t>(config->sponge_outlet);
         g.sponge_sides = static_cast<uint32_t>(config->sponge_sides);
+        const auto open_side = [](const orr_wall& w) {
+            return w.kind == ORR_WALL_PERIODIC || w.kind == ORR_WALL_SLIP;
+        };
+        g.flat = open_side(config->y_low) && open_side(config->y_high) && open_side(config->z_low) &&
+                 open_side(config->z_high) && config->solid_wall == ORR_SOLID_HALFWAY &&
+                 (config->x_boundary == ORR_X_PERIODIC || config->outlet == ORR_OUTLET_EXTRAPOLATION);
         const bool binary32 = o.storage != ORR_STORAGE_F64;
         if (binary32) {
             g.forced = to_f32(config->body_force_x) != 0.0f || to_f32(config->body_force_y) != 0.0f ||

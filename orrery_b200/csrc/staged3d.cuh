@@ -18,7 +18,8 @@
 //                  the per-node gather of step_node3 from global memory.
 // Items of all lattices are numbered globally (prefix offsets in the lattice
 // table) and CTA b takes items b, b + G, b + 2G, ... so that the CTAs in
-// flight work on neighbouring spans, as a one-shot grid would.
+// flight work on neighbouring spans, as a one-shot grid would.  A CTA takes
+// its direct items at a point of its span loop of its own.
 //
 // Pipeline.  A CTA has B consumer threads and one producer warp.  The
 // producer keeps up to `stages` items in flight: for each it waits until
@@ -246,7 +247,21 @@ __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typen
         }
         return;
     }
-    if (cls == kBoundary) {
+    if (cls == kBoundary && g.flat) {
+        const uint32_t mask = b.nmask[here];
+        if (x == 0u || x + 1u == g.nx) {
+            gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
+        } else {
+            // Halfway bounce-back: the staged pull of every solid-source
+            // direction is replaced by f*_opp at the node (independent loads).
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                if ((mask >> i) & 1u) {
+                    f[i] = T::load(src + static_cast<uint64_t>(d3::opposite(i)) * g.cells + here);
+                }
+            }
+        }
+    } else if (cls == kBoundary) {
         const uint32_t mask = b.nmask[here];
         const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
         if (x == 0u || x + 1u == g.nx) {
@@ -371,23 +386,35 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             }
         }
     } else {
-        // ---- consumer warps: direct items first, while the first stages load
-        for (uint32_t d = blockIdx.x; d < direct_total; d += G) {
-            const uint32_t l = kSingle ? 0u : find_lattice<A, false>(lats, n, d);
-            const Lattice3D<A>& L = table[kSingle ? 0u : l];
-            const uint32_t tiles = L.g.tiles_x;
-            const uint32_t local = d - static_cast<uint32_t>(L.direct_begin);
-            const uint32_t x = (local % tiles) * B + tid;
-            uint32_t y, z;
-            direct_row(L.g, L.staged != 0, local / tiles, y, z);
-            if (x < L.g.nx) {
-                const uint32_t from = L.parity ^ flip;
-                step_node3<S, kSmag>(L.g, L.p, static_cast<const S*>(L.f[from]),
-                                     static_cast<S*>(L.f[from ^ 1u]), L.b, x, y, z);
+        // ---- consumer warps.  The direct items (face rows, unstaged
+        // lattices) wait on global loads; each CTA takes them at its own
+        // point of the span loop, so that other CTAs' span work hides the
+        // waits (all at the start, they would stall every CTA at once).
+        const auto run_direct = [&]() {
+            for (uint32_t d = blockIdx.x; d < direct_total; d += G) {
+                const uint32_t l = kSingle ? 0u : find_lattice<A, false>(lats, n, d);
+                const Lattice3D<A>& L = table[kSingle ? 0u : l];
+                const uint32_t tiles = L.g.tiles_x;
+                const uint32_t local = d - static_cast<uint32_t>(L.direct_begin);
+                const uint32_t x = (local % tiles) * B + tid;
+                uint32_t y, z;
+                direct_row(L.g, L.staged != 0, local / tiles, y, z);
+                if (x < L.g.nx) {
+                    const uint32_t from = L.parity ^ flip;
+                    step_node3<S, kSmag>(L.g, L.p, static_cast<const S*>(L.f[from]),
+                                         static_cast<S*>(L.f[from ^ 1u]), L.b, x, y, z);
+                }
             }
+        };
+        const uint32_t direct_at = count > 0 ? static_cast<uint32_t>((blockIdx.x * 2654435761ull) % count) : 0u;
+        if (count == 0) {
+            run_direct();
         }
         uint32_t s = 0, phase = 0;
         for (uint32_t j = 0; j < count; ++j) {
+            if (j == direct_at) {
+                run_direct();
+            }
             if (!mbar_wait_bounded(smem_u32(full + s), phase, abort_word)) {
                 if (lane == 0) {
                     *abort_word = 1u;
