@@ -285,7 +285,7 @@ orr_status orr_batch3d_tune(orr_batch3d* batch, uint32_t graphs_per_trial, orr_b
         uint32_t n = 0;
         for (const Candidate& c : kCandidates) {
             if (c.kernel == ORR_KERNEL_STAGED &&
-                b->ops->staged_occupancy(b->smag, c.block, c.npt, c.stages) <= 0) {
+                (!b->all_flat() || b->ops->staged_occupancy(b->smag, c.block, c.npt, c.stages) <= 0)) {
                 continue;
             }
             b->kernel = c.kernel;

@@ -209,6 +209,10 @@ struct orr_batch3d {
             return;
         }
         if (kernel == ORR_KERNEL_STAGED) {
+            if (!all_flat()) {
+                throw Refusal{ORR_ERR_INVALID, "batch3d: the staged step needs members with periodic or "
+                                               "free-slip sides, halfway walls and a zero-gradient outlet"};
+            }
             shape = staged_shape(*ops, smag, block, npt ? npt : default_npt(storage), stages, device);
             if (shape.per_sm <= 0) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the staged step cannot launch with this shape"};
@@ -262,6 +266,13 @@ struct orr_batch3d {
     }
 
     bool branched() const { return branches > 0; }
+
+    bool all_flat() const {
+        for (const orr_lbm3d* m : members) {
+            if (!m->g.flat) return false;
+        }
+        return true;
+    }
 
     // One row-tile step of member m from buffer `from` on stream s.
     void member_step(orr_lbm3d* m, uint32_t from, cudaStream_t s) {

@@ -769,7 +769,7 @@ __device__ __forceinline__ void bulk_edges3(const Geom3D& g, const Phys3D<typena
 //               gather, whose side rules are uniform along the row;
 //   boundary    a node with a solid source (bounce-back / interpolated wall):
 //               the general gather with the plan's per-node direction mask.
-template <class S, bool kSmag>
+template <class S, bool kSmag, bool kFlat>
 __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
                                            const S* __restrict__ src, S* __restrict__ dst,
                                            const StepBuffers3D& b, uint32_t x, uint32_t y,
@@ -778,33 +778,70 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
     using T = Storage<S>;
     const uint64_t cells = g.cells;
     const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
-    const uint8_t cls = b.cls[here];
-    if (cls == kSolid) {
-#pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
-            T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
-        }
-        return;
-    }
     A f[d3::Q];
-    if (cls == kBulk) {
-        const int64_t nx = g.nx, plane = g.plane;
+    if constexpr (kFlat) {
+        // Interior rows: every plain pull address lies inside the lattice, so
+        // the 19 pulls are issued together with the class load (no dependent
+        // round trip) and then used, overridden or dropped by class.
+        const bool interior = (y - 1u < g.ny - 2u) && (z - 1u < g.nz - 2u);
+        if (interior) {
+            const int64_t nx = g.nx, plane = g.plane;
 #pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
-            const int64_t source = static_cast<int64_t>(here) -
-                                   (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-            f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+            for (int i = 0; i < d3::Q; ++i) {
+                const int64_t source = static_cast<int64_t>(here) -
+                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+            }
         }
-        bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
-    } else if (g.flat) {
-        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
-        gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
+        const uint8_t cls = b.cls[here];
+        if (cls == kSolid) {
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
+            }
+            return;
+        }
+        if (cls == kBulk) {
+            bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
+        } else if (interior && x != 0u && x + 1u != g.nx) {
+            // Boundary node of an interior row: halfway bounce-back replaces
+            // the pulls of its solid-source directions by f*_opp at the node.
+            const uint32_t mask = b.nmask[here];
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                if ((mask >> i) & 1u) {
+                    f[i] = T::load(src + static_cast<uint64_t>(d3::opposite(i)) * cells + here);
+                }
+            }
+        } else {
+            const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+            gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
+        }
     } else {
-        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
-        const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
-        A wall_rho = A(-1);
-        gather_all3<S, 0, true>(g, p, src, b, slot, mask, static_cast<int>(x), static_cast<int>(y),
-                                static_cast<int>(z), here, wall_rho, f);
+        const uint8_t cls = b.cls[here];
+        if (cls == kSolid) {
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
+            }
+            return;
+        }
+        if (cls == kBulk) {
+            const int64_t nx = g.nx, plane = g.plane;
+#pragma unroll
+            for (int i = 0; i < d3::Q; ++i) {
+                const int64_t source = static_cast<int64_t>(here) -
+                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
+            }
+            bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
+        } else {
+            const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+            const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
+            A wall_rho = A(-1);
+            gather_all3<S, 0, true>(g, p, src, b, slot, mask, static_cast<int>(x), static_cast<int>(y),
+                                    static_cast<int>(z), here, wall_rho, f);
+        }
     }
     if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
         inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
@@ -816,7 +853,9 @@ template <class S> constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A)
 
 // Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B)
 // of row (y, z).
-template <class S, bool kSmag>
+// kFlat: the lattice has g.flat set (the independent-load gather; the
+// general one otherwise).
+template <class S, bool kSmag, bool kFlat>
 __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
                                                         const S* __restrict__ src,
                                                         S* __restrict__ dst, StepBuffers3D b) {
@@ -824,7 +863,7 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
     if (x >= g.nx) {
         return;
     }
-    step_node3<S, kSmag>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
+    step_node3<S, kSmag, kFlat>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------ init / misc --

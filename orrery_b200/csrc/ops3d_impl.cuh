@@ -19,12 +19,20 @@ template <class S> struct Launch3D {
         gg.tiles_x = (g.nx + block - 1) / block;
         const dim3 grid(gg.tiles_x, g.ny, g.nz);
         const auto& p = *static_cast<const Phys3D<A>*>(phys);
+        const auto* in = static_cast<const S*>(src);
+        auto* out = static_cast<S*>(dst);
         if (smag) {
-            step3d_kernel<S, true><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
-                                                          static_cast<S*>(dst), b);
+            if (g.flat) {
+                step3d_kernel<S, true, true><<<grid, block, 0, s>>>(gg, p, in, out, b);
+            } else {
+                step3d_kernel<S, true, false><<<grid, block, 0, s>>>(gg, p, in, out, b);
+            }
         } else {
-            step3d_kernel<S, false><<<grid, block, 0, s>>>(gg, p, static_cast<const S*>(src),
-                                                           static_cast<S*>(dst), b);
+            if (g.flat) {
+                step3d_kernel<S, false, true><<<grid, block, 0, s>>>(gg, p, in, out, b);
+            } else {
+                step3d_kernel<S, false, false><<<grid, block, 0, s>>>(gg, p, in, out, b);
+            }
         }
         return cudaGetLastError();
     }
@@ -79,8 +87,8 @@ template <class S> struct Launch3D {
 
     static int step_registers(bool smag) {
         cudaFuncAttributes a{};
-        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, step3d_kernel<S, true>)
-                                   : cudaFuncGetAttributes(&a, step3d_kernel<S, false>);
+        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, step3d_kernel<S, true, true>)
+                                   : cudaFuncGetAttributes(&a, step3d_kernel<S, false, true>);
         return e == cudaSuccess ? a.numRegs : -1;
     }
 

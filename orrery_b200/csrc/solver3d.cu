@@ -319,8 +319,12 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         // automatically for the 2-byte storage forms when the lattice's rows
         // can be staged (there it is the faster one; for binary32 and
         // binary64 the row-tile step is).
+        if (o.kernel == ORR_KERNEL_STAGED && !g.flat) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step needs periodic or free-slip sides, "
+                                           "halfway walls and a zero-gradient outlet"};
+        }
         const bool want = o.kernel == ORR_KERNEL_STAGED ||
-                          (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && stageable(g) &&
+                          (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && g.flat && stageable(g) &&
                            (o.block_x == 0 || o.block_x == 128 || o.block_x == 256));
         if (want) {
             const uint32_t sblock = o.block_x == 128 ? 128u : 256u;

@@ -2,6 +2,9 @@
 // every interior row tile staged in shared memory by bulk asynchronous
 // copies (cp.async.bulk, completion on an mbarrier).
 //
+// The kernel serves lattices with g.flat set (periodic or free-slip sides,
+// halfway walls, zero-gradient outlet), whose every pull is one stored value.
+//
 // Work items.
 //   staged items   spans of N = NPT * B consecutive nodes (flattened order) of
 //                  the interior rows (1 <= y <= ny-2) of an interior z-plane
@@ -18,8 +21,7 @@
 //                  the per-node gather of step_node3 from global memory.
 // Items of all lattices are numbered globally (prefix offsets in the lattice
 // table) and CTA b takes items b, b + G, b + 2G, ... so that the CTAs in
-// flight work on neighbouring spans, as a one-shot grid would.  A CTA takes
-// its direct items at a point of its span loop of its own.
+// flight work on neighbouring spans, as a one-shot grid would.
 //
 // Pipeline.  A CTA has B consumer threads and one producer warp.  The
 // producer keeps up to `stages` items in flight: for each it waits until
@@ -206,28 +208,6 @@ __device__ __forceinline__ void direct_row(const Geom3D& g, bool staged, uint64_
 
 // --------------------------------------------------------- node finish --
 
-// Bounce-back overrides of a boundary node of an interior row away from the
-// x edges: the staged value of every direction whose source is solid is
-// replaced by the reflected population (gather_one3's solid branch).
-template <class S, int I>
-__device__ __forceinline__ void reflect_masked3(const Geom3D& g, const StepBuffers3D& b,
-                                                const S* __restrict__ src, uint32_t mask,
-                                                int32_t slot, uint64_t here,
-                                                typename Storage<S>::A (&f)[d3::Q]) {
-    using A = typename Storage<S>::A;
-    if constexpr (I < d3::Q) {
-        if ((mask >> I) & 1u) {
-            const A q = slot >= 0 ? static_cast<const A*>(b.wall_q)[static_cast<uint64_t>(slot) * d3::Q + I]
-                                  : A(0.5);
-            const int64_t farther_off = static_cast<int64_t>(d3::cx(I)) +
-                                        static_cast<int64_t>(g.nx) * d3::cy(I) +
-                                        static_cast<int64_t>(g.plane) * d3::cz(I);
-            f[I] = reflected3<S, I>(src, g.cells, here, farther_off, q);
-        }
-        reflect_masked3<S, I + 1>(g, b, src, mask, slot, here, f);
-    }
-}
-
 // Finish of a staged node: f holds the 19 plain pulls of the node, and for a
 // bulk node at the outlet (x = nx - 1, inflow / outflow) already the
 // zero-gradient copies of its c_x < 0 directions (the consumer loop takes
@@ -247,7 +227,7 @@ __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typen
         }
         return;
     }
-    if (cls == kBoundary && g.flat) {
+    if (cls == kBoundary) {
         const uint32_t mask = b.nmask[here];
         if (x == 0u || x + 1u == g.nx) {
             gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
@@ -260,16 +240,6 @@ __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typen
                     f[i] = T::load(src + static_cast<uint64_t>(d3::opposite(i)) * g.cells + here);
                 }
             }
-        }
-    } else if (cls == kBoundary) {
-        const uint32_t mask = b.nmask[here];
-        const int32_t slot = b.nslot != nullptr ? b.nslot[here] : -1;
-        if (x == 0u || x + 1u == g.nx) {
-            A wall_rho = A(-1);
-            gather_all3<S, 0, true>(g, p, src, b, slot, mask, static_cast<int>(x), static_cast<int>(y),
-                                    static_cast<int>(z), here, wall_rho, f);
-        } else {
-            reflect_masked3<S, 0>(g, b, src, mask, slot, here, f);
         }
     } else if (x + 1u == g.nx && g.x_mode == ORR_X_INFLOW_OUTFLOW) {
         convective_blend3<S>(g, p, b, y, z, f);
@@ -386,10 +356,8 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             }
         }
     } else {
-        // ---- consumer warps.  The direct items (face rows, unstaged
-        // lattices) wait on global loads; each CTA takes them at its own
-        // point of the span loop, so that other CTAs' span work hides the
-        // waits (all at the start, they would stall every CTA at once).
+        // ---- consumer warps: the direct items (face rows, unstaged
+        // lattices) first, while the first stages load.
         const auto run_direct = [&]() {
             for (uint32_t d = blockIdx.x; d < direct_total; d += G) {
                 const uint32_t l = kSingle ? 0u : find_lattice<A, false>(lats, n, d);
@@ -401,20 +369,14 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
                 direct_row(L.g, L.staged != 0, local / tiles, y, z);
                 if (x < L.g.nx) {
                     const uint32_t from = L.parity ^ flip;
-                    step_node3<S, kSmag>(L.g, L.p, static_cast<const S*>(L.f[from]),
-                                         static_cast<S*>(L.f[from ^ 1u]), L.b, x, y, z);
+                    step_node3<S, kSmag, true>(L.g, L.p, static_cast<const S*>(L.f[from]),
+                                               static_cast<S*>(L.f[from ^ 1u]), L.b, x, y, z);
                 }
             }
         };
-        const uint32_t direct_at = count > 0 ? static_cast<uint32_t>((blockIdx.x * 2654435761ull) % count) : 0u;
-        if (count == 0) {
-            run_direct();
-        }
+        run_direct();
         uint32_t s = 0, phase = 0;
         for (uint32_t j = 0; j < count; ++j) {
-            if (j == direct_at) {
-                run_direct();
-            }
             if (!mbar_wait_bounded(smem_u32(full + s), phase, abort_word)) {
                 if (lane == 0) {
                     *abort_word = 1u;

@@ -12,33 +12,42 @@ from orrery_b200 import masks as M
 from orrery_b200 import solver as S
 from orrery_b200 import workloads as W
 from orrery_b200.batch import CudaBatch3D
-from orrery_b200.lbm3d import Outlet, Smagorinsky, SolidWall
+from orrery_b200.lbm3d import Outlet, Smagorinsky, SolidWall, WallKind, wall
 
 pytestmark = pytest.mark.gpu
 
 
-def lattices():
-    """Four lattices of different sizes and rules, all with the LES closure."""
+def lattices(general=False):
+    """Four lattices of different sizes and rules, all with the LES closure.
+    The default set has periodic or free-slip sides, halfway walls and the
+    zero-gradient outlet (every schedule takes it); `general` swaps in a
+    convective outlet, an interpolated wall and no-slip duct walls (row
+    schedules only)."""
     out = []
     cfg, mask = sphere_channel(64, 32, 32, 8.0, 2.5, 0.05, 20.0)
     cfg.smagorinsky = Smagorinsky(True, 0.1)
     out.append((cfg, mask))
-    cfg, mask = sphere_channel(272, 12, 10, 6.0, 4.0, 0.05, 30.0)     # ragged tile
+    cfg, mask = sphere_channel(272, 12, 10, 6.0, 4.0, 0.05, 30.0)     # spans end inside rows
     cfg.smagorinsky = Smagorinsky(True, 0.1)
-    cfg.outlet = Outlet.convective
+    if general:
+        cfg.outlet = Outlet.convective
     out.append((cfg, mask))
     cfg, mask = sphere_channel(40, 16, 16, 6.0, 2.5, 0.05, 30.0)      # rows not staged
     cfg.smagorinsky = Smagorinsky(True, 0.1)
-    cfg.solid_wall = SolidWall.interpolated
+    if general:
+        cfg.solid_wall = SolidWall.interpolated
     out.append((cfg, mask))
-    cfg = duct_config(48, 16, 12, 0.8, 1e-5)                            # periodic x, no-slip walls
+    cfg = duct_config(48, 16, 12, 0.8, 1e-5)                            # periodic x, body force
+    if not general:
+        cfg.y_low = cfg.y_high = wall(WallKind.periodic)
+        cfg.z_low = cfg.z_high = wall(WallKind.periodic)
     cfg.smagorinsky = Smagorinsky(True, 0.1)
     out.append((cfg, M.box_mask(48, 16, 12, (10, 4, 3), (16, 9, 8))))
     return out
 
 
-def solvers(storage):
-    return [S.make_gpu_solver(c, m, storage=storage) for c, m in lattices()]
+def solvers(storage, general=False):
+    return [S.make_gpu_solver(c, m, storage=storage) for c, m in lattices(general)]
 
 
 # (kernel, block, stages, nodes per thread, graph branches)
@@ -147,3 +156,25 @@ def test_reinitialised_member():
     a.initialize(*w)
     a.step(6)
     assert np.array_equal(a.populations(), b.populations())
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_general_members_take_row_schedules(storage):
+    """Members with a convective outlet, an interpolated wall or no-slip walls:
+    row schedules step them exactly as alone; the staged ones are refused."""
+    alone = solvers(storage, general=True)
+    for s in alone:
+        s.step(24)
+    members = solvers(storage, general=True)
+    batch = CudaBatch3D()
+    for s in members:
+        batch.add(s)
+    batch.set_schedule("staged", 256, 2, 1, 0)
+    with pytest.raises(S.LbmError):
+        batch.step(2)
+    batch.set_schedule("rows", 128, 0, 0, 3)
+    batch.step(24)
+    for a, b in zip(alone, members):
+        assert np.array_equal(a.populations(), b.populations())
+    trials = batch.tune(1)
+    assert all(t["kernel"] == "rows" for t in trials)

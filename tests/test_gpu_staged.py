@@ -4,11 +4,12 @@ Both kernels finish every node with the same device code (the staged kernel
 only changes where the 19 plain pulls come from: a shared-memory stage
 instead of global loads), so for every storage form they must give the same
 populations bit for bit.  The cases cover each rule the staged kernel has to
-route correctly: inlet and extrapolation / convective outlets at the x edges
-of interior rows, halfway and interpolated bounce-back next to staged
-values, periodic x with moving no-slip walls and a body force, the absorbing
-layers, row tiles that end inside a row (nx not a multiple of the tile) and
-lattices whose rows cannot be staged (every row on the per-node path).
+route correctly: the inlet and the zero-gradient outlet at the x edges of
+interior rows, halfway bounce-back next to staged values, periodic y and
+periodic x with a body force, the absorbing layers, spans that end inside a
+row or hold several rows, and lattices whose rows cannot be staged (every row
+on the per-node path).  Lattices with no-slip sides, interpolated walls or a
+convective outlet are refused by the staged kernel.
 """
 import numpy as np
 import pytest
@@ -28,18 +29,27 @@ def case(name):
         cfg, mask = sphere_channel(64, 32, 32, 8.0, 2.5, 0.05, 20.0)
         cfg.smagorinsky = Smagorinsky(True, 0.1)
         return cfg, mask
-    if name == "interpolated_convective_sponge":
+    if name == "sponge_periodic_y":
+        cfg, mask = sphere_channel(64, 24, 20, 7.0, 3.0, 0.05, 40.0)
+        cfg.sponge = Sponge(0.5, 6, 8, 4)
+        cfg.y_low = wall(WallKind.periodic)
+        cfg.y_high = wall(WallKind.periodic)
+        cfg.smagorinsky = Smagorinsky(True, 0.12)
+        return cfg, mask
+    if name == "periodic_box_obstacle":
+        # periodic in all three directions, body force, a box obstacle
+        cfg = duct_config(48, 16, 12, 0.8, 1e-5)
+        cfg.y_low = cfg.y_high = wall(WallKind.periodic)
+        cfg.z_low = cfg.z_high = wall(WallKind.periodic)
+        mask = M.box_mask(48, 16, 12, (10, 4, 3), (16, 9, 8))
+        return cfg, mask
+    if name == "interpolated_convective_no_slip":
+        # not staged: the rows kernel must refuse nothing, the staged one refuses
         cfg, mask = sphere_channel(64, 24, 20, 7.0, 3.0, 0.05, 40.0)
         cfg.solid_wall = SolidWall.interpolated
         cfg.outlet = Outlet.convective
-        cfg.sponge = Sponge(0.5, 6, 8, 4)
         cfg.z_low = wall(WallKind.no_slip, 0.01)
         cfg.z_high = wall(WallKind.no_slip, -0.02)
-        cfg.smagorinsky = Smagorinsky(True, 0.12)
-        return cfg, mask
-    if name == "periodic_duct_obstacle":
-        cfg = duct_config(48, 16, 12, 0.8, 1e-5)
-        mask = M.box_mask(48, 16, 12, (10, 4, 3), (16, 9, 8))
         return cfg, mask
     if name == "ragged_tile":
         # 272 = 256 + 16: the second tile of a 256-node row holds 16 nodes.
@@ -52,8 +62,7 @@ def case(name):
     raise KeyError(name)
 
 
-CASES = ["sphere_les", "interpolated_convective_sponge", "periodic_duct_obstacle", "ragged_tile",
-         "unaligned_rows"]
+CASES = ["sphere_les", "sponge_periodic_y", "periodic_box_obstacle", "ragged_tile", "unaligned_rows"]
 
 
 def run(cfg, mask, storage, kernel, block=0, stages=0, steps=STEPS, inlet=None, npt=0):
@@ -87,7 +96,7 @@ def test_staged_equals_rows_bitwise(name, storage):
 
 @pytest.mark.parametrize("block,stages,npt", [(128, 1, 1), (128, 3, 2), (256, 2, 1), (256, 4, 1), (256, 2, 2),
                                               (256, 3, 2)])
-@pytest.mark.parametrize("name", ["sphere_les", "ragged_tile", "interpolated_convective_sponge"])
+@pytest.mark.parametrize("name", ["sphere_les", "ragged_tile", "sponge_periodic_y"])
 def test_launch_shapes_agree(name, block, stages, npt):
     """Spans of one or two nodes per thread, across rows (64 and 272 nodes
     wide: spans hold several rows, or end inside one)."""
@@ -116,6 +125,14 @@ def test_automatic_choice():
     assert S.make_gpu_solver(cfg, mask, storage="f16").kernel_info()["kernel"] == "rows"
     cfg, mask = case("sphere_les")
     assert S.make_gpu_solver(cfg, mask, storage="f16", kernel="rows").kernel_info()["kernel"] == "rows"
+
+
+def test_staged_refuses_general_boundaries():
+    cfg, mask = case("interpolated_convective_no_slip")
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, storage="f16", kernel="staged")
+    # the automatic choice takes the row kernel for it
+    assert S.make_gpu_solver(cfg, mask, storage="f16").kernel_info()["kernel"] == "rows"
 
 
 def test_refused_shapes():
