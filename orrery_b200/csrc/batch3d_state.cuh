@@ -211,7 +211,7 @@ struct orr_batch3d {
         if (kernel == ORR_KERNEL_STAGED) {
             if (!all_flat()) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the staged step needs members with periodic or "
-                                               "free-slip sides, halfway walls and a zero-gradient outlet"};
+                                               "free-slip sides and halfway walls"};
             }
             shape = staged_shape(*ops, smag, block, npt ? npt : default_npt(storage), stages, device);
             if (shape.per_sm <= 0) {

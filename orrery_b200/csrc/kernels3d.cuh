@@ -36,9 +36,10 @@ struct Geom3D {
     int32_t forced;           // a body force is set (Guo forcing)
     int32_t sponge;           // absorbing layers active
     uint32_t sponge_inlet, sponge_outlet, sponge_sides;
-    // Every source resolves to one stored value or an inlet unknown: y and z
-    // sides periodic or free-slip, halfway solid walls, zero-gradient outlet
-    // (gather_flat3 then serves face and boundary nodes).
+    // Every source resolves to one stored value or an inlet unknown (the
+    // convective outlet then blends the zero-gradient copy): y and z sides
+    // periodic or free-slip, halfway solid walls (gather_flat3 then serves
+    // face and boundary nodes).
     int32_t flat;
 };
 
@@ -635,9 +636,10 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
 }
 
 // General gather of a lattice with g.flat set: the rules of gather_one3 for
-// periodic / free-slip sides, the inlet unknowns, the zero-gradient outlet
-// and halfway bounce-back, in which every direction's value is one stored
-// population (or 0 for an inlet unknown).  The source of each direction is
+// periodic / free-slip sides, the inlet unknowns, the outlet copy and
+// halfway bounce-back, in which every direction's value is one stored
+// population (or 0 for an inlet unknown).  At x = nx - 1 of an inflow /
+// outflow lattice the caller applies convective_blend3 to the copies.  The source of each direction is
 // resolved with integer selects first and the 19 loads are then independent,
 // so a face or boundary node waits for one round trip instead of a chain.
 template <class S>
@@ -769,6 +771,63 @@ __device__ __forceinline__ void bulk_edges3(const Geom3D& g, const Phys3D<typena
 //               gather, whose side rules are uniform along the row;
 //   boundary    a node with a solid source (bounce-back / interpolated wall):
 //               the general gather with the plan's per-node direction mask.
+// The rest of a node's step on a flat lattice once its pulls are in f (for
+// an interior row; elsewhere f is filled here): class, edge and wall rules,
+// the inlet, the collision and the 19 stores.
+template <class S, bool kSmag>
+__device__ __forceinline__ void flat_finish3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                             const S* __restrict__ src, S* __restrict__ dst,
+                                             const StepBuffers3D& b, typename Storage<S>::A (&f)[d3::Q],
+                                             uint8_t cls, bool interior, uint32_t x, uint32_t y, uint32_t z,
+                                             uint64_t here) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    const uint64_t cells = g.cells;
+    if (cls == kSolid) {
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
+        }
+        return;
+    }
+    if (cls == kBulk) {
+        bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
+    } else if (interior && x != 0u && x + 1u != g.nx) {
+        // Boundary node of an interior row: halfway bounce-back replaces
+        // the pulls of its solid-source directions by f*_opp at the node.
+        const uint32_t mask = b.nmask[here];
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            if ((mask >> i) & 1u) {
+                f[i] = T::load(src + static_cast<uint64_t>(d3::opposite(i)) * cells + here);
+            }
+        }
+    } else {
+        const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
+        gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
+        if (x + 1u == g.nx && g.x_mode == ORR_X_INFLOW_OUTFLOW) {
+            convective_blend3<S>(g, p, b, y, z, f);
+        }
+    }
+    if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
+        inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
+    }
+    finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
+}
+
+// The 19 plain pulls of node `here` (valid addresses for interior rows).
+template <class S>
+__device__ __forceinline__ void pull3(const Geom3D& g, const S* __restrict__ src, uint64_t here,
+                                      typename Storage<S>::A (&f)[d3::Q]) {
+    using T = Storage<S>;
+    const int64_t nx = g.nx, plane = g.plane;
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const int64_t source = static_cast<int64_t>(here) - (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+        f[i] = T::load(src + static_cast<uint64_t>(i) * g.cells + static_cast<uint64_t>(source));
+    }
+}
+
 template <class S, bool kSmag, bool kFlat>
 __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
                                            const S* __restrict__ src, S* __restrict__ dst,
@@ -785,38 +844,10 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
         // round trip) and then used, overridden or dropped by class.
         const bool interior = (y - 1u < g.ny - 2u) && (z - 1u < g.nz - 2u);
         if (interior) {
-            const int64_t nx = g.nx, plane = g.plane;
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                const int64_t source = static_cast<int64_t>(here) -
-                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
-            }
+            pull3<S>(g, src, here, f);
         }
-        const uint8_t cls = b.cls[here];
-        if (cls == kSolid) {
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
-            }
-            return;
-        }
-        if (cls == kBulk) {
-            bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
-        } else if (interior && x != 0u && x + 1u != g.nx) {
-            // Boundary node of an interior row: halfway bounce-back replaces
-            // the pulls of its solid-source directions by f*_opp at the node.
-            const uint32_t mask = b.nmask[here];
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                if ((mask >> i) & 1u) {
-                    f[i] = T::load(src + static_cast<uint64_t>(d3::opposite(i)) * cells + here);
-                }
-            }
-        } else {
-            const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
-            gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
-        }
+        flat_finish3<S, kSmag>(g, p, src, dst, b, f, b.cls[here], interior, x, y, z, here);
+        return;
     } else {
         const uint8_t cls = b.cls[here];
         if (cls == kSolid) {

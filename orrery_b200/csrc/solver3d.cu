@@ -247,8 +247,7 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             return w.kind == ORR_WALL_PERIODIC || w.kind == ORR_WALL_SLIP;
         };
         g.flat = open_side(config->y_low) && open_side(config->y_high) && open_side(config->z_low) &&
-                 open_side(config->z_high) && config->solid_wall == ORR_SOLID_HALFWAY &&
-                 (config->x_boundary == ORR_X_PERIODIC || config->outlet == ORR_OUTLET_EXTRAPOLATION);
+                 open_side(config->z_high) && config->solid_wall == ORR_SOLID_HALFWAY;
         const bool binary32 = o.storage != ORR_STORAGE_F64;
         if (binary32) {
             g.forced = to_f32(config->body_force_x) != 0.0f || to_f32(config->body_force_y) != 0.0f ||
@@ -320,8 +319,8 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         // can be staged (there it is the faster one; for binary32 and
         // binary64 the row-tile step is).
         if (o.kernel == ORR_KERNEL_STAGED && !g.flat) {
-            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step needs periodic or free-slip sides, "
-                                           "halfway walls and a zero-gradient outlet"};
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step needs periodic or free-slip sides "
+                                           "and halfway walls"};
         }
         const bool want = o.kernel == ORR_KERNEL_STAGED ||
                           (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && g.flat && stageable(g) &&

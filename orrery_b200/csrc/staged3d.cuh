@@ -3,7 +3,7 @@
 // copies (cp.async.bulk, completion on an mbarrier).
 //
 // The kernel serves lattices with g.flat set (periodic or free-slip sides,
-// halfway walls, zero-gradient outlet), whose every pull is one stored value.
+// halfway walls), whose every pull is one stored value.
 //
 // Work items.
 //   staged items   spans of N = NPT * B consecutive nodes (flattened order) of
@@ -231,6 +231,9 @@ __device__ __forceinline__ void staged_node3(const Geom3D& g, const Phys3D<typen
         const uint32_t mask = b.nmask[here];
         if (x == 0u || x + 1u == g.nx) {
             gather_flat3<S>(g, src, mask, static_cast<int>(x), static_cast<int>(y), static_cast<int>(z), here, f);
+            if (x + 1u == g.nx && g.x_mode == ORR_X_INFLOW_OUTFLOW) {
+                convective_blend3<S>(g, p, b, y, z, f);
+            }
         } else {
             // Halfway bounce-back: the staged pull of every solid-source
             // direction is replaced by f*_opp at the node (independent loads).

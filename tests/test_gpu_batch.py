@@ -19,10 +19,9 @@ pytestmark = pytest.mark.gpu
 
 def lattices(general=False):
     """Four lattices of different sizes and rules, all with the LES closure.
-    The default set has periodic or free-slip sides, halfway walls and the
-    zero-gradient outlet (every schedule takes it); `general` swaps in a
-    convective outlet, an interpolated wall and no-slip duct walls (row
-    schedules only)."""
+    The default set has periodic or free-slip sides and halfway walls (every
+    schedule takes it); `general` swaps in an interpolated wall and no-slip
+    duct walls (row schedules only)."""
     out = []
     cfg, mask = sphere_channel(64, 32, 32, 8.0, 2.5, 0.05, 20.0)
     cfg.smagorinsky = Smagorinsky(True, 0.1)
@@ -160,7 +159,7 @@ def test_reinitialised_member():
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 def test_general_members_take_row_schedules(storage):
-    """Members with a convective outlet, an interpolated wall or no-slip walls:
+    """Members with an interpolated wall or no-slip walls:
     row schedules step them exactly as alone; the staged ones are refused."""
     alone = solvers(storage, general=True)
     for s in alone:

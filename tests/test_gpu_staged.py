@@ -8,8 +8,8 @@ route correctly: the inlet and the zero-gradient outlet at the x edges of
 interior rows, halfway bounce-back next to staged values, periodic y and
 periodic x with a body force, the absorbing layers, spans that end inside a
 row or hold several rows, and lattices whose rows cannot be staged (every row
-on the per-node path).  Lattices with no-slip sides, interpolated walls or a
-convective outlet are refused by the staged kernel.
+on the per-node path).  Lattices with no-slip sides or interpolated walls are
+refused by the staged kernel.
 """
 import numpy as np
 import pytest
