@@ -195,7 +195,7 @@ def main(argv=None) -> int:
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
     ap.add_argument("--stages", type=int, default=0)
-    ap.add_argument("--npt", type=int, default=0, help="staged kernel: nodes per thread of a span")
+    ap.add_argument("--npt", type=int, default=0, help="nodes per thread of a staged span, or of the row kernel (2: the pair step)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"])
     ap.add_argument("--lattices", type=int, default=64, help="batched form: lattices")
     ap.add_argument("--requests", type=int, default=48, help="serve form: requests")

@@ -111,7 +111,10 @@ typedef struct orr_solver_options {
     int32_t block_x;          /* threads per block of the step kernel; 0 = tuned default */
     int32_t kernel;           /* ORR_KERNEL_*: the D3Q19 step kernel (0 = automatic) */
     int32_t stages;           /* pipeline stages of ORR_KERNEL_STAGED; 0 = tuned default */
-    int32_t nodes_per_thread; /* ORR_KERNEL_STAGED: 1 or 2 nodes per thread of a span; 0 = default */
+    int32_t nodes_per_thread; /* STAGED: 1 or 2 nodes per thread of a span; ROWS: 1, or 2
+                                 neighbouring nodes per thread (2-byte storage, periodic or
+                                 free-slip sides, halfway walls, even nx, block_x <= 128 only);
+                                 0 = default */
 } orr_solver_options;
 
 /* D3Q19 step kernels.  ROWS: one block per row tile, every population read
@@ -259,7 +262,9 @@ typedef struct orr_batch_schedule {
     uint32_t block;
     uint32_t stages;
     uint32_t grid;
-    uint32_t nodes_per_thread;   /* staged: 1 or 2 (0 = default) */
+    uint32_t nodes_per_thread;   /* staged: 1 or 2 nodes per thread of a span (0 = default);
+                                    rows: 2 takes two neighbouring nodes per thread on the
+                                    members that allow it (as orr_solver_options), 1 elsewhere */
     uint32_t branches;           /* 0: as above; n > 0: each member runs its own single-lattice
                                     launches (staged: a grid proportional to its nodes), the
                                     members spread over n parallel graph branches */

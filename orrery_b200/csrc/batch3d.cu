@@ -180,13 +180,16 @@ orr_status orr_batch3d_set_schedule(orr_batch3d* batch, const orr_batch_schedule
             if (s.block == 0 || s.block > 256 || s.block % 32 != 0) {
                 throw Refusal{ORR_ERR_INVALID, "batch3d: the row step takes a block of 32 to 256 threads"};
             }
+            if (s.nodes_per_thread > 2) {
+                throw Refusal{ORR_ERR_INVALID, "batch3d: nodes_per_thread must be 0 (default), 1 or 2"};
+            }
         } else {
             throw Refusal{ORR_ERR_INVALID, "batch3d: unknown step kernel"};
         }
         b->kernel = s.kernel;
         b->block = s.block;
         b->stages = s.kernel == ORR_KERNEL_STAGED ? s.stages : 0;
-        b->npt = s.kernel == ORR_KERNEL_STAGED ? s.nodes_per_thread : 0;
+        b->npt = s.nodes_per_thread;
         b->branches = s.branches;
         b->dirty = true;
         return ORR_OK;
@@ -204,7 +207,7 @@ orr_status orr_batch3d_schedule(const orr_batch3d* batch, orr_batch_schedule* sc
     s.grid = batch->kernel == ORR_KERNEL_STAGED ? batch->shape.grid : 0;
     s.nodes_per_thread = batch->kernel == ORR_KERNEL_STAGED
                              ? (batch->shape.npt && !batch->dirty ? batch->shape.npt : batch->npt)
-                             : 0;
+                             : (batch->npt == 2 ? 2u : 1u);
     s.branches = batch->branches;
     s.ms_per_step = 0.0;
     *schedule = s;

@@ -16,8 +16,8 @@
 namespace orr {
 
 // Candidate schedules of the autotuner (kernel, block, stages, nodes per
-// thread of a staged span, graph branches; 64 branches means one per member
-// up to 64).
+// thread of a staged span or of the row-tile step, graph branches: 64
+// branches means one per member up to 64).
 struct Candidate {
     int32_t kernel;
     uint32_t block;
@@ -30,6 +30,7 @@ inline constexpr Candidate kCandidates[] = {
     {ORR_KERNEL_STAGED, 256, 2, 2, 64}, {ORR_KERNEL_STAGED, 256, 3, 2, 64},
     {ORR_KERNEL_STAGED, 256, 4, 1, 64}, {ORR_KERNEL_STAGED, 128, 3, 2, 64},
     {ORR_KERNEL_ROWS, 128, 0, 0, 0},    {ORR_KERNEL_ROWS, 128, 0, 0, 64},
+    {ORR_KERNEL_ROWS, 128, 0, 2, 0},    {ORR_KERNEL_ROWS, 128, 0, 2, 64},
 };
 
 } // namespace orr
@@ -49,7 +50,8 @@ struct orr_batch3d {
     int32_t kernel = ORR_KERNEL_STAGED;
     uint32_t block = 256;
     uint32_t stages = 0;      // 0: the shape's default
-    uint32_t npt = 0;         // nodes per thread of a staged span, 0: the storage's default
+    uint32_t npt = 0;         // nodes per thread of a staged span (0: the storage's default),
+                              // or of the row-tile step (2: the pair step where it serves a member)
     uint32_t branches = 0;    // 0: one stream; else members spread over this many graph branches
     StagedShape shape{};
 
@@ -276,7 +278,8 @@ struct orr_batch3d {
 
     // One row-tile step of member m from buffer `from` on stream s.
     void member_step(orr_lbm3d* m, uint32_t from, cudaStream_t s) {
-        check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block, s),
+        check(ops->step(m->g, m->phys(), m->f[from], m->f[1 - from], m->buffers(), smag, block,
+                        npt == 2 ? 2u : 1u, s),
               "batch step kernel");
     }
 

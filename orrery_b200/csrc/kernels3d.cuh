@@ -371,6 +371,125 @@ __device__ __forceinline__ void absorb3(A (&f)[d3::Q], A s, const A* inlet) {
     }
 }
 
+// Two nodes at once in packed binary32 lanes (node A in .x, node B in .y).
+// Each helper rounds every lane like the scalar r_* operation it stands for
+// (a - b as the single-rounding fma(b, -1, a); -a as a * -1, exact), so the
+// pair collision gives the bits of two single-node collisions.
+__device__ __forceinline__ float2 v2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) { return __ffma2_rn(b, v2(-1.0f), a); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_neg(float2 a) { return __fmul2_rn(a, v2(-1.0f)); }
+__device__ __forceinline__ float2 p_rcp(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
+__device__ __forceinline__ float2 p_sqrt(float2 a) { return make_float2(fast_sqrt(a.x), fast_sqrt(a.y)); }
+
+// One opposite pair (plus member with c.u = cu, minus member with -cu) of two
+// nodes: the relaxation of relax_pairs2 lane by lane.
+__device__ __forceinline__ void relax_opposite2(float2& fp, float2& fm, float2 cu, float w, float2 r3, float2 base,
+                                                float2 rho45, float2 omega) {
+    const float2 even = p_mul(v2(w), p_fma(rho45, p_mul(cu, cu), base));
+    const float2 odd = p_mul(r3, cu);
+    const float2 eqp = p_add(even, odd);
+    const float2 eqm = p_sub(even, odd);
+    fp = p_fma(omega, p_sub(eqp, fp), fp);
+    fm = p_fma(omega, p_sub(eqm, fm), fm);
+}
+
+// The shifted binary32 collision of collide3 for two nodes, operation for
+// operation (each scalar operation there is one packed operation here, each
+// packed pair there two here).
+template <bool kSmag>
+__device__ __forceinline__ void collide3_pair(float2 (&f)[d3::Q], const Phys3D<float>& p, int forced) {
+    const float2 p1 = p_add(f[1], f[2]), p3 = p_add(f[3], f[4]), p5 = p_add(f[5], f[6]);
+    const float2 p7 = p_add(f[7], f[8]), p9 = p_add(f[9], f[10]), p11 = p_add(f[11], f[12]);
+    const float2 p13 = p_add(f[13], f[14]), p15 = p_add(f[15], f[16]), p17 = p_add(f[17], f[18]);
+    const float2 m1 = p_sub(f[1], f[2]), m3 = p_sub(f[3], f[4]), m5 = p_sub(f[5], f[6]);
+    const float2 m7 = p_sub(f[7], f[8]), m9 = p_sub(f[9], f[10]), m11 = p_sub(f[11], f[12]);
+    const float2 m13 = p_sub(f[13], f[14]), m15 = p_sub(f[15], f[16]), m17 = p_sub(f[17], f[18]);
+    const float2 drho = p_add(f[0], p_add(p_add(p_add(p1, p3), p_add(p5, p7)),
+                                          p_add(p_add(p9, p11), p_add(p_add(p13, p15), p17))));
+    const float2 jx = p_add(p_add(m1, m7), p_add(m9, p_add(m11, m13)));
+    const float2 jy = p_add(p_add(m3, m7), p_sub(p_add(m15, m17), m9));
+    const float2 jz = p_add(p_add(m5, m11), p_sub(p_sub(m15, m13), m17));
+    const float2 rho = p_add(v2(1.0f), drho);
+    const float2 inv = p_rcp(rho);
+    const float2 ux = p_mul(p_fma(v2(0.5f), v2(p.fx), jx), inv);
+    const float2 uy = p_mul(p_fma(v2(0.5f), v2(p.fy), jy), inv);
+    const float2 uz = p_mul(p_fma(v2(0.5f), v2(p.fz), jz), inv);
+    const float2 uu = p_fma(uz, uz, p_fma(uy, uy, p_mul(ux, ux)));
+    float2 omega;
+    if constexpr (kSmag) {
+        const float2 sxx = p_add(p_add(p1, p7), p_add(p9, p_add(p11, p13)));
+        const float2 syy = p_add(p_add(p3, p7), p_add(p9, p_add(p15, p17)));
+        const float2 szz = p_add(p_add(p5, p11), p_add(p13, p_add(p15, p17)));
+        const float2 sxy = p_sub(p7, p9);
+        const float2 sxz = p_sub(p11, p13);
+        const float2 syz = p_sub(p15, p17);
+        const float2 iso = p_mul(drho, v2(1.0f / 3.0f));
+        const float2 nrux = p_neg(p_mul(rho, ux)), nruy = p_neg(p_mul(rho, uy)), nruz = p_neg(p_mul(rho, uz));
+        const float2 pxx = p_fma(nrux, ux, p_sub(sxx, iso));
+        const float2 pyy = p_fma(nruy, uy, p_sub(syy, iso));
+        const float2 pzz = p_fma(nruz, uz, p_sub(szz, iso));
+        const float2 pxy = p_fma(nrux, uy, sxy);
+        const float2 pxz = p_fma(nrux, uz, sxz);
+        const float2 pyz = p_fma(nruy, uz, syz);
+        const float2 diag = p_fma(pzz, pzz, p_fma(pyy, pyy, p_mul(pxx, pxx)));
+        const float2 off = p_fma(pyz, pyz, p_fma(pxz, pxz, p_mul(pxy, pxy)));
+        const float2 strain = p_sqrt(p_fma(v2(2.0f), off, diag));
+        const float2 k = p_mul(p_mul(v2(r_mul(static_cast<float>(kSmagFactor), p.smag_c2)), strain), inv);
+        const float2 tau = v2(p.tau);
+        omega = p_rcp(p_mul(v2(0.5f), p_add(tau, p_sqrt(p_fma(tau, tau, k)))));
+    } else {
+        omega = v2(fast_rcp(p.tau));
+    }
+    const float2 base = p_fma(p_mul(v2(-1.5f), rho), uu, drho);
+    const float2 rho45 = p_mul(v2(4.5f), rho);
+    constexpr float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+    f[0] = p_fma(omega, p_fma(v2(w0), base, p_neg(f[0])), f[0]);
+    const float2 r3a = p_mul(v2(3.0f * w1), rho), r3b = p_mul(v2(3.0f * w2), rho);
+    relax_opposite2(f[1], f[2], ux, w1, r3a, base, rho45, omega);
+    relax_opposite2(f[3], f[4], uy, w1, r3a, base, rho45, omega);
+    relax_opposite2(f[5], f[6], uz, w1, r3a, base, rho45, omega);
+    relax_opposite2(f[7], f[8], p_add(ux, uy), w2, r3b, base, rho45, omega);
+    relax_opposite2(f[9], f[10], p_sub(ux, uy), w2, r3b, base, rho45, omega);
+    relax_opposite2(f[11], f[12], p_add(ux, uz), w2, r3b, base, rho45, omega);
+    relax_opposite2(f[13], f[14], p_sub(ux, uz), w2, r3b, base, rho45, omega);
+    relax_opposite2(f[15], f[16], p_add(uy, uz), w2, r3b, base, rho45, omega);
+    relax_opposite2(f[17], f[18], p_sub(uy, uz), w2, r3b, base, rho45, omega);
+    if (forced) {
+        const float2 scale = p_fma(v2(-0.5f), omega, v2(1.0f));
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            const float ex = static_cast<float>(d3::cx(i)), ey = static_cast<float>(d3::cy(i)),
+                        ez = static_cast<float>(d3::cz(i));
+            const float2 cu = p_fma(v2(ez), uz, p_fma(v2(ey), uy, p_mul(v2(ex), ux)));
+            const float cf = r_fma(ez, p.fz, r_fma(ey, p.fy, r_mul(ex, p.fx)));
+            const float2 uf = p_fma(p_sub(v2(ez), uz), v2(p.fz),
+                                    p_fma(p_sub(v2(ey), uy), v2(p.fy), p_mul(p_sub(v2(ex), ux), v2(p.fx))));
+            const float2 term = p_fma(v2(3.0f), uf, p_mul(p_mul(v2(9.0f), cu), v2(cf)));
+            f[i] = p_fma(p_mul(scale, v2(static_cast<float>(d3::w(i)))), term, f[i]);
+        }
+    }
+}
+
+// absorb3 for two nodes with their own layer rates (a node with rate 0 keeps
+// its values, as absorb3 is then not applied to it).
+__device__ __forceinline__ void absorb3_pair(float2 (&f)[d3::Q], float sa, float sb, const float* inlet) {
+    const float ux = inlet[0], uy = inlet[1], uz = inlet[2];
+    const float2 s = make_float2(sa, sb);
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const float cu = r_add(r_add(r_mul(float(d3::cx(i)), ux), r_mul(float(d3::cy(i)), uy)),
+                               r_mul(float(d3::cz(i)), uz));
+        const float uu = r_add(r_add(r_mul(ux, ux), r_mul(uy, uy)), r_mul(uz, uz));
+        const float quad = r_add(r_mul(3.0f, cu), r_mul(r_mul(4.5f, cu), cu));
+        const float target = r_mul(float(d3::w(i)), r_sub(quad, r_mul(1.5f, uu)));
+        const float2 r = p_sub(f[i], p_mul(s, p_sub(f[i], v2(target))));
+        f[i] = make_float2(sa > 0.0f ? r.x : f[i].x, sb > 0.0f ? r.y : f[i].y);
+    }
+}
+
 // Regularized Zou-He velocity inlet on the west face.
 // Shifted: lbm3_inlet_west (glsl:105-162).  Unshifted binary64:
 // velocity_inlet_west (lbm3d_internal.h:312-365), same operation order.
@@ -771,25 +890,17 @@ __device__ __forceinline__ void bulk_edges3(const Geom3D& g, const Phys3D<typena
 //               gather, whose side rules are uniform along the row;
 //   boundary    a node with a solid source (bounce-back / interpolated wall):
 //               the general gather with the plan's per-node direction mask.
-// The rest of a node's step on a flat lattice once its pulls are in f (for
-// an interior row; elsewhere f is filled here): class, edge and wall rules,
-// the inlet, the collision and the 19 stores.
-template <class S, bool kSmag>
-__device__ __forceinline__ void flat_finish3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
-                                             const S* __restrict__ src, S* __restrict__ dst,
-                                             const StepBuffers3D& b, typename Storage<S>::A (&f)[d3::Q],
-                                             uint8_t cls, bool interior, uint32_t x, uint32_t y, uint32_t z,
-                                             uint64_t here) {
+// The rules of a fluid node of a flat lattice once its plain pulls are in f
+// (for an interior row; elsewhere f is filled here): x-edge, wall and outlet
+// rules and the inlet, everything before the collision.
+template <class S>
+__device__ __forceinline__ void flat_fix3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                          const S* __restrict__ src, const StepBuffers3D& b,
+                                          typename Storage<S>::A (&f)[d3::Q], uint8_t cls, bool interior,
+                                          uint32_t x, uint32_t y, uint32_t z, uint64_t here) {
     using A = typename Storage<S>::A;
     using T = Storage<S>;
     const uint64_t cells = g.cells;
-    if (cls == kSolid) {
-#pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
-            T::store(dst + static_cast<uint64_t>(i) * cells + here, T::kShifted ? A(0) : A(d3::w(i)));
-        }
-        return;
-    }
     if (cls == kBulk) {
         bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
     } else if (interior && x != 0u && x + 1u != g.nx) {
@@ -812,6 +923,27 @@ __device__ __forceinline__ void flat_finish3(const Geom3D& g, const Phys3D<typen
     if (g.x_mode == ORR_X_INFLOW_OUTFLOW && x == 0u) {
         inlet_west3<A, T::kShifted>(f, static_cast<const A*>(b.inlet));
     }
+}
+
+// The rest of a node's step on a flat lattice once its pulls are in f (for
+// an interior row; elsewhere f is filled here): class, edge and wall rules,
+// the inlet, the collision and the 19 stores.
+template <class S, bool kSmag>
+__device__ __forceinline__ void flat_finish3(const Geom3D& g, const Phys3D<typename Storage<S>::A>& p,
+                                             const S* __restrict__ src, S* __restrict__ dst,
+                                             const StepBuffers3D& b, typename Storage<S>::A (&f)[d3::Q],
+                                             uint8_t cls, bool interior, uint32_t x, uint32_t y, uint32_t z,
+                                             uint64_t here) {
+    using A = typename Storage<S>::A;
+    using T = Storage<S>;
+    if (cls == kSolid) {
+#pragma unroll
+        for (int i = 0; i < d3::Q; ++i) {
+            T::store(dst + static_cast<uint64_t>(i) * g.cells + here, T::kShifted ? A(0) : A(d3::w(i)));
+        }
+        return;
+    }
+    flat_fix3<S>(g, p, src, b, f, cls, interior, x, y, z, here);
     finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
 }
 
@@ -895,6 +1027,109 @@ __global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g
         return;
     }
     step_node3<S, kSmag, kFlat>(g, p, src, dst, b, x, blockIdx.y, blockIdx.z);
+}
+
+// Row tiles of neighbouring node pairs, for the 2-byte storage forms of a
+// flat lattice with even nx: thread t of block (k, y, z) takes the nodes
+// x0 = 2 (k B + t) and x0 + 1 of row (y, z).  In an interior row each
+// direction is one aligned 32-bit load per lane: the two values of the pair
+// for c_x = 0; for c_x != 0 the pair's row word, whose missing half is the
+// neighbouring lane's word (a warp shuffle; the first and last lanes of the
+// warp load the word beyond the warp themselves).  A warp so moves 128 bytes
+// per load and per store instruction instead of 64.  Both nodes then take the
+// per-node rules (x edges, walls, inlet) on their own values and collide
+// together in packed binary32 lanes (collide3_pair).  Face rows go node by
+// node through step_node3.  Every value is rounded as in step3d_kernel: the
+// same bits.
+constexpr int kPairMinBlocks = 5;
+
+template <class S, bool kSmag>
+__global__ void __launch_bounds__(128, kPairMinBlocks) step3d_pair_kernel(Geom3D g, Phys3D<float> p,
+                                                                          const S* __restrict__ src,
+                                                                          S* __restrict__ dst, StepBuffers3D b) {
+    using T = Storage<S>;
+    static_assert(sizeof(S) == 2, "pairs of 2-byte values");
+    const uint32_t x0 = 2u * (blockIdx.x * blockDim.x + threadIdx.x);
+    const uint32_t y = blockIdx.y, z = blockIdx.z;
+    if (y - 1u >= g.ny - 2u || z - 1u >= g.nz - 2u) {
+        if (x0 < g.nx) {
+            step_node3<S, kSmag, true>(g, p, src, dst, b, x0, y, z);
+            step_node3<S, kSmag, true>(g, p, src, dst, b, x0 + 1u, y, z);
+        }
+        return;
+    }
+    // Interior row (uniform over the block): every lane loads and shuffles;
+    // lanes past the row end load the row's last pair.
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t xl = min(x0, g.nx - 2u);
+    const uint64_t here = xl + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
+    const int64_t nx = g.nx, plane = g.plane;
+    uint32_t word[d3::Q], edge[d3::Q];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        const int64_t row = static_cast<int64_t>(here) - (nx * d3::cy(i) + plane * d3::cz(i));
+        const auto* at = reinterpret_cast<const uint32_t*>(src + static_cast<uint64_t>(i) * g.cells +
+                                                           static_cast<uint64_t>(row));
+        word[i] = __ldg(at);
+        edge[i] = 0u;
+        if (d3::cx(i) > 0 && lane == 0u) {
+            edge[i] = __ldg(at - 1);
+        }
+        if (d3::cx(i) < 0 && lane == 31u) {
+            edge[i] = __ldg(at + 1);
+        }
+    }
+    const uint32_t cls2 = __ldg(reinterpret_cast<const uint16_t*>(b.cls + here));
+    float fa[d3::Q], fb[d3::Q];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        if (d3::cx(i) == 0) {
+            fa[i] = T::lo(word[i]);
+            fb[i] = T::hi(word[i]);
+        } else if (d3::cx(i) > 0) {
+            // sources x0 - 1 (the left lane's upper half) and x0
+            uint32_t left = __shfl_up_sync(0xffffffffu, word[i], 1);
+            left = lane == 0u ? edge[i] : left;
+            fa[i] = T::hi(left);
+            fb[i] = T::lo(word[i]);
+        } else {
+            // sources x0 + 1 and x0 + 2 (the right lane's lower half)
+            uint32_t right = __shfl_down_sync(0xffffffffu, word[i], 1);
+            right = lane == 31u ? edge[i] : right;
+            fa[i] = T::hi(word[i]);
+            fb[i] = T::lo(right);
+        }
+    }
+    if (x0 >= g.nx) {
+        return;
+    }
+    const uint8_t ca = static_cast<uint8_t>(cls2 & 0xffu), cb = static_cast<uint8_t>(cls2 >> 8);
+    if (ca != kSolid && (ca != kBulk || x0 == 0u)) {
+        flat_fix3<S>(g, p, src, b, fa, ca, true, x0, y, z, here);
+    }
+    if (cb != kSolid && (cb != kBulk || x0 + 2u == g.nx)) {
+        flat_fix3<S>(g, p, src, b, fb, cb, true, x0 + 1u, y, z, here + 1u);
+    }
+    float2 f[d3::Q];
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        f[i] = make_float2(fa[i], fb[i]);
+    }
+    collide3_pair<kSmag>(f, p, g.forced);
+    if (g.sponge) {
+        const float sa = sponge_rate3<float>(g, p, x0, y, z);
+        const float sb = sponge_rate3<float>(g, p, x0 + 1u, y, z);
+        if (sa > 0.0f || sb > 0.0f) {
+            absorb3_pair(f, sa, sb, static_cast<const float*>(b.inlet));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < d3::Q; ++i) {
+        // solid nodes store 0 (f - w of the rest state)
+        const float va = ca == kSolid ? 0.0f : f[i].x;
+        const float vb = cb == kSolid ? 0.0f : f[i].y;
+        *reinterpret_cast<uint32_t*>(dst + static_cast<uint64_t>(i) * g.cells + here) = T::pack(va, vb);
+    }
 }
 
 // ------------------------------------------------------------ init / misc --

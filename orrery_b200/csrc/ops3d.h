@@ -16,9 +16,10 @@ struct StepBuffers3D;
 struct Ops3D {
     // One fused step src -> dst (one launch).  `phys` points at a Phys3D of
     // the storage's arithmetic type; `block` is the block width (threads
-    // along x of a row, and list entries per block).
+    // along x of a row); npt 2 takes the pair step (two neighbouring nodes
+    // per thread) where pairs_ok allows it, the one-node step otherwise.
     cudaError_t (*step)(const Geom3D& g, const void* phys, const void* src, void* dst,
-                        const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s);
+                        const StepBuffers3D& b, bool smag, uint32_t block, uint32_t npt, cudaStream_t s);
     // Equilibrium initialisation of a population buffer; rho..uz may be
     // device arrays (all non-null) or null for the uniform state (r0, u0).
     cudaError_t (*init)(const Geom3D& g, const uint8_t* cls, const double* rho, const double* ux,
@@ -33,7 +34,11 @@ struct Ops3D {
     cudaError_t (*mass)(const Geom3D& g, const uint8_t* cls, const void* f, double* out,
                         cudaStream_t s);
     // Registers per thread of the step kernel (for the tuner and the docs).
-    int (*step_registers)(bool smag);
+    int (*step_registers)(bool smag, uint32_t npt);
+    // Whether the pair step serves lattice g with blocks of `block` threads
+    // (2-byte storage, periodic or free-slip sides and halfway walls, even nx,
+    // whole warps up to 128 threads).
+    bool (*pairs_ok)(const Geom3D& g, uint32_t block);
     // Persistent step over a device table of n Lattice3D entries of the
     // storage's arithmetic type (staged3d.cuh): `grid` CTAs of `block`
     // consumer threads (128 or 256) plus a producer warp, spans of

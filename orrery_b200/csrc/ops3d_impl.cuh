@@ -14,13 +14,25 @@ template <class S> struct Launch3D {
     using A = typename Storage<S>::A;
 
     static cudaError_t step(const Geom3D& g, const void* phys, const void* src, void* dst,
-                            const StepBuffers3D& b, bool smag, uint32_t block, cudaStream_t s) {
+                            const StepBuffers3D& b, bool smag, uint32_t block, uint32_t npt, cudaStream_t s) {
         Geom3D gg = g;
         gg.tiles_x = (g.nx + block - 1) / block;
-        const dim3 grid(gg.tiles_x, g.ny, g.nz);
         const auto& p = *static_cast<const Phys3D<A>*>(phys);
         const auto* in = static_cast<const S*>(src);
         auto* out = static_cast<S*>(dst);
+        if constexpr (sizeof(S) == 2) {
+            if (npt == 2 && pairs_ok(g, block)) {
+                gg.tiles_x = (g.nx + 2 * block - 1) / (2 * block);
+                const dim3 grid2(gg.tiles_x, g.ny, g.nz);
+                if (smag) {
+                    step3d_pair_kernel<S, true><<<grid2, block, 0, s>>>(gg, p, in, out, b);
+                } else {
+                    step3d_pair_kernel<S, false><<<grid2, block, 0, s>>>(gg, p, in, out, b);
+                }
+                return cudaGetLastError();
+            }
+        }
+        const dim3 grid(gg.tiles_x, g.ny, g.nz);
         if (smag) {
             if (g.flat) {
                 step3d_kernel<S, true, true><<<grid, block, 0, s>>>(gg, p, in, out, b);
@@ -85,10 +97,24 @@ template <class S> struct Launch3D {
         return cudaGetLastError();
     }
 
-    static int step_registers(bool smag) {
+    // The pair step serves 2-byte storage on flat lattices with even nx, in
+    // blocks of whole warps up to 128 threads.
+    static bool pairs_ok(const Geom3D& g, uint32_t block) {
+        return sizeof(S) == 2 && g.flat && g.nx % 2 == 0 && block % 32 == 0 && block <= 128;
+    }
+
+    static int step_registers(bool smag, uint32_t npt) {
         cudaFuncAttributes a{};
-        const cudaError_t e = smag ? cudaFuncGetAttributes(&a, step3d_kernel<S, true, true>)
-                                   : cudaFuncGetAttributes(&a, step3d_kernel<S, false, true>);
+        cudaError_t e = cudaErrorInvalidValue;
+        if constexpr (sizeof(S) == 2) {
+            if (npt == 2) {
+                e = smag ? cudaFuncGetAttributes(&a, step3d_pair_kernel<S, true>)
+                         : cudaFuncGetAttributes(&a, step3d_pair_kernel<S, false>);
+                return e == cudaSuccess ? a.numRegs : -1;
+            }
+        }
+        e = smag ? cudaFuncGetAttributes(&a, step3d_kernel<S, true, true>)
+                 : cudaFuncGetAttributes(&a, step3d_kernel<S, false, true>);
         return e == cudaSuccess ? a.numRegs : -1;
     }
 
@@ -208,8 +234,8 @@ template <class S> struct Launch3D {
 
     static const Ops3D& table() {
         static const Ops3D ops{&step,   &init,   &history,        &moments,          &force,
-                               &mass,   &step_registers, &staged, &staged_occupancy, &staged_smem,
-                               &staged_registers, &force_batch};
+                               &mass,   &step_registers, &pairs_ok, &staged, &staged_occupancy,
+                               &staged_smem, &staged_registers, &force_batch};
         return ops;
     }
 };

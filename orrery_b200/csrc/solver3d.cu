@@ -347,6 +347,15 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
                 h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
             }
         }
+        if (!h->persistent && o.nodes_per_thread == 2) {
+            // Row-tile step with two neighbouring nodes per thread.
+            if (!h->ops->pairs_ok(g, h->block)) {
+                throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: two nodes per thread of the row step need 2-byte "
+                                               "storage, periodic or free-slip sides, halfway walls, an even nx "
+                                               "and blocks of at most 128 threads"};
+            }
+            h->row_npt = 2;
+        }
         initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
         check(cudaStreamSynchronize(s), "create");
         // The per-node tables are on the device now; keep the links.
@@ -610,9 +619,10 @@ orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info)
         } else {
             k.kernel = ORR_KERNEL_ROWS;
             k.block = solver->block;
-            k.nodes_per_thread = 1;
-            k.grid = ((solver->g.nx + solver->block - 1) / solver->block) * solver->g.ny * solver->g.nz;
-            k.registers = solver->ops->step_registers(solver->smag);
+            const uint32_t span = solver->block * solver->row_npt;
+            k.nodes_per_thread = solver->row_npt;
+            k.grid = ((solver->g.nx + span - 1) / span) * solver->g.ny * solver->g.nz;
+            k.registers = solver->ops->step_registers(solver->smag, solver->row_npt);
         }
         *info = k;
         return ORR_OK;

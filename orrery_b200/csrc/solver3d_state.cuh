@@ -91,6 +91,7 @@ struct orr_lbm3d {
     bool allow_high_mach = false;
     int device = 0;
     uint32_t block = kDefaultBlock;
+    uint32_t row_npt = 1;  // nodes per thread of the row-tile step (2: the pair step)
     const Ops3D* ops = nullptr;
     Geom3D g{};
     Phys3D<float> phys32{};
@@ -203,7 +204,7 @@ struct orr_lbm3d {
                               shape.stages, smag, shape.block, shape.npt, shape.grid, status(), stream),
                   "step kernel");
         } else {
-            check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, stream),
+            check(ops->step(g, phys(), f[from], f[1 - from], buffers(), smag, block, row_npt, stream),
                   "step kernel");
         }
         ++launches;

@@ -45,6 +45,18 @@ template <> struct Storage<__half> {
     __device__ __forceinline__ static void store(__half* p, A v) {
         *p = __float2half_rn(v);
     }
+    // Two neighbouring values as one aligned 32-bit word (lower address in
+    // the low half).
+    __device__ __forceinline__ static A lo(uint32_t w) {
+        return __half2float(__ushort_as_half(static_cast<unsigned short>(w & 0xffffu)));
+    }
+    __device__ __forceinline__ static A hi(uint32_t w) {
+        return __half2float(__ushort_as_half(static_cast<unsigned short>(w >> 16)));
+    }
+    __device__ __forceinline__ static uint32_t pack(A a, A b) {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
     __device__ static __half encode(double shifted) {
         return __float2half_rn(static_cast<float>(shifted));
     }
@@ -62,6 +74,16 @@ template <> struct Storage<__nv_bfloat16> {
     __device__ __forceinline__ static A value(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, A v) {
         *p = __float2bfloat16_rn(v);
+    }
+    __device__ __forceinline__ static A lo(uint32_t w) {
+        return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w & 0xffffu)));
+    }
+    __device__ __forceinline__ static A hi(uint32_t w) {
+        return __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(w >> 16)));
+    }
+    __device__ __forceinline__ static uint32_t pack(A a, A b) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
     }
     __device__ static __nv_bfloat16 encode(double shifted) {
         return __float2bfloat16_rn(static_cast<float>(shifted));

@@ -59,6 +59,11 @@ def case(name):
         # nx = 40 is not a multiple of 16: every row takes the per-node path.
         cfg, mask = sphere_channel(40, 16, 16, 6.0, 2.5, 0.05, 30.0)
         return cfg, mask
+    if name == "odd_rows_convective":
+        # ny = 21: the last row of a two-row block stands alone; convective outlet.
+        cfg, mask = sphere_channel(48, 21, 17, 7.0, 3.0, 0.05, 40.0)
+        cfg.outlet = Outlet.convective
+        return cfg, mask
     raise KeyError(name)
 
 
@@ -108,6 +113,22 @@ def test_launch_shapes_agree(name, block, stages, npt):
     assert np.array_equal(ref.populations(), s.populations())
 
 
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("name", CASES + ["odd_rows_convective"])
+def test_pair_step_bitwise(name, storage):
+    """The pair step (two neighbouring nodes per thread, packed collision)
+    rounds every value as the one-node row step: equal populations bit for
+    bit, across tiles that end inside a row and warps past the row end."""
+    cfg, mask = case(name)
+    a = run(cfg, mask, storage, "rows")
+    for block in (128, 64, 32):
+        b = run(cfg, mask, storage, "rows", block=block, npt=2)
+        info = b.kernel_info()
+        assert (info["kernel"], info["nodes_per_thread"], info["block"]) == ("rows", 2, block)
+        fa, fb = a.populations(), b.populations()
+        assert np.array_equal(fa, fb), f"block {block}: {np.count_nonzero(fa != fb)} values differ"
+
+
 def test_skewed_inlet_bitwise():
     cfg, mask = case("sphere_les")
     cfg = copy_config(cfg)
@@ -133,6 +154,17 @@ def test_staged_refuses_general_boundaries():
         S.make_gpu_solver(cfg, mask, storage="f16", kernel="staged")
     # the automatic choice takes the row kernel for it
     assert S.make_gpu_solver(cfg, mask, storage="f16").kernel_info()["kernel"] == "rows"
+    # the pair step: 2-byte storage on flat lattices with even nx only
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, storage="f16", kernel="rows", nodes_per_thread=2)
+    cfg, mask = case("sphere_les")
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, storage="f32", kernel="rows", nodes_per_thread=2)
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, storage="f16", kernel="rows", nodes_per_thread=2, block_x=256)
+    cfg, mask = sphere_channel(45, 16, 16, 6.0, 2.5, 0.05, 30.0)
+    with pytest.raises(S.LbmError):
+        S.make_gpu_solver(cfg, mask, storage="f16", kernel="rows", nodes_per_thread=2)
 
 
 def test_refused_shapes():
