@@ -748,9 +748,13 @@ __device__ __forceinline__ void finish3(const Geom3D& g, const Phys3D<typename S
             absorb3<A, T::kShifted>(f, s, static_cast<const A*>(b.inlet));
         }
     }
+    // Population i of the node at (dst + i * cells) + here: the first sum is
+    // the same for every thread, the second one wide multiply-add of the
+    // 32-bit node index (lattices hold fewer than 2^32 / 19 nodes).
+    const uint32_t h = static_cast<uint32_t>(here);
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
-        T::store(dst + static_cast<uint64_t>(i) * g.cells + here, f[i]);
+        T::store(dst + static_cast<uint64_t>(i) * g.cells + h, f[i]);
     }
 }
 
@@ -952,11 +956,14 @@ template <class S>
 __device__ __forceinline__ void pull3(const Geom3D& g, const S* __restrict__ src, uint64_t here,
                                       typename Storage<S>::A (&f)[d3::Q]) {
     using T = Storage<S>;
-    const int64_t nx = g.nx, plane = g.plane;
+    const int64_t nx = g.nx, plane = g.plane, cells = static_cast<int64_t>(g.cells);
+    const uint32_t h = static_cast<uint32_t>(here);
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
-        const int64_t source = static_cast<int64_t>(here) - (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-        f[i] = T::load(src + static_cast<uint64_t>(i) * g.cells + static_cast<uint64_t>(source));
+        // (src + i * cells - c_i . (1, nx, plane)) is the same for every
+        // thread; the node index is added last as a 32-bit value.
+        const int64_t shift = i * cells - (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
+        f[i] = T::load(src + shift + h);
     }
 }
 
@@ -968,7 +975,7 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
     using A = typename Storage<S>::A;
     using T = Storage<S>;
     const uint64_t cells = g.cells;
-    const uint64_t here = x + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
+    const uint64_t here = x + g.nx * (y + g.ny * z);   // below 2^32 / 19
     A f[d3::Q];
     if constexpr (kFlat) {
         // Interior rows: every plain pull address lies inside the lattice, so
@@ -990,13 +997,7 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
             return;
         }
         if (cls == kBulk) {
-            const int64_t nx = g.nx, plane = g.plane;
-#pragma unroll
-            for (int i = 0; i < d3::Q; ++i) {
-                const int64_t source = static_cast<int64_t>(here) -
-                                       (d3::cx(i) + nx * d3::cy(i) + plane * d3::cz(i));
-                f[i] = T::load(src + static_cast<uint64_t>(i) * cells + static_cast<uint64_t>(source));
-            }
+            pull3<S>(g, src, here, f);
             bulk_edges3<S>(g, p, src, b, x, y, z, here, f);
         } else {
             const uint32_t mask = cls == kBoundary ? b.nmask[here] : 0u;
@@ -1062,14 +1063,14 @@ __global__ void __launch_bounds__(128, kPairMinBlocks) step3d_pair_kernel(Geom3D
     // lanes past the row end load the row's last pair.
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t xl = min(x0, g.nx - 2u);
-    const uint64_t here = xl + static_cast<uint64_t>(g.nx) * (y + static_cast<uint64_t>(g.ny) * z);
-    const int64_t nx = g.nx, plane = g.plane;
+    const uint32_t h = xl + g.nx * (y + g.ny * z);
+    const uint64_t here = h;
+    const int64_t nx = g.nx, plane = g.plane, cells = static_cast<int64_t>(g.cells);
     uint32_t word[d3::Q], edge[d3::Q];
 #pragma unroll
     for (int i = 0; i < d3::Q; ++i) {
-        const int64_t row = static_cast<int64_t>(here) - (nx * d3::cy(i) + plane * d3::cz(i));
-        const auto* at = reinterpret_cast<const uint32_t*>(src + static_cast<uint64_t>(i) * g.cells +
-                                                           static_cast<uint64_t>(row));
+        const int64_t shift = i * cells - (nx * d3::cy(i) + plane * d3::cz(i));
+        const auto* at = reinterpret_cast<const uint32_t*>(src + shift + h);
         word[i] = __ldg(at);
         edge[i] = 0u;
         if (d3::cx(i) > 0 && lane == 0u) {
@@ -1128,7 +1129,7 @@ __global__ void __launch_bounds__(128, kPairMinBlocks) step3d_pair_kernel(Geom3D
         // solid nodes store 0 (f - w of the rest state)
         const float va = ca == kSolid ? 0.0f : f[i].x;
         const float vb = cb == kSolid ? 0.0f : f[i].y;
-        *reinterpret_cast<uint32_t*>(dst + static_cast<uint64_t>(i) * g.cells + here) = T::pack(va, vb);
+        *reinterpret_cast<uint32_t*>(dst + static_cast<uint64_t>(i) * g.cells + h) = T::pack(va, vb);
     }
 }
 
