@@ -155,6 +155,32 @@ def run_reference_arm(args, rank: int):
     return 0
 
 
+def voxelize_cpu_baseline(forms, arrays, planes: int = 48) -> dict:
+    """The reference's own geom::voxelize + geom::signed_distance_band
+    (oracle/_ref, single-threaded as in the reference) on `planes` z-planes
+    through the middle of the voxelize workload's grid, and whether its output
+    equals the device's on those planes."""
+    import numpy as np
+    from oracle import oracle as O
+    if not O.reference_available():
+        return {}
+    mesh, spec = forms.voxelize_workload()
+    k0 = spec.nz // 2 - planes // 2
+    origin = (spec.origin[0], spec.origin[1], spec.origin[2] + k0 * spec.spacing)
+    n = (spec.nx, spec.ny, planes)
+    t0 = time.perf_counter()
+    solid, _ = O.reference_voxelize(mesh.vertices, mesh.triangles, origin, spec.spacing, n)
+    dist, inb, _ = O.reference_signed_distance_band(mesh.vertices, mesh.triangles, origin, spec.spacing, n, solid)
+    seconds = time.perf_counter() - t0
+    lo, hi = k0 * spec.nx * spec.ny, (k0 + planes) * spec.nx * spec.ny
+    return {"cpu_baseline": {"value": spec.nx * spec.ny * planes / seconds / 1e6, "unit": "Mcells/s", "cores": 1,
+                             "kind": "reference", "seconds": seconds,
+                             "sample": f"{planes} z-planes of {spec.nx} x {spec.ny} cells through the body's middle"},
+            "cpu_slab_matches_device": bool(np.array_equal(solid, arrays["solid"][lo:hi]) and
+                                            np.array_equal(dist, arrays["distance"][lo:hi]) and
+                                            np.array_equal(inb, arrays["in_band"][lo:hi]))}
+
+
 def run_form(args, rank: int) -> int:
     """The batched and served forms (one GPU; other ranks idle)."""
     if rank != 0:
@@ -164,6 +190,21 @@ def run_form(args, rank: int) -> int:
     from orrery_b200 import forms
     clocks = ClockSampler(0)
     clocks.start()
+    if args.form == "voxelize":
+        r = forms.run_voxelize()
+        arrays = r.pop("arrays")
+        if not args.no_cpu_baseline:
+            r.update(voxelize_cpu_baseline(forms, arrays))
+        metric, value, unit = "voxelize + distance band Mcells/s", r["device_mcells_per_s"], "Mcells/s"
+        clock_info = clocks.stop()
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "form": args.form,
+                "config": {"workload": "sphere-cone body, 49 K triangles, 320 x 160 x 160 cells"},
+                "e2e": {"value": r["e2e_mcells_per_s"], "unit": "Mcells/s", "h2d_bytes_per_step": r["h2d_bytes"],
+                        "d2h_bytes_per_step": r["d2h_bytes"]},
+                "cpu_baseline": r.get("cpu_baseline"), "result": r, "clocks": clock_info}
+        print(json.dumps(line), flush=True)
+        return 0
     if args.form == "batched":
         steps = args.steps if args.steps != 1000 else 3000
         r = forms.run_batched(storage=args.storage, count=args.lattices, steps=steps, plain=not args.no_plain,
@@ -196,7 +237,7 @@ def main(argv=None) -> int:
     ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
     ap.add_argument("--stages", type=int, default=0)
     ap.add_argument("--npt", type=int, default=0, help="nodes per thread of a staged span, or of the row kernel (2: the pair step)")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve"])
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve", "voxelize"])
     ap.add_argument("--lattices", type=int, default=64, help="batched form: lattices")
     ap.add_argument("--requests", type=int, default=48, help="serve form: requests")
     ap.add_argument("--max-steps", type=int, default=20000, help="serve form: step cap per solve")

@@ -460,6 +460,46 @@ ORR_API orr_status orr_lbm2d_links(const orr_lbm2d* solver, uint32_t* cell, uint
 ORR_API orr_status orr_lbm2d_stream(const orr_lbm2d* solver, void** stream);
 ORR_API orr_status orr_lbm2d_launch_count(const orr_lbm2d* solver, uint64_t* launches);
 
+/* ---- mesh voxelization (solid masks and wall distances) ------------------
+ *
+ * The adapter builds every lattice's solid mask and wall distances from the
+ * body's triangle mesh (lbm_aero_solver3d.cpp:249-258) with geom::voxelize and
+ * geom::signed_distance_band (src/geom/include/orrery/geom/voxel_grid.h:35-69).
+ * These entry points compute the same arrays on the device; inputs and
+ * outputs are host arrays.  Cell (i, j, k) has its centre at
+ * origin + spacing (i + 1/2, j + 1/2, k + 1/2) and index i + nx (j + ny k). */
+typedef struct orr_grid_spec {     /* geom::GridSpec (voxel_grid.h:14-27) */
+    double origin[3];
+    double spacing;
+    uint64_t nx, ny, nz;
+} orr_grid_spec;
+
+typedef struct orr_mesh {           /* geom::TriangleMesh (triangle_mesh.h:15-19) */
+    const double* vertices;         /* 3 per vertex */
+    uint64_t vertex_count;
+    const uint32_t* triangles;      /* 3 corner indices per triangle, counter-clockwise seen from outside */
+    uint64_t triangle_count;
+} orr_mesh;
+
+/* geom::grid_around (voxel_grid.h:31-33): the grid covering the box with
+ * `padding` extra cells on every side, centred on it. */
+ORR_API orr_status orr_grid_around(const double box_min[3], const double box_max[3], double spacing,
+                                   uint64_t padding, orr_grid_spec* out);
+/* geom::voxelize (voxel_grid.h:47-52): solid[c] = winding number at the cell
+ * centre >= threshold (0.5 in the reference); `winding` (nx*ny*nz doubles) may
+ * be NULL.  Refusals carry the reference's texts.  *device_ms (may be NULL)
+ * receives the kernel time. */
+ORR_API orr_status orr_voxelize(const orr_mesh* mesh, const orr_grid_spec* spec, double threshold,
+                                int32_t device, uint8_t* solid, double* winding, double* device_ms);
+/* geom::signed_distance_band (voxel_grid.h:54-69) for the solid flags of
+ * orr_voxelize: distance to the closest triangle within band_cells * spacing
+ * (negative in solid cells, +-band outside the band), in_band flags, and the
+ * band width in *band (may be NULL). */
+ORR_API orr_status orr_signed_distance_band(const orr_mesh* mesh, const orr_grid_spec* spec,
+                                            const uint8_t* solid, uint64_t solid_count, double band_cells,
+                                            int32_t device, double* distance, uint8_t* in_band, double* band,
+                                            double* device_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -442,3 +442,107 @@ def set_threads(n: int) -> None:
     restated_lib().lo_set_threads(int(n))
     if reference_available():
         reference_lib().ref_set_threads(int(n))
+
+
+# ---- mesh voxelization (reference geom::voxelize, geom::signed_distance_band) ----
+
+def _geom_lib():
+    lib = reference_lib()
+    if not getattr(lib, "_geom_declared", False):
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        cp, sz = ctypes.c_char_p, ctypes.c_size_t
+        lib.ref_mesh_sphere.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_double, u64p, u64p, cp, sz]
+        lib.ref_mesh_ellipsoid.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_double, u64p, u64p, cp, sz]
+        lib.ref_mesh_cone.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, u64p, u64p, cp, sz]
+        lib.ref_mesh_box.argtypes = [ctypes.c_double] * 3 + [u64p, u64p, cp, sz]
+        lib.ref_mesh_naca_wing.argtypes = [cp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                           u64p, u64p, cp, sz]
+        lib.ref_mesh_copy.argtypes = [_dp, _u32p]
+        lib.ref_grid_around.argtypes = [_dp, _dp, ctypes.c_double, ctypes.c_uint64, _dp, u64p, cp, sz]
+        lib.ref_voxelize.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_double,
+                                     ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_double, _u8p, _dp,
+                                     cp, sz]
+        lib.ref_signed_distance_band.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp,
+                                                 ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_uint64, _u8p, ctypes.c_uint64, ctypes.c_double, _dp,
+                                                 _u8p, _dp, cp, sz]
+        lib.ref_winding_direct.restype = ctypes.c_double
+        lib.ref_winding_direct.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp]
+        lib.ref_solid_angle.restype = ctypes.c_double
+        lib.ref_solid_angle.argtypes = [_dp, _dp, _dp, _dp]
+        lib.ref_closest_point.argtypes = [_dp, _dp, _dp, _dp, _dp]
+        lib.ref_hypot3.restype = ctypes.c_double
+        lib.ref_hypot3.argtypes = [ctypes.c_double] * 3
+        lib._geom_declared = True
+    return lib
+
+
+class ReferenceError_(RuntimeError):
+    """A std::invalid_argument (or other exception) of the reference."""
+
+
+def reference_mesh(kind: str, *args):
+    """Vertices (n, 3) and triangles (m, 3) of a reference mesh builder:
+    'sphere' (radius, around, arc_step), 'ellipsoid' (a, b, c, around,
+    arc_step), 'cone' (radius, height, around), 'box' (lx, ly, lz),
+    'naca_wing' (digits, chord, span, n, span_divisions)."""
+    lib = _geom_lib()
+    nv, nt = ctypes.c_uint64(), ctypes.c_uint64()
+    msg = ctypes.create_string_buffer(1024)
+    fn = getattr(lib, "ref_mesh_" + kind)
+    if kind == "naca_wing":
+        args = (args[0].encode(),) + tuple(args[1:])
+    rc = fn(*args, ctypes.byref(nv), ctypes.byref(nt), msg, 1024)
+    if rc != 0:
+        raise ReferenceError_(msg.value.decode())
+    v = np.empty((nv.value, 3), np.float64)
+    t = np.empty((nt.value, 3), np.uint32)
+    lib.ref_mesh_copy(_ptr(v, _dp), _ptr(t, _u32p))
+    return v, t
+
+
+def reference_grid_around(lo, hi, spacing, padding):
+    lib = _geom_lib()
+    lo = np.ascontiguousarray(lo, np.float64)
+    hi = np.ascontiguousarray(hi, np.float64)
+    origin = np.empty(3, np.float64)
+    n = np.empty(3, np.uint64)
+    msg = ctypes.create_string_buffer(1024)
+    if lib.ref_grid_around(_ptr(lo, _dp), _ptr(hi, _dp), float(spacing), int(padding), _ptr(origin, _dp),
+                           n.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), msg, 1024) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return origin, [int(x) for x in n]
+
+
+def reference_voxelize(vertices, triangles, origin, spacing, n, threshold=0.5):
+    lib = _geom_lib()
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    o = np.ascontiguousarray(origin, np.float64)
+    cells = int(n[0]) * int(n[1]) * int(n[2])
+    cells = cells if 0 < cells <= (1 << 27) else 1   # refused grids are not written
+    solid = np.zeros(cells, np.uint8)
+    wind = np.zeros(cells, np.float64)
+    msg = ctypes.create_string_buffer(1024)
+    if lib.ref_voxelize(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(o, _dp), float(spacing), int(n[0]),
+                        int(n[1]), int(n[2]), float(threshold), _ptr(solid, _u8p), _ptr(wind, _dp), msg, 1024) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return solid, wind
+
+
+def reference_signed_distance_band(vertices, triangles, origin, spacing, n, solid, band_cells=3.0):
+    lib = _geom_lib()
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    o = np.ascontiguousarray(origin, np.float64)
+    s = np.ascontiguousarray(solid, np.uint8)
+    cells = max(len(s), 1)
+    dist = np.zeros(cells, np.float64)
+    inb = np.zeros(cells, np.uint8)
+    band = ctypes.c_double()
+    msg = ctypes.create_string_buffer(1024)
+    if lib.ref_signed_distance_band(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(o, _dp), float(spacing),
+                                    int(n[0]), int(n[1]), int(n[2]), _ptr(s, _u8p), len(s), float(band_cells),
+                                    _ptr(dist, _dp), _ptr(inb, _u8p), ctypes.byref(band), msg, 1024) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return dist[:len(s)], inb[:len(s)], band.value

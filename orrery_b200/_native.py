@@ -91,6 +91,11 @@ SIGNATURES = {
     "orr_serve_wait": (_st, [_vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(abi.CSolveResult)]),
     "orr_serve_drain": (_st, [_vp, ctypes.c_double]),
     "orr_serve_stats": (_st, [_vp, ctypes.POINTER(abi.CServeStatistics)]),
+    "orr_grid_around": (_st, [_dp, _dp, ctypes.c_double, ctypes.c_uint64, ctypes.POINTER(abi.CGridSpec)]),
+    "orr_voxelize": (_st, [ctypes.POINTER(abi.CMesh), ctypes.POINTER(abi.CGridSpec), ctypes.c_double, ctypes.c_int32,
+                           _u8p, _dp, _dp]),
+    "orr_signed_distance_band": (_st, [ctypes.POINTER(abi.CMesh), ctypes.POINTER(abi.CGridSpec), _u8p,
+                                       ctypes.c_uint64, ctypes.c_double, ctypes.c_int32, _dp, _u8p, _dp, _dp]),
 }
 
 

@@ -141,3 +141,15 @@ class CServeStatistics(ctypes.Structure):
                 ("busy_seconds", ctypes.c_double), ("peak_device_bytes", ctypes.c_uint64),
                 ("mean_active", ctypes.c_double), ("chunks", ctypes.c_uint64), ("worker_failed", ctypes.c_int32),
                 ("message", ctypes.c_char * 160)]
+
+
+class CGridSpec(ctypes.Structure):
+    """orr_grid_spec (geom::GridSpec)."""
+    _fields_ = [("origin", ctypes.c_double * 3), ("spacing", ctypes.c_double), ("nx", ctypes.c_uint64),
+                ("ny", ctypes.c_uint64), ("nz", ctypes.c_uint64)]
+
+
+class CMesh(ctypes.Structure):
+    """orr_mesh (geom::TriangleMesh as flat arrays)."""
+    _fields_ = [("vertices", ctypes.POINTER(ctypes.c_double)), ("vertex_count", ctypes.c_uint64),
+                ("triangles", ctypes.POINTER(ctypes.c_uint32)), ("triangle_count", ctypes.c_uint64)]

@@ -40,6 +40,7 @@ SOURCES = {
     "force_static.cu": [],
     "batch3d.cu": [],
     "serve3d.cu": [],
+    "voxel.cu": ["-fmad=false"],
 }
 
 

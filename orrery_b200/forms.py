@@ -7,6 +7,9 @@ batched   the 64 NACA-wing lattices of ``workloads.naca_batch`` advanced as
           solve = one lattice for the full step count), next to the plain
           form: the same lattices solved one after another by single binary32
           solvers with the same sampling.
+voxelize  the solid mask and wall distances of the largest served body (a
+          sphere-cone of 49 K triangles in a 320 x 160 x 160 grid) by
+          geometry.voxelize + signed_distance_band on the device.
 serve     the sphere-cone request stream of ``workloads.sphere_cone_requests``
           submitted at its (seeded Poisson) arrival times to a ``serve.Server``;
           every solve runs until its window-mean Cd settles or its step cap.
@@ -180,3 +183,46 @@ def run_serve(storage: str = "f16", count: int = 48, rate: float = 20.0, seed: i
         out["cd_rel_error_vs_f64"] = {"max": max(errs), "mean": float(np.mean(errs)), "n": n,
                                       "per_request": errs, "steps": caps, "steps_f64": ref["steps"]}
     return out
+
+
+def voxelize_workload():
+    """The largest served body: a sphere-cone (base radius ny / 8, half-angle
+    25 degrees, nose radius 0.3 of the base radius; 256 vertices per ring,
+    49,152 triangles) at x = nx / 4 of a 320 x 160 x 160 grid of unit cells."""
+    from . import geometry as G
+
+    nx, ny, nz = 320, 160, 160
+    base = ny / 8.0
+    mesh = G.sphere_cone_mesh(base, math.radians(25.0), 0.3 * base, around=256, nose_steps=48, cone_steps=48)
+    mesh = G.TriangleMesh(mesh.vertices + np.array([nx / 4.0, ny / 2.0, nz / 2.0]), mesh.triangles)
+    return mesh, G.GridSpec((0.0, 0.0, 0.0), 1.0, nx, ny, nz)
+
+
+def run_voxelize(repeats: int = 5) -> dict:
+    """Device voxelization of `voxelize_workload`: cells per second for the
+    two kernels (device time by CUDA events inside the library) and end to
+    end through the C ABI (host mesh in, host flags and distances out: tree
+    build, uploads, kernels, read-backs).  The last results are returned
+    under "arrays" for a caller's checks."""
+    from . import geometry as G
+
+    mesh, spec = voxelize_workload()
+    cells = spec.cells()
+    vox = G.voxelize(mesh, spec)          # first call: module load and warm-up
+    G.signed_distance_band(mesh, vox)
+    dev, wall = [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        vox = G.voxelize(mesh, spec, winding=False)
+        sdf = G.signed_distance_band(mesh, vox)
+        wall.append(time.perf_counter() - t0)
+        dev.append((vox.device_ms + sdf.device_ms) * 1e-3)
+    return {"form": "voxelize", "grid": [spec.nx, spec.ny, spec.nz], "cells": cells,
+            "triangles": int(len(mesh.triangles)), "solid_cells": vox.solid_count(),
+            "band_cells": int(np.count_nonzero(sdf.in_band)), "device_s": min(dev),
+            "voxelize_ms": vox.device_ms, "distance_ms": sdf.device_ms,
+            "device_mcells_per_s": cells / min(dev) / 1e6, "e2e_s": min(wall),
+            "e2e_mcells_per_s": cells / min(wall) / 1e6,
+            "h2d_bytes": int(mesh.vertices.nbytes + mesh.triangles.nbytes) * 2 + cells,
+            "d2h_bytes": cells * (1 + 8 + 1),
+            "arrays": {"solid": vox.solid, "distance": sdf.distance, "in_band": sdf.in_band}}
