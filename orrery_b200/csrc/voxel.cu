@@ -9,9 +9,10 @@
 // Layout: the tree is built on the host (it is small: about n / 4 nodes for n
 // triangles) and copied with the triangles' corners in tree order, 9 doubles
 // per triangle, so a leaf's triangles are one contiguous run.  One thread per
-// grid cell walks the tree with a stack of at most 64 entries in local memory;
-// the 32 threads of a warp are 32 neighbouring cells of a grid row and mostly
-// take the same path.
+// grid cell.  For the winding number the 32 cells of a warp (a 4 x 4 x 2
+// brick) walk the tree together on one stack in shared memory; for the
+// distance each thread walks on its own with a stack of at most 64 entries in
+// local memory (its nearest-first order is its own).
 //
 // Results: the tree has the reference's node ranges, triangle order and node
 // quantities (same median split with the same tie-break, same sums in the same
@@ -338,59 +339,114 @@ __device__ inline double box_distance2(const Node& n, V3 p) {
     return dx * dx + dy * dy + dz * dz;
 }
 
+// Cells of a warp: a brick of 4 x 4 x 2 neighbouring cells (lane l at
+// (l % 4, l / 4 % 4, l / 16) of its brick), whose tree walks differ little.
+constexpr uint32_t kBrickX = 4, kBrickY = 4, kBrickZ = 2;
+constexpr int kWarpsPerBlock = 4;
+
+struct Bricks {
+    uint32_t bx, by, bz;
+};
+
+__host__ __device__ inline Bricks bricks_of(const Grid& g) {
+    return {(g.nx + kBrickX - 1) / kBrickX, (g.ny + kBrickY - 1) / kBrickY, (g.nz + kBrickZ - 1) / kBrickZ};
+}
+
 // Generalized winding number of every cell centre (hierarchical evaluation
 // of Barill et al. 2018; MeshTree::winding_number, winding_number.cpp:242-279):
 // a node far enough away (distance above beta times its radius) counts as its
-// dipole, a near leaf as the exact solid angles of its triangles.  Children
-// are pushed left then right, so the sum runs in the reference's order.
+// dipole, a near leaf as the exact solid angles of its triangles.
+//
+// The 32 lanes of a warp walk the tree together: one stack per warp in
+// shared memory holds (node, lanes that reach it).  Each lane of the popped
+// entry either adds the node's dipole or opens it; the lanes that open a
+// leaf add its solid angles together, those that open an inner node push its
+// children (left, then right) with their mask.  The walk is the union of the
+// lanes' own depth-first walks in the same order, so every lane adds the same
+// terms in the same order as a walk of its own (the reference's order), with
+// one instruction stream per warp instead of 32 diverging ones.
 __global__ void __launch_bounds__(128) winding_kernel(Grid g, const Node* __restrict__ nodes,
                                                       const double* __restrict__ corners, uint32_t node_count,
                                                       double scale, double threshold, uint8_t* __restrict__ solid,
                                                       double* __restrict__ winding, uint32_t* __restrict__ overflow) {
-    const uint32_t cells = g.nx * g.ny * g.nz;
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cells) {
+    __shared__ uint2 stacks[kWarpsPerBlock][kStack];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint2* stack = stacks[warp];
+    const Bricks nb = bricks_of(g);
+    const uint64_t brick = static_cast<uint64_t>(blockIdx.x) * kWarpsPerBlock + warp;
+    const uint32_t bi = static_cast<uint32_t>(brick % nb.bx), bj = static_cast<uint32_t>((brick / nb.bx) % nb.by);
+    const uint64_t bk = brick / (static_cast<uint64_t>(nb.bx) * nb.by);
+    const uint32_t i = bi * kBrickX + lane % kBrickX, j = bj * kBrickY + (lane / kBrickX) % kBrickY;
+    const uint64_t k = bk * kBrickZ + lane / (kBrickX * kBrickY);
+    const bool valid = i < g.nx && j < g.ny && k < g.nz;
+    const uint32_t lanes = __ballot_sync(0xffffffffu, valid);
+    if (lanes == 0u) {
         return;
     }
+    const uint32_t c = valid ? i + g.nx * (j + g.ny * static_cast<uint32_t>(k)) : 0u;
     const V3 p = cell_centre(g, c);
     double sum = 0.0;
-    uint32_t stack[kStack];
     int top = 0;
     if (node_count > 0) {
-        stack[top++] = 0;
+        if (lane == 0) {
+            stack[0] = make_uint2(0u, lanes);
+        }
+        top = 1;
     }
+    __syncwarp();
     while (top > 0) {
-        const Node& n = nodes[stack[--top]];
-        const V3 d = V3{__ldg(&n.centre[0]), __ldg(&n.centre[1]), __ldg(&n.centre[2])} - p;
-        const double dist = length3(d);
-        if (dist > kBeta * __ldg(&n.radius)) {
-            const double flux = dot(V3{__ldg(&n.area[0]), __ldg(&n.area[1]), __ldg(&n.area[2])}, d / dist);
-            if (flux != 0.0) {
-                const double ratio = scale / dist;
-                sum += flux * ratio * ratio;
+        --top;
+        const uint2 e = stack[top];
+        __syncwarp();
+        const Node& n = nodes[e.x];
+        bool open = false;
+        if ((e.y >> lane) & 1u) {
+            const V3 d = V3{__ldg(&n.centre[0]), __ldg(&n.centre[1]), __ldg(&n.centre[2])} - p;
+            const double dist = length3(d);
+            if (dist > kBeta * __ldg(&n.radius)) {
+                const double flux = dot(V3{__ldg(&n.area[0]), __ldg(&n.area[1]), __ldg(&n.area[2])}, d / dist);
+                if (flux != 0.0) {
+                    const double ratio = scale / dist;
+                    sum += flux * ratio * ratio;
+                }
+            } else {
+                open = true;
             }
+        }
+        const uint32_t opened = __ballot_sync(0xffffffffu, open);
+        if (opened == 0u) {
             continue;
         }
-        const uint32_t first = __ldg(&n.first), count = __ldg(&n.count);
         if (__ldg(&n.leaf)) {
-            for (uint32_t i = first; i < first + count; ++i) {
-                const double* t = corners + 9 * static_cast<size_t>(i);
-                sum += solid_angle(p, load3(t), load3(t + 3), load3(t + 6));
+            if (open) {
+                const uint32_t first = __ldg(&n.first), count = __ldg(&n.count);
+                for (uint32_t t = first; t < first + count; ++t) {
+                    const double* tri = corners + 9 * static_cast<size_t>(t);
+                    sum += solid_angle(p, load3(tri), load3(tri + 3), load3(tri + 6));
+                }
             }
             continue;
         }
         if (top + 2 > kStack) {
-            atomicOr(overflow, 1u);
+            if (lane == 0) {
+                atomicOr(overflow, 1u);
+            }
             break;
         }
-        stack[top++] = __ldg(&n.left);
-        stack[top++] = __ldg(&n.right);
+        if (lane == 0) {
+            stack[top] = make_uint2(__ldg(&n.left), opened);
+            stack[top + 1] = make_uint2(__ldg(&n.right), opened);
+        }
+        top += 2;
+        __syncwarp();
     }
-    const double w = sum / (4.0 * std::numbers::pi);
-    if (winding != nullptr) {
-        winding[c] = w;
+    if (valid) {
+        const double w = sum / (4.0 * std::numbers::pi);
+        if (winding != nullptr) {
+            winding[c] = w;
+        }
+        solid[c] = static_cast<uint8_t>(w >= threshold);
     }
-    solid[c] = static_cast<uint8_t>(w >= threshold);
 }
 
 // Distance from every cell centre to the surface, up to `band`, signed by the
@@ -618,9 +674,11 @@ orr_status orr_voxelize(const orr_mesh* mesh, const orr_grid_spec* spec, double 
                 cudaFree(b);
             }
         } release{dsolid, dwinding};
-        const unsigned blocks = static_cast<unsigned>((cells + 127) / 128);
+        const Bricks nb = bricks_of(grid_of(*spec));
+        const uint64_t bricks = static_cast<uint64_t>(nb.bx) * nb.by * nb.bz;
+        const unsigned blocks = static_cast<unsigned>((bricks + kWarpsPerBlock - 1) / kWarpsPerBlock);
         check(cudaEventRecord(call.t0, call.stream), "event");
-        winding_kernel<<<blocks, 128, 0, call.stream>>>(grid_of(*spec), d.nodes, d.corners, d.node_count,
+        winding_kernel<<<blocks, 32 * kWarpsPerBlock, 0, call.stream>>>(grid_of(*spec), d.nodes, d.corners, d.node_count,
                                                         tree.scale, threshold, dsolid, dwinding, d.overflow);
         check(cudaGetLastError(), "winding kernel");
         check(cudaEventRecord(call.t1, call.stream), "event");
