@@ -35,12 +35,14 @@ _reference = None
 
 
 def build(reference: str | None = None) -> None:
-    """Builds the restatement, and the reference library when the reference tree exists."""
+    """Builds the restatement, and the reference libraries when the reference
+    tree exists (the adapter harness after the product library)."""
     env = dict(os.environ)
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True, env=env)
     ref = reference or os.environ.get("ORR_REFERENCE", "/root/reference")
     if os.path.isdir(os.path.join(ref, "src", "aero", "lbm3d")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True, env=env)
+        subprocess.run(["make", "-s", "-C", HERE, "adapter", f"REF={ref}"], check=True, env=env)
 
 
 def _ptr(a, t):
@@ -546,3 +548,49 @@ def reference_signed_distance_band(vertices, triangles, origin, spacing, n, soli
                                     _ptr(dist, _dp), _ptr(inb, _u8p), ctypes.byref(band), msg, 1024) != 0:
         raise ReferenceError_(msg.value.decode())
     return dist[:len(s)], inb[:len(s)], band.value
+
+
+# ---- the reference's 3D adapter (LbmAeroSolver3D), CPU solver or CUDA solver ----
+
+ADAPTER_SO = os.path.join(os.path.dirname(REFERENCE_SO), "libref_adapter.so")
+_adapter = None
+
+ADAPTER_DEFAULTS = {
+    "length": 1.0, "area": 1.0, "speed": 1.0, "density": 1.225, "viscosity": 1.789e-5,
+    "angle_of_attack": 0.0, "sideslip": 0.0, "cells_per_length": 16.0, "lattice_velocity": 0.05,
+    "upstream": 5.0, "downstream": 10.0, "width": 6.0, "duration": 30.0, "average_window": 8.0,
+    "steps_per_call": 200, "wall": 1, "sponge_strength": 0.1, "start_ramp": 3.0, "les": 0, "sample_every": 10,
+}
+_ADAPTER_ORDER = ["length", "area", "speed", "density", "viscosity", "angle_of_attack", "sideslip",
+                  "cells_per_length", "lattice_velocity", "upstream", "downstream", "width", "duration",
+                  "average_window", "steps_per_call", "wall", "sponge_strength", "start_ramp", "les", "sample_every"]
+_ADAPTER_OUT = ["cd", "cl", "cy", "cm", "fx", "fy", "fz", "mx", "my", "mz", "iterations", "converged", "seconds",
+                "nx", "ny", "nz", "lattice_steps"]
+
+
+def adapter_available() -> bool:
+    return os.path.exists(ADAPTER_SO)
+
+
+def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: int = 0, **params) -> dict:
+    """One LbmAeroSolver3D solve (setup, then step() until done) of the
+    reference's own adapter; backend 'cpu' is its CPU solver, 'cuda' the CUDA
+    solver through the Lbm3DSolver seam (ORR_STORAGE_* `storage`)."""
+    global _adapter
+    if _adapter is None:
+        lib = ctypes.CDLL(ADAPTER_SO)
+        lib.ref_adapter_run.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_int,
+                                        ctypes.c_int, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        _adapter = lib
+    p = dict(ADAPTER_DEFAULTS)
+    p.update(params)
+    arr = np.array([float(p[k]) for k in _ADAPTER_ORDER])
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    out = np.zeros(len(_ADAPTER_OUT))
+    msg = ctypes.create_string_buffer(2048)
+    rc = _adapter.ref_adapter_run(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(arr, _dp),
+                                  1 if backend == "cuda" else 0, int(storage), _ptr(out, _dp), msg, 2048)
+    if rc != 0:
+        raise ReferenceError_(msg.value.decode())
+    return dict(zip(_ADAPTER_OUT, out.tolist()))
