@@ -553,7 +553,8 @@ def reference_signed_distance_band(vertices, triangles, origin, spacing, n, soli
 # ---- the reference's 3D adapter (LbmAeroSolver3D), CPU solver or CUDA solver ----
 
 ADAPTER_SO = os.path.join(os.path.dirname(REFERENCE_SO), "libref_adapter.so")
-_adapter = None
+ADAPTER_VOXEL_SO = os.path.join(os.path.dirname(REFERENCE_SO), "libref_adapter_voxel.so")
+_adapter = {}
 
 ADAPTER_DEFAULTS = {
     "length": 1.0, "area": 1.0, "speed": 1.0, "density": 1.225, "viscosity": 1.789e-5,
@@ -569,19 +570,23 @@ _ADAPTER_OUT = ["cd", "cl", "cy", "cm", "fx", "fy", "fz", "mx", "my", "mz", "ite
 
 
 def adapter_available() -> bool:
-    return os.path.exists(ADAPTER_SO)
+    return os.path.exists(ADAPTER_SO) and os.path.exists(ADAPTER_VOXEL_SO)
 
 
-def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: int = 0, **params) -> dict:
+def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: int = 0, voxelizer: str = "cpu",
+                          **params) -> dict:
     """One LbmAeroSolver3D solve (setup, then step() until done) of the
     reference's own adapter; backend 'cpu' is its CPU solver, 'cuda' the CUDA
-    solver through the Lbm3DSolver seam (ORR_STORAGE_* `storage`)."""
-    global _adapter
-    if _adapter is None:
-        lib = ctypes.CDLL(ADAPTER_SO)
+    solver through the Lbm3DSolver seam (ORR_STORAGE_* `storage`); voxelizer
+    'cpu' is the reference's geom::voxelize, 'device' the drop-in of
+    orrery_b200/adapter/voxel_grid_cuda.cpp."""
+    path = ADAPTER_VOXEL_SO if voxelizer == "device" else ADAPTER_SO
+    if path not in _adapter:
+        lib = ctypes.CDLL(path)
         lib.ref_adapter_run.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_int,
                                         ctypes.c_int, _dp, ctypes.c_char_p, ctypes.c_size_t]
-        _adapter = lib
+        _adapter[path] = lib
+    lib = _adapter[path]
     p = dict(ADAPTER_DEFAULTS)
     p.update(params)
     arr = np.array([float(p[k]) for k in _ADAPTER_ORDER])
@@ -589,7 +594,7 @@ def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: in
     t = np.ascontiguousarray(triangles, np.uint32)
     out = np.zeros(len(_ADAPTER_OUT))
     msg = ctypes.create_string_buffer(2048)
-    rc = _adapter.ref_adapter_run(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(arr, _dp),
+    rc = lib.ref_adapter_run(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(arr, _dp),
                                   1 if backend == "cuda" else 0, int(storage), _ptr(out, _dp), msg, 2048)
     if rc != 0:
         raise ReferenceError_(msg.value.decode())

@@ -74,3 +74,19 @@ def test_adapter_halfway_les_and_incidence():
     assert gpu["iterations"] == cpu["iterations"]
     assert abs(gpu["cd"] - cpu["cd"]) / abs(cpu["cd"]) < 1e-4, (gpu["cd"], cpu["cd"])
     assert abs(gpu["cl"] - cpu["cl"]) < 1e-4 * abs(cpu["cd"]), (gpu["cl"], cpu["cl"])
+
+
+def test_adapter_with_the_device_voxelizer():
+    """The adapter with the reference's voxel_grid.cpp replaced by the device
+    voxelizer (orrery_b200/adapter/voxel_grid_cuda.cpp): the same mask and
+    wall distances, so the CPU solver's solve is the same bit for bit, and
+    the whole pipeline on the device meets the reference test's bar."""
+    O = _oracle()
+    v, t, p = sphere_case(O)
+    ref = O.reference_adapter_run(v, t, "cpu", voxelizer="cpu", **p)
+    dev = O.reference_adapter_run(v, t, "cpu", voxelizer="device", **p)
+    assert dev == {**ref, "seconds": dev["seconds"]}
+    gpu = O.reference_adapter_run(v, t, "cuda", 0, voxelizer="device", **p)
+    print(f"measured: adapter on the device end to end, Cd {gpu['cd']!r} (CPU {ref['cd']!r})")
+    assert gpu["iterations"] == ref["iterations"]
+    assert abs(gpu["cd"] - ref["cd"]) / abs(ref["cd"]) < 1e-4
