@@ -574,12 +574,13 @@ def adapter_available() -> bool:
 
 
 def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: int = 0, voxelizer: str = "cpu",
-                          **params) -> dict:
+                          fields: bool = False, **params) -> dict:
     """One LbmAeroSolver3D solve (setup, then step() until done) of the
     reference's own adapter; backend 'cpu' is its CPU solver, 'cuda' the CUDA
     solver through the Lbm3DSolver seam (ORR_STORAGE_* `storage`); voxelizer
     'cpu' is the reference's geom::voxelize, 'device' the drop-in of
-    orrery_b200/adapter/voxel_grid_cuda.cpp."""
+    orrery_b200/adapter/voxel_grid_cuda.cpp.  fields: also the result's wall
+    pressure coefficients ("cp") and velocity field ("velocity", m/s, n x 3)."""
     path = ADAPTER_VOXEL_SO if voxelizer == "device" else ADAPTER_SO
     if path not in _adapter:
         lib = ctypes.CDLL(path)
@@ -598,4 +599,15 @@ def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: in
                                   1 if backend == "cuda" else 0, int(storage), _ptr(out, _dp), msg, 2048)
     if rc != 0:
         raise ReferenceError_(msg.value.decode())
-    return dict(zip(_ADAPTER_OUT, out.tolist()))
+    result = dict(zip(_ADAPTER_OUT, out.tolist()))
+    if fields:
+        u64 = ctypes.POINTER(ctypes.c_uint64)
+        lib.ref_adapter_fields.argtypes = [u64, u64, _dp, _dp]
+        nc, nv_ = ctypes.c_uint64(), ctypes.c_uint64()
+        lib.ref_adapter_fields(ctypes.byref(nc), ctypes.byref(nv_), None, None)
+        cp = np.zeros(max(nc.value, 1))
+        vel = np.zeros(max(nv_.value, 1))
+        lib.ref_adapter_fields(ctypes.byref(nc), ctypes.byref(nv_), _ptr(cp, _dp), _ptr(vel, _dp))
+        result["cp"] = cp[:nc.value]
+        result["velocity"] = vel[:nv_.value].reshape(-1, 3)
+    return result

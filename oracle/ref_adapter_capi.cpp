@@ -16,6 +16,7 @@
 #include <exception>
 #include <numbers>
 #include <string>
+#include <vector>
 
 #include "lbm3d_cuda.h"
 #include "orrery/aero/compute/null_compute_backend.h"
@@ -36,6 +37,11 @@ core::Result<std::unique_ptr<Lbm3DSolver>, std::string> make_gpu_solver(compute:
 } // namespace orrery::aero::lbm
 
 namespace {
+
+// Wall pressure coefficients and the velocity field (3 per node, m/s) of the
+// last solve, for ref_adapter_fields.
+std::vector<double> g_cp;
+std::vector<double> g_velocity;
 
 void copy_message(const std::string& text, char* message, size_t capacity) {
     if (message == nullptr || capacity == 0) {
@@ -58,7 +64,9 @@ extern "C" {
 // sample_every.  backend: 0 the reference CPU solver, 1 the CUDA solver with
 // `storage`.  out: cd, cl, cy, cm, force x y z, moment x y z, iterations,
 // converged, seconds, nx, ny, nz, lattice steps.  0 on success; -1 with the
-// exception's text.
+// exception's text.  The wall pressure coefficients and the velocity field
+// (update_result, lbm_aero_solver3d.cpp:489-550) are kept for
+// ref_adapter_fields.
 int ref_adapter_run(const double* vertices, uint64_t nv, const uint32_t* triangles, uint64_t nt, const double* p,
                     int backend, int storage, double* out, char* message, size_t capacity) {
     namespace lbm = orrery::aero::lbm;
@@ -105,6 +113,14 @@ int ref_adapter_run(const double* vertices, uint64_t nv, const uint32_t* triangl
         }
         const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         const orrery::aero::AeroResult& r = solver.result();
+        g_cp = r.surface.cp;
+        g_velocity.clear();
+        if (r.velocity) {
+            g_velocity.reserve(3 * r.velocity->values.size());
+            for (const auto& v : r.velocity->values) {
+                g_velocity.insert(g_velocity.end(), {v.x, v.y, v.z});
+            }
+        }
         const double v[] = {r.cd,
                             r.cl,
                             r.cy,
@@ -127,6 +143,19 @@ int ref_adapter_run(const double* vertices, uint64_t nv, const uint32_t* triangl
     } catch (const std::exception& e) {
         copy_message(e.what(), message, capacity);
         return -1;
+    }
+}
+
+// Sizes (cp values, velocity doubles) of the last solve's fields, and a copy
+// of them when the pointers are not null.
+void ref_adapter_fields(uint64_t* cp_count, uint64_t* velocity_count, double* cp, double* velocity) {
+    *cp_count = g_cp.size();
+    *velocity_count = g_velocity.size();
+    if (cp != nullptr) {
+        std::memcpy(cp, g_cp.data(), g_cp.size() * sizeof(double));
+    }
+    if (velocity != nullptr) {
+        std::memcpy(velocity, g_velocity.data(), g_velocity.size() * sizeof(double));
     }
 }
 

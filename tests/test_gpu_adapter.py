@@ -11,6 +11,7 @@ force to the rounding of its summation order.
 """
 import math
 
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -38,13 +39,19 @@ def sphere_case(O):
 def test_adapter_runs_on_the_cuda_solver():
     O = _oracle()
     v, t, p = sphere_case(O)
-    cpu = O.reference_adapter_run(v, t, "cpu", **p)
-    gpu = O.reference_adapter_run(v, t, "cuda", 0, **p)
+    cpu = O.reference_adapter_run(v, t, "cpu", fields=True, **p)
+    gpu = O.reference_adapter_run(v, t, "cuda", 0, fields=True, **p)
     print(f"measured: 3D adapter Cd CPU {cpu['cd']!r}, CUDA {gpu['cd']!r}; lattice "
           f"{int(cpu['nx'])}x{int(cpu['ny'])}x{int(cpu['nz'])}, {int(cpu['lattice_steps'])} steps; "
           f"{cpu['seconds']:.2f} s CPU, {gpu['seconds']:.2f} s CUDA")
     assert (gpu["nx"], gpu["ny"], gpu["nz"]) == (cpu["nx"], cpu["ny"], cpu["nz"])
     assert gpu["iterations"] == cpu["iterations"]
+    # the result's wall pressure and velocity field (update_result), read back
+    # through the solver's macroscopic(): the same samples, binary32 close
+    assert len(gpu["cp"]) == len(cpu["cp"]) > 0
+    assert np.max(np.abs(gpu["cp"] - cpu["cp"])) < 1e-3 * np.max(np.abs(cpu["cp"]))
+    assert gpu["velocity"].shape == cpu["velocity"].shape
+    assert np.max(np.abs(gpu["velocity"] - cpu["velocity"])) < 1e-4 * p["speed"]
     assert gpu["lattice_steps"] == cpu["lattice_steps"]
     assert abs(gpu["cd"] - cpu["cd"]) / abs(cpu["cd"]) < 1e-4, (gpu["cd"], cpu["cd"])
 
