@@ -357,8 +357,32 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     if (interpolated) {
         p.nslot.assign(p.cells, -1);
     }
+    // Rows (y, z) holding a solid node.  An interior row whose 3 x 3 block of
+    // neighbouring rows holds none is bulk from end to end with no link (its
+    // x-edge sources are in the same rows, or an inlet / outlet), so it is
+    // skipped; the others are classified node by node, in scan order.
+    std::vector<uint8_t> row_solid(static_cast<std::size_t>(ny * nz), 0);
+    for (long r = 0; r < ny * nz; ++r) {
+        const uint8_t* row = solid + r * nx;
+        row_solid[static_cast<std::size_t>(r)] =
+            std::any_of(row, row + nx, [](uint8_t s) { return s != 0; }) ? 1 : 0;
+    }
+    const auto quiet = [&](long y, long z) {
+        for (long dz = -1; dz <= 1; ++dz) {
+            for (long dy = -1; dy <= 1; ++dy) {
+                if (row_solid[static_cast<std::size_t>((y + dy) + ny * (z + dz))] != 0) {
+                    return false;
+                }
+            }
+        }
+        return true;
+    };
     for (long z = 0; z < nz; ++z) {
         for (long y = 0; y < ny; ++y) {
+            if (y > 0 && y + 1 < ny && z > 0 && z + 1 < nz && quiet(y, z)) {
+                p.fluid += static_cast<std::size_t>(nx);
+                continue;
+            }
             for (long x = 0; x < nx; ++x) {
                 const std::size_t h = static_cast<std::size_t>(x + nx * (y + ny * z));
                 if (solid[h] != 0) {

@@ -460,6 +460,20 @@ orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
     });
 }
 
+namespace {
+
+// Binary64 moment planes from the binary32 ones of the shifted forms (rho is
+// stored as rho - 1), written where the host copies them from.
+__global__ void widen_moments_kernel(const float* __restrict__ m, double* __restrict__ out, uint64_t cells) {
+    const uint64_t n = 4 * cells;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        out[i] = static_cast<double>(m[i]) + (i < cells ? 1.0 : 0.0);
+    }
+}
+
+} // namespace
+
 orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, double* uy,
                                  double* uz) {
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
@@ -470,26 +484,26 @@ orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, dou
               "moments kernel");
         ++h->launches;
         double* outs[4] = {rho, ux, uy, uz};
-        const bool shifted = h->storage != ORR_STORAGE_F64;
-        std::vector<float> tmp(shifted ? cells : 0);
+        // The binary32 planes are widened on the device into the idle
+        // population buffer (19 values of at least 2 bytes per node hold 4
+        // doubles; the next step overwrites it whole), then copied straight
+        // into the caller's arrays.
+        const double* planes = static_cast<const double*>(h->moments);
+        if (h->storage != ORR_STORAGE_F64) {
+            double* wide = static_cast<double*>(h->f[1 - h->cur]);
+            widen_moments_kernel<<<std::min<uint64_t>((4 * cells + 255) / 256, 4 * 1184), 256, 0, h->stream>>>(
+                static_cast<const float*>(h->moments), wide, cells);
+            check(cudaGetLastError(), "moment widening");
+            ++h->launches;
+            planes = wide;
+        }
         for (int k = 0; k < 4; ++k) {
-            if (outs[k] == nullptr) {
-                continue;
-            }
-            const char* plane = static_cast<const char*>(h->moments) + k * cells * h->abytes;
-            if (shifted) {
-                check(cudaMemcpyAsync(tmp.data(), plane, cells * 4, cudaMemcpyDeviceToHost, h->stream),
+            if (outs[k] != nullptr) {
+                check(cudaMemcpyAsync(outs[k], planes + k * cells, cells * 8, cudaMemcpyDeviceToHost, h->stream),
                       "moment read-back");
-                check(cudaStreamSynchronize(h->stream), "moment read-back");
-                for (std::size_t c = 0; c < cells; ++c) {
-                    outs[k][c] = static_cast<double>(tmp[c]) + (k == 0 ? 1.0 : 0.0);
-                }
-            } else {
-                check(cudaMemcpyAsync(outs[k], plane, cells * 8, cudaMemcpyDeviceToHost, h->stream),
-                      "moment read-back");
-                check(cudaStreamSynchronize(h->stream), "moment read-back");
             }
         }
+        check(cudaStreamSynchronize(h->stream), "moment read-back");
         return ORR_OK;
     });
 }
