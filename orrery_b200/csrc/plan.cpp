@@ -2,6 +2,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <thread>
 #include <cmath>
 #include <iomanip>
 #include <limits>
@@ -357,16 +358,23 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     if (interpolated) {
         p.nslot.assign(p.cells, -1);
     }
+    // Large lattices are planned in z-slabs on several host threads; each slab
+    // keeps its links and wall slots in scan order and the slabs are joined in
+    // z order, which is the scan order of the whole lattice.
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const long workers = p.cells >= (std::size_t{1} << 20) ? std::min<long>({static_cast<long>(hw), 32L, nz}) : 1L;
     // Rows (y, z) holding a solid node.  An interior row whose 3 x 3 block of
     // neighbouring rows holds none is bulk from end to end with no link (its
     // x-edge sources are in the same rows, or an inlet / outlet), so it is
     // skipped; the others are classified node by node, in scan order.
     std::vector<uint8_t> row_solid(static_cast<std::size_t>(ny * nz), 0);
-    for (long r = 0; r < ny * nz; ++r) {
-        const uint8_t* row = solid + r * nx;
-        row_solid[static_cast<std::size_t>(r)] =
-            std::any_of(row, row + nx, [](uint8_t s) { return s != 0; }) ? 1 : 0;
-    }
+    const auto scan_rows = [&](long r0, long r1) {
+        for (long r = r0; r < r1; ++r) {
+            const uint8_t* row = solid + r * nx;
+            row_solid[static_cast<std::size_t>(r)] =
+                std::any_of(row, row + nx, [](uint8_t s) { return s != 0; }) ? 1 : 0;
+        }
+    };
     const auto quiet = [&](long y, long z) {
         for (long dz = -1; dz <= 1; ++dz) {
             for (long dy = -1; dy <= 1; ++dy) {
@@ -377,66 +385,105 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
         }
         return true;
     };
-    for (long z = 0; z < nz; ++z) {
-        for (long y = 0; y < ny; ++y) {
-            if (y > 0 && y + 1 < ny && z > 0 && z + 1 < nz && quiet(y, z)) {
-                p.fluid += static_cast<std::size_t>(nx);
-                continue;
-            }
-            for (long x = 0; x < nx; ++x) {
-                const std::size_t h = static_cast<std::size_t>(x + nx * (y + ny * z));
-                if (solid[h] != 0) {
-                    p.cls[h] = kSolid;
+    struct Slab {
+        std::size_t fluid = 0, general = 0;
+        std::vector<uint32_t> link_cell, link_dir;
+        std::vector<double> link_q;
+        std::vector<double> wall_q;        // 19 per local slot
+        std::vector<std::size_t> slotted;  // cells given a local slot
+    };
+    const auto classify = [&](long z0, long z1, Slab& s) {
+        for (long z = z0; z < z1; ++z) {
+            for (long y = 0; y < ny; ++y) {
+                if (y > 0 && y + 1 < ny && z > 0 && z + 1 < nz && quiet(y, z)) {
+                    s.fluid += static_cast<std::size_t>(nx);
                     continue;
                 }
-                ++p.fluid;
-                const bool face_row = y == 0 || z == 0 || y + 1 == ny || z + 1 == nz;
-                const bool x_edge = x == 0 || x + 1 == nx;
-                if (!face_row && !x_edge) {
-                    bool near = false;
-                    for (int i = 1; i < d3::Q && !near; ++i) {
-                        near = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
-                    }
-                    if (!near) {
-                        continue; // kBulk
-                    }
-                }
-                int32_t slot = -1;
-                bool linked = false;
-                uint32_t mask = 0;
-                for (int i = 1; i < d3::Q; ++i) {
-                    if (!bounces3d(c, solid, x, y, z, i)) {
+                for (long x = 0; x < nx; ++x) {
+                    const std::size_t h = static_cast<std::size_t>(x + nx * (y + ny * z));
+                    if (solid[h] != 0) {
+                        p.cls[h] = kSolid;
                         continue;
                     }
-                    linked = true;
-                    mask |= 1u << i;
-                    const double q = link_fraction3d(c, solid, distance, x, y, z, i);
-                    p.link_cell.push_back(static_cast<uint32_t>(h));
-                    p.link_dir.push_back(static_cast<uint32_t>(i));
-                    p.link_q.push_back(q);
-                    if (interpolated) {
-                        if (slot < 0) {
-                            slot = static_cast<int32_t>(p.wall_q.size() / d3::Q);
-                            p.wall_q.insert(p.wall_q.end(), d3::Q, 0.5);
+                    ++s.fluid;
+                    const bool face_row = y == 0 || z == 0 || y + 1 == ny || z + 1 == nz;
+                    const bool x_edge = x == 0 || x + 1 == nx;
+                    if (!face_row && !x_edge) {
+                        bool near = false;
+                        for (int i = 1; i < d3::Q && !near; ++i) {
+                            near = solid[static_cast<std::size_t>(static_cast<long>(h) + off[i])] != 0;
                         }
-                        p.wall_q[static_cast<std::size_t>(slot) * d3::Q + static_cast<std::size_t>(i)] = q;
+                        if (!near) {
+                            continue; // kBulk
+                        }
                     }
-                }
-                if (!linked) {
-                    if (face_row) {
-                        p.cls[h] = kFace;
-                        ++p.general;
+                    int32_t slot = -1;
+                    bool linked = false;
+                    uint32_t mask = 0;
+                    for (int i = 1; i < d3::Q; ++i) {
+                        if (!bounces3d(c, solid, x, y, z, i)) {
+                            continue;
+                        }
+                        linked = true;
+                        mask |= 1u << i;
+                        const double q = link_fraction3d(c, solid, distance, x, y, z, i);
+                        s.link_cell.push_back(static_cast<uint32_t>(h));
+                        s.link_dir.push_back(static_cast<uint32_t>(i));
+                        s.link_q.push_back(q);
+                        if (interpolated) {
+                            if (slot < 0) {
+                                slot = static_cast<int32_t>(s.wall_q.size() / d3::Q);
+                                s.wall_q.insert(s.wall_q.end(), d3::Q, 0.5);
+                            }
+                            s.wall_q[static_cast<std::size_t>(slot) * d3::Q + static_cast<std::size_t>(i)] = q;
+                        }
                     }
-                    continue; // interior-row x-edge node: bulk
-                }
-                p.cls[h] = kBoundary;
-                ++p.general;
-                p.nmask[h] = mask;
-                if (interpolated) {
-                    p.nslot[h] = slot;
+                    if (!linked) {
+                        if (face_row) {
+                            p.cls[h] = kFace;
+                            ++s.general;
+                        }
+                        continue; // interior-row x-edge node: bulk
+                    }
+                    p.cls[h] = kBoundary;
+                    ++s.general;
+                    p.nmask[h] = mask;
+                    if (interpolated) {
+                        p.nslot[h] = slot;
+                        s.slotted.push_back(h);
+                    }
                 }
             }
         }
+    };
+    std::vector<Slab> slabs(static_cast<std::size_t>(workers));
+    const auto slab_z = [&](long w) { return nz * w / workers; };
+    if (workers == 1) {
+        scan_rows(0, ny * nz);
+        classify(0, nz, slabs[0]);
+    } else {
+        std::vector<std::thread> pool;
+        for (long w = 0; w < workers; ++w) {
+            pool.emplace_back([&, w] { scan_rows(ny * slab_z(w), ny * slab_z(w + 1)); });
+        }
+        for (std::thread& t : pool) t.join();
+        pool.clear();
+        for (long w = 0; w < workers; ++w) {
+            pool.emplace_back([&, w] { classify(slab_z(w), slab_z(w + 1), slabs[static_cast<std::size_t>(w)]); });
+        }
+        for (std::thread& t : pool) t.join();
+    }
+    for (Slab& s : slabs) {
+        const int32_t first_slot = static_cast<int32_t>(p.wall_q.size() / d3::Q);
+        for (const std::size_t h : s.slotted) {
+            p.nslot[h] += first_slot;
+        }
+        p.fluid += s.fluid;
+        p.general += s.general;
+        p.link_cell.insert(p.link_cell.end(), s.link_cell.begin(), s.link_cell.end());
+        p.link_dir.insert(p.link_dir.end(), s.link_dir.begin(), s.link_dir.end());
+        p.link_q.insert(p.link_q.end(), s.link_q.begin(), s.link_q.end());
+        p.wall_q.insert(p.wall_q.end(), s.wall_q.begin(), s.wall_q.end());
     }
     return p;
 }
