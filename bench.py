@@ -212,7 +212,8 @@ def run_form(args, rank: int) -> int:
         metric, value, unit = "D3Q19 batched solves/s", r["solves_per_s"], "solves/s"
     else:
         r = forms.run_serve(storage=args.storage, count=args.requests, max_steps=args.max_steps,
-                            plain=not args.no_plain, oracle_check=args.oracle_check)
+                            plain=not args.no_plain, oracle_check=args.oracle_check,
+                            kernel=args.serve_kernel, branches=args.serve_branches)
         metric, value, unit = "D3Q19 served solves/s", r["served"]["solves_per_s"], "solves/s"
     clock_info = clocks.stop()
     peak, peak_kind = measured_peak()
@@ -244,6 +245,10 @@ def main(argv=None) -> int:
     ap.add_argument("--oracle-check", type=int, default=0,
                     help="serve form: requests whose Cd is checked against the binary64 form")
     ap.add_argument("--no-plain", action="store_true", help="batched/serve: skip the plain-form baseline")
+    ap.add_argument("--serve-kernel", default="auto", choices=["auto", "rows", "staged"],
+                    help="serve form: the batch schedule's kernel")
+    ap.add_argument("--serve-branches", type=int, default=0,
+                    help="serve form: parallel graph branches of per-lattice launches (0: one launch / stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1000)
     args = ap.parse_args(argv)

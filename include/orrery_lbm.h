@@ -331,9 +331,13 @@ typedef struct orr_serve_options {
     uint32_t max_active;      /* lattices on the device at once */
     uint32_t chunk_steps;     /* steps per round (a multiple of sample_every) */
     uint32_t sample_every;    /* force sampling interval, even */
-    int32_t kernel;           /* batch schedule: ORR_KERNEL_STAGED (default) or ORR_KERNEL_ROWS */
+    int32_t kernel;           /* batch schedule: ORR_KERNEL_AUTO (the row kernel, each lattice on its
+                                 own graph branch, up to 64), ORR_KERNEL_ROWS or ORR_KERNEL_STAGED */
     uint32_t block;           /* 0: the schedule's default */
     uint32_t stages;          /* 0: tuned default */
+    uint32_t branches;        /* as orr_batch_schedule::branches: 0 one launch (staged) or one stream
+                                 (rows) for all lattices; n > 0 each lattice its own launches, the
+                                 lattices spread over n parallel graph branches */
 } orr_serve_options;
 
 typedef struct orr_solve_request {

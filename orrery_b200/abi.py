@@ -104,7 +104,7 @@ class CServeOptions(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int32), ("device", ctypes.c_int32), ("memory_budget", ctypes.c_uint64),
                 ("max_active", ctypes.c_uint32), ("chunk_steps", ctypes.c_uint32),
                 ("sample_every", ctypes.c_uint32), ("kernel", ctypes.c_int32), ("block", ctypes.c_uint32),
-                ("stages", ctypes.c_uint32)]
+                ("stages", ctypes.c_uint32), ("branches", ctypes.c_uint32)]
 
 
 class CSolveRequest(ctypes.Structure):

@@ -311,9 +311,13 @@ struct orr_server {
             check(cudaSetDevice(opt.device), "cudaSetDevice");
             check_status(orr_batch3d_create(opt.device, &batch), "serve: batch");
             orr_batch_schedule sched{};
-            sched.kernel = opt.kernel == ORR_KERNEL_ROWS ? ORR_KERNEL_ROWS : ORR_KERNEL_STAGED;
+            // Automatic: the row kernel with every lattice on its own graph
+            // branch (up to 64), the fastest schedule measured on the served
+            // sphere-cone stream and on the batch of wings.
+            sched.kernel = opt.kernel == ORR_KERNEL_STAGED ? ORR_KERNEL_STAGED : ORR_KERNEL_ROWS;
             sched.block = opt.block ? opt.block : (sched.kernel == ORR_KERNEL_ROWS ? 128 : 256);
             sched.stages = opt.stages;
+            sched.branches = opt.kernel == ORR_KERNEL_AUTO && opt.branches == 0 ? 64u : opt.branches;
             if (orr_batch3d_set_schedule(batch, &sched) != ORR_OK) {
                 throw Refusal{ORR_ERR_INVALID, orr_batch3d_last_error(batch)};
             }

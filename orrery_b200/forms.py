@@ -115,9 +115,9 @@ def run_batched(storage: str = "f32", count: int = 64, steps: int = 3000, seed: 
 
 
 def _serve_once(requests, workloads, storage, max_active, memory_budget, window, tolerance, max_steps,
-                chunk_steps) -> dict:
+                chunk_steps, kernel="auto", branches=0) -> dict:
     with Server(storage=storage, memory_budget=memory_budget, max_active=max_active,
-                chunk_steps=chunk_steps, sample_every=10) as srv:
+                chunk_steps=chunk_steps, sample_every=10, kernel=kernel, branches=branches) as srv:
         ids = []
         t0 = time.perf_counter()
         caps = max_steps if isinstance(max_steps, (list, tuple)) else [max_steps] * len(requests)
@@ -146,7 +146,7 @@ def _serve_once(requests, workloads, storage, max_active, memory_budget, window,
 def run_serve(storage: str = "f16", count: int = 48, rate: float = 20.0, seed: int = 5,
               window: int = 500, tolerance: float = 1e-4, max_steps: int = 20000,
               memory_budget: float = 150e9, max_active: int = 64, chunk_steps: int = 100,
-              plain: bool = True, oracle_check: int = 0) -> dict:
+              plain: bool = True, oracle_check: int = 0, kernel: str = "auto", branches: int = 0) -> dict:
     requests = W.sphere_cone_requests(seed=seed, count=count, rate=rate)
     t0 = time.perf_counter()
     workloads = []
@@ -162,10 +162,13 @@ def run_serve(storage: str = "f16", count: int = 48, rate: float = 20.0, seed: i
            "tolerance": tolerance, "max_steps": max_steps, "memory_budget_gb": memory_budget / 1e9,
            "nodes_total": int(sum(r.cells for r in requests)), "host_build_s": t_build}
     out["served"] = _serve_once(requests, workloads, storage, max_active, memory_budget, window, tolerance,
-                                max_steps, chunk_steps)
+                                max_steps, chunk_steps, kernel, branches)
+    out["served"]["schedule"] = {"kernel": kernel, "branches": branches}
     if plain:
+        # one slot, binary32, on the row kernel (the single solver's choice
+        # for binary32 storage)
         out["plain"] = _serve_once(requests, workloads, "f32", 1, memory_budget, window, tolerance,
-                                   max_steps, chunk_steps)
+                                   max_steps, chunk_steps, "rows", 0)
         out["speedup_vs_plain"] = out["served"]["solves_per_s"] / max(out["plain"]["solves_per_s"], 1e-12)
     if oracle_check > 0:
         # Cd of the first requests against the binary64 form of the same

@@ -32,7 +32,7 @@ def _result(r: abi.CSolveResult) -> dict:
 class Server:
     def __init__(self, storage: str = "f32", device: int = 0, memory_budget: float = 150e9,
                  max_active: int = 64, chunk_steps: int = 100, sample_every: int = 10,
-                 kernel: str = "staged", block: int = 0, stages: int = 0):
+                 kernel: str = "auto", block: int = 0, stages: int = 0, branches: int = 0):
         self._lib = lib()
         self._h = None
         o = abi.CServeOptions()
@@ -45,6 +45,7 @@ class Server:
         o.kernel = abi.KERNEL_NAMES[kernel]
         o.block = int(block)
         o.stages = int(stages)
+        o.branches = int(branches)
         h = ctypes.c_void_p()
         check(self._lib.orr_serve_create(ctypes.byref(o), ctypes.byref(h)), self._lib.orr_last_error)
         self._h = h
