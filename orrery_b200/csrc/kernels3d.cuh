@@ -513,11 +513,22 @@ __device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
         rho = r_div(known, r_sub(A(1), ux));
         drho = 0;
     }
+    if constexpr (kShifted) {
+        // The five unknowns (c_x = +1): c.u written out per direction.
+        const A r6a = r_mul(A(6) * A(1.0 / 18.0), rho), r6b = r_mul(A(6) * A(1.0 / 36.0), rho);
+        f[1] = r_add(f[2], r_mul(r6a, ux));
+        f[7] = r_add(f[8], r_mul(r6b, r_add(ux, uy)));
+        f[9] = r_add(f[10], r_mul(r6b, r_sub(ux, uy)));
+        f[11] = r_add(f[12], r_mul(r6b, r_add(ux, uz)));
+        f[13] = r_add(f[14], r_mul(r6b, r_sub(ux, uz)));
+    } else {
 #pragma unroll
-    for (int i = 0; i < d3::Q; ++i) {
-        if (d3::cx(i) > 0) {
-            const A cu = r_add(r_add(r_mul(A(d3::cx(i)), ux), r_mul(A(d3::cy(i)), uy)), r_mul(A(d3::cz(i)), uz));
-            f[i] = r_add(f[d3::opposite(i)], r_mul(r_mul(A(6) * A(d3::w(i)), rho), cu));
+        for (int i = 0; i < d3::Q; ++i) {
+            if (d3::cx(i) > 0) {
+                const A cu = r_add(r_add(r_mul(A(d3::cx(i)), ux), r_mul(A(d3::cy(i)), uy)),
+                                   r_mul(A(d3::cz(i)), uz));
+                f[i] = r_add(f[d3::opposite(i)], r_mul(r_mul(A(6) * A(d3::w(i)), rho), cu));
+            }
         }
     }
     const A uu = r_add(r_add(r_mul(ux, ux), r_mul(uy, uy)), r_mul(uz, uz));
@@ -544,19 +555,34 @@ __device__ __forceinline__ void inlet_west3(A (&f)[d3::Q], const A* inlet) {
         const A pxy = r_sub(r_sub(r_sub(r_add(f[7], f[8]), f[9]), f[10]), r_mul(r_mul(rho, ux), uy));
         const A pxz = r_sub(r_sub(r_sub(r_add(f[11], f[12]), f[13]), f[14]), r_mul(r_mul(rho, ux), uz));
         const A pyz = r_sub(r_sub(r_sub(r_add(f[15], f[16]), f[17]), f[18]), r_mul(r_mul(rho, uy), uz));
-        const A cs2 = A(1.0 / 3.0);
-#pragma unroll
-        for (int i = 0; i < d3::Q; ++i) {
-            const A ex = A(d3::cx(i)), ey = A(d3::cy(i)), ez = A(d3::cz(i));
-            const A cu = r_add(r_add(r_mul(ex, ux), r_mul(ey, uy)), r_mul(ez, uz));
-            const A quad = r_sub(r_add(r_mul(A(3), cu), r_mul(r_mul(A(4.5), cu), cu)), r_mul(A(1.5), uu));
-            const A feq = r_mul(A(d3::w(i)), r_add(drho, r_mul(rho, quad)));
-            const A t = r_add(r_add(r_add(r_mul(ex * ex - cs2, pxx), r_mul(ey * ey - cs2, pyy)),
-                                    r_mul(ez * ez - cs2, pzz)),
-                              r_mul(A(2), r_add(r_add(r_mul(ex * ey, pxy), r_mul(ex * ez, pxz)),
-                                                r_mul(ey * ez, pyz))));
-            f[i] = r_add(feq, r_mul(A(4.5) * A(d3::w(i)), t));
-        }
+        // (c c - c_s^2 I) : Pi_neq by direction, the zero terms left out:
+        // -tr/3 plus the diagonal entries of the axes c moves along, plus
+        // 2 c_a c_b of the off-diagonal one; even in c, so shared by opposites.
+        const A t0 = r_mul(A(-1.0 / 3.0), r_add(r_add(pxx, pyy), pzz));
+        const A tx = r_add(pxx, t0), ty = r_add(pyy, t0), tz = r_add(pzz, t0);
+        const A txy = r_add(tx, pyy), txz = r_add(tx, pzz), tyz = r_add(ty, pzz);
+        const A p2xy = r_mul(A(2), pxy), p2xz = r_mul(A(2), pxz), p2yz = r_mul(A(2), pyz);
+        // f_eq - w = w (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u.u)) for a pair of
+        // opposite directions (c.u = +-cu): even part shared, odd part signed.
+        const A uu15 = r_mul(A(1.5), uu);
+        const auto pair = [&](int plus, int minus, A cu, A t, A w) {
+            const A even = r_sub(r_mul(r_mul(A(4.5), cu), cu), uu15);
+            const A odd = r_mul(A(3), cu);
+            const A neq = r_mul(A(4.5) * w, t);
+            f[plus] = r_add(r_mul(w, r_add(drho, r_mul(rho, r_add(even, odd)))), neq);
+            f[minus] = r_add(r_mul(w, r_add(drho, r_mul(rho, r_sub(even, odd)))), neq);
+        };
+        constexpr A w0 = A(1.0 / 3.0), w1 = A(1.0 / 18.0), w2 = A(1.0 / 36.0);
+        f[0] = r_add(r_mul(w0, r_add(drho, r_mul(rho, -uu15))), r_mul(A(4.5) * w0, t0));
+        pair(1, 2, ux, tx, w1);
+        pair(3, 4, uy, ty, w1);
+        pair(5, 6, uz, tz, w1);
+        pair(7, 8, r_add(ux, uy), r_add(txy, p2xy), w2);
+        pair(9, 10, r_sub(ux, uy), r_sub(txy, p2xy), w2);
+        pair(11, 12, r_add(ux, uz), r_add(txz, p2xz), w2);
+        pair(13, 14, r_sub(ux, uz), r_sub(txz, p2xz), w2);
+        pair(15, 16, r_add(uy, uz), r_add(tyz, p2yz), w2);
+        pair(17, 18, r_sub(uy, uz), r_sub(tyz, p2yz), w2);
         return;
     }
     A feq[d3::Q];
