@@ -135,6 +135,23 @@ def cpu_reference_mlups(workload, seconds: float, threads: int | None = None, us
     return mlups, threads, kind, sample, steps
 
 
+def slowest_rank(value: float, dist=None, device="cuda") -> float:
+    """The largest `value` over all ranks (every rank receives it); the value
+    itself without a process group.  Times are taken as the slowest rank's."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, steps: int, ms: float, world: int) -> float:
+    """Millions of units all ranks processed per second over `ms`, the slowest
+    rank's time (every rank runs the same replica size: weak scaling)."""
+    return units_per_rank * steps * world / (ms * 1e-3) / 1e6
+
+
 def run_reference_arm(args, rank: int):
     from orrery_b200 import workloads as W
     if rank != 0:
@@ -305,14 +322,9 @@ def main(argv=None) -> int:
     barrier()
     clock_info = clocks.stop() if clocks else None
     launches = solver.launch_count() - launches_before
-    ms = start.elapsed_time(stop)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = slowest_rank(start.elapsed_time(stop), dist)
     ms_per_step = ms / args.steps
-    mlups_rank = w.cells * args.steps / (ms * 1e-3) / 1e6
-    mlups = mlups_rank * world
+    mlups = whole_job_rate(w.cells, args.steps, ms, world)
 
     # Force sanity and the coefficient at the end of the timed run.
     f = solver.force()
@@ -344,11 +356,7 @@ def main(argv=None) -> int:
             samples += 1
         fields = s2.macroscopic()
         torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = slowest_rank(time.perf_counter() - t0, dist)
         k = samples * 10
         h2d = w.cells * (1 + 4 * 8) + 8 * 3  # mask, four initial fields, inlet velocity
         d2h = samples * 48 + 4 * 8 * w.cells
