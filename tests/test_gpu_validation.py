@@ -50,3 +50,23 @@ def test_sphere_drag_follows_schiller_naumann(re, cells, up, down, width, durati
     assert abs(r["cd"] / sn - 1.0) < 0.15
     if steady:
         assert r["converged"]
+
+
+def test_square_plate_has_the_drag_of_a_flat_plate():
+    """The reference's plate case (tests/aero_validation/lbm3d/test_plate.cpp):
+    a square plate 1/16 of its side thick, normal to the flow, Re 1000, 24
+    cells per side, 3 sides ahead, 6 behind, 5 wide, 40 convective times with
+    the last 25 averaged; Cd within 15 percent of 1.28 (frontal area)."""
+    from oracle import oracle as O
+    if not O.adapter_available():
+        pytest.skip("adapter harness not built (needs the reference tree at build time)")
+    v, t = O.reference_mesh("box", 1.0 / 16.0, 1.0, 1.0)
+    re = 1000.0
+    r = O.reference_adapter_run(v, t, "cuda", 0, voxelizer="device", length=1.0, area=1.0, speed=0.1,
+                                density=1000.0, viscosity=1000.0 * 0.1 * 1.0 / re, cells_per_length=24.0,
+                                lattice_velocity=0.05, upstream=3.0, downstream=6.0, width=5.0, duration=40.0,
+                                average_window=25.0, steps_per_call=2000, les=2, sample_every=10)
+    print(f"measured: plate Re {re:g}: Cd {r['cd']:.4f}, reference 1.28, ratio {r['cd'] / 1.28:.4f}; "
+          f"lattice {int(r['nx'])}x{int(r['ny'])}x{int(r['nz'])}, {int(r['lattice_steps'])} steps, "
+          f"{r['seconds']:.1f} s")
+    assert abs(r["cd"] / 1.28 - 1.0) < 0.15
