@@ -31,6 +31,7 @@ inline constexpr Candidate kCandidates[] = {
     {ORR_KERNEL_STAGED, 256, 4, 1, 64}, {ORR_KERNEL_STAGED, 128, 3, 2, 64},
     {ORR_KERNEL_ROWS, 128, 0, 0, 0},    {ORR_KERNEL_ROWS, 128, 0, 0, 64},
     {ORR_KERNEL_ROWS, 128, 0, 2, 0},    {ORR_KERNEL_ROWS, 128, 0, 2, 64},
+    {ORR_KERNEL_ROWS, 64, 0, 0, 0},     {ORR_KERNEL_ROWS, 64, 0, 0, 64},
 };
 
 } // namespace orr
