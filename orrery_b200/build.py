@@ -30,6 +30,7 @@ COMMON = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 
 SOURCES = {
     "common.cpp": [],
+    "host_copy.cpp": [],
     "plan.cpp": [],
     "kernels_f32.cu": [],
     "kernels_f16.cu": [],

@@ -36,12 +36,15 @@ void require_device(int device) {
     if (device < 0 || device >= count) {
         throw Refusal{ORR_ERR_INVALID, "CUDA device ordinal out of range"};
     }
-    cudaDeviceProp prop{};
-    check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    if (prop.major != 10) {
+    // Two attributes rather than the whole property record, whose query
+    // takes milliseconds.
+    int major = 0, minor = 0;
+    check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "cudaDeviceGetAttribute");
+    check(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device), "cudaDeviceGetAttribute");
+    if (major != 10) {
         throw Refusal{ORR_ERR_NO_DEVICE,
                       "the kernels are built for sm_100a; device " + std::to_string(device) +
-                          " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor)};
+                          " is sm_" + std::to_string(major) + std::to_string(minor)};
     }
     check(cudaSetDevice(device), "cudaSetDevice");
 }

@@ -20,6 +20,38 @@ bool finite(double v) {
     return std::isfinite(v);
 }
 
+// Whether any of the n values is a NaN (the only value unequal to itself).
+// Blocks of 4096 values are tested whole, which the compiler vectorises, and
+// large arrays are split over host threads.
+bool any_nan(const double* v, std::size_t n) {
+    const auto scan = [v](std::size_t a, std::size_t b) {
+        for (std::size_t k = a; k < b; k += 4096) {
+            const std::size_t e = std::min(b, k + 4096);
+            bool bad = false;
+            for (std::size_t i = k; i < e; ++i) {
+                bad |= v[i] != v[i];
+            }
+            if (bad) {
+                return true;
+            }
+        }
+        return false;
+    };
+    const std::size_t workers = n >= (std::size_t{1} << 20)
+                                    ? std::min<std::size_t>(std::max(1u, std::thread::hardware_concurrency()), 16)
+                                    : 1;
+    if (workers == 1) {
+        return scan(0, n);
+    }
+    std::vector<char> found(workers, 0);
+    std::vector<std::thread> pool;
+    for (std::size_t w = 0; w < workers; ++w) {
+        pool.emplace_back([&, w] { found[w] = scan(n * w / workers, n * (w + 1) / workers) ? 1 : 0; });
+    }
+    for (std::thread& t : pool) t.join();
+    return std::find(found.begin(), found.end(), 1) != found.end();
+}
+
 double lattice_mach(double speed) {
     // lattice_mach (src/aero/lbm/lattice_units.cpp:19-21): |u| / sqrt(c_s^2).
     return std::abs(speed) / std::sqrt(1.0 / 3.0);
@@ -191,10 +223,8 @@ std::string problem3d(const orr_lbm3d_config& c, const uint8_t* solid, const dou
         if (distance == nullptr) {
             return "lbm3d: the interpolated wall needs the mask's signed distance";
         }
-        for (std::size_t k = 0; k < *cells; ++k) {
-            if (std::isnan(distance[k])) {
-                return "lbm3d: the mask's signed distance must not be NaN";
-            }
+        if (any_nan(distance, *cells)) {
+            return "lbm3d: the mask's signed distance must not be NaN";
         }
     } else if (c.solid_wall != ORR_SOLID_HALFWAY) {
         return "lbm3d: unknown solid wall treatment";
@@ -341,7 +371,7 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     const long nx = static_cast<long>(c.nx), ny = static_cast<long>(c.ny),
                nz = static_cast<long>(c.nz);
     p.cells = static_cast<std::size_t>(nx * ny * nz);
-    p.cls.assign(p.cells, kBulk);
+    p.cls.resize(p.cells);              // filled slab by slab below
     const long plane = nx * ny;
     long off[d3::Q];
     for (int i = 0; i < d3::Q; ++i) {
@@ -354,9 +384,9 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     // face path.  Links are collected in scan order (cell, then direction),
     // the order of boundary_links.
     const bool interpolated = c.solid_wall == ORR_SOLID_INTERPOLATED;
-    p.nmask.assign(p.cells, 0u);
+    p.nmask.resize(p.cells);
     if (interpolated) {
-        p.nslot.assign(p.cells, -1);
+        p.nslot.resize(p.cells);
     }
     // Large lattices are planned in z-slabs on several host threads; each slab
     // keeps its links and wall slots in scan order and the slabs are joined in
@@ -393,6 +423,12 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
         std::vector<std::size_t> slotted;  // cells given a local slot
     };
     const auto classify = [&](long z0, long z1, Slab& s) {
+        const std::size_t c0 = static_cast<std::size_t>(plane * z0), c1 = static_cast<std::size_t>(plane * z1);
+        std::fill(p.cls.begin() + c0, p.cls.begin() + c1, kBulk);
+        std::fill(p.nmask.begin() + c0, p.nmask.begin() + c1, 0u);
+        if (interpolated) {
+            std::fill(p.nslot.begin() + c0, p.nslot.begin() + c1, -1);
+        }
         for (long z = z0; z < z1; ++z) {
             for (long y = 0; y < ny; ++y) {
                 if (y > 0 && y + 1 < ny && z > 0 && z + 1 < nz && quiet(y, z)) {

@@ -6,8 +6,10 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <optional>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "orrery_lbm.h"
@@ -36,13 +38,33 @@ std::string problem3d(const orr_lbm3d_config& c, const uint8_t* solid, const dou
 std::string inlet_problem3d(const orr_lbm3d_config& c, const double velocity[3],
                             bool allow_high_mach);
 
+// Allocator whose value-less construction leaves the element uninitialised:
+// a per-cell table sized with resize() is then written once, by the planner
+// threads that own its slabs, instead of being zeroed first on one thread.
+template <class T> struct UninitAllocator : std::allocator<T> {
+    using value_type = T;
+    template <class U> struct rebind {
+        using other = UninitAllocator<U>;
+    };
+    UninitAllocator() = default;
+    template <class U> UninitAllocator(const UninitAllocator<U>&) noexcept {}
+    template <class U, class... Args> void construct(U* p, Args&&... args) {
+        if constexpr (sizeof...(Args) == 0) {
+            ::new (static_cast<void*>(p)) U;
+        } else {
+            ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+        }
+    }
+};
+template <class T> using CellTable = std::vector<T, UninitAllocator<T>>;
+
 struct Plan3D {
     orr_lbm3d_config c{};
     std::size_t cells = 0;
     std::size_t fluid = 0;
-    std::vector<uint8_t> cls;           // kSolid / kBulk / kBoundary / kFace per cell
-    std::vector<uint32_t> nmask;        // per cell, bit i: direction i bounces back
-    std::vector<int32_t> nslot;         // per cell wall slot (interpolated wall only), -1 none
+    CellTable<uint8_t> cls;             // kSolid / kBulk / kBoundary / kFace per cell
+    CellTable<uint32_t> nmask;          // per cell, bit i: direction i bounces back
+    CellTable<int32_t> nslot;           // per cell wall slot (interpolated wall only), -1 none
     std::size_t general = 0;            // nodes on the general gather (face + boundary)
     std::vector<double> wall_q;         // 19 fractions per slot
     std::vector<uint32_t> link_cell;    // boundary links, scan order

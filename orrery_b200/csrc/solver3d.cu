@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.h"
+#include "host_copy.h"
 #include "kernels3d.cuh"
 #include "lattice.h"
 #include "lattice_table.cuh"
@@ -81,12 +82,12 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
         // node fit in 19 storage values of at least 2 bytes.
         double* base = static_cast<double*>(h->f[1]);
         const double* src[4] = {rho, ux, uy, uz};
+        orr::HostSpan spans[4];
         for (int k = 0; k < 4; ++k) {
             staged[k] = base + static_cast<std::size_t>(k) * cells;
-            check(cudaMemcpyAsync(staged[k], src[k], cells * sizeof(double), cudaMemcpyHostToDevice,
-                                  h->stream),
-                  "initial state upload");
+            spans[k] = {const_cast<double*>(src[k]), staged[k], cells * sizeof(double)};
         }
+        orr::copy_to_device(spans, 4, h->stream, h->device);
     }
     const bool inflow = c.x_boundary == ORR_X_INFLOW_OUTFLOW;
     check(h->ops->init(h->g, h->cls, staged[0], staged[1], staged[2], staged[3], 1.0,
@@ -285,12 +286,12 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         check(cudaMalloc(&h->table, kTableBytes), "lattice table");
         // Uploads.
         cudaStream_t s = h->stream;
-        check(cudaMemcpyAsync(h->cls, p.cls.data(), cells, cudaMemcpyHostToDevice, s), "class upload");
-        check(cudaMemcpyAsync(h->nmask, p.nmask.data(), cells * 4, cudaMemcpyHostToDevice, s),
-              "mask upload");
-        if (!p.nslot.empty()) {
-            check(cudaMemcpyAsync(h->nslot, p.nslot.data(), cells * 4, cudaMemcpyHostToDevice, s),
-                  "slot upload");
+        {
+            orr::HostSpan tables[3] = {
+                {const_cast<uint8_t*>(p.cls.data()), h->cls, cells},
+                {const_cast<uint32_t*>(p.nmask.data()), h->nmask, cells * 4},
+                {const_cast<int32_t*>(p.nslot.data()), h->nslot, p.nslot.empty() ? 0 : cells * 4}};
+            orr::copy_to_device(tables, 3, s, h->device);
         }
         {
             std::vector<double> q = p.wall_q;
@@ -497,13 +498,14 @@ orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, dou
             ++h->launches;
             planes = wide;
         }
+        orr::HostSpan spans[4];
+        int count = 0;
         for (int k = 0; k < 4; ++k) {
             if (outs[k] != nullptr) {
-                check(cudaMemcpyAsync(outs[k], planes + k * cells, cells * 8, cudaMemcpyDeviceToHost, h->stream),
-                      "moment read-back");
+                spans[count++] = {outs[k], const_cast<double*>(planes + k * cells), cells * 8};
             }
         }
-        check(cudaStreamSynchronize(h->stream), "moment read-back");
+        orr::copy_to_host(spans, count, h->stream, h->device);
         return ORR_OK;
     });
 }
@@ -518,15 +520,13 @@ orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
         const std::size_t cells = h->plan.cells;
         const std::size_t n = d3::Q * cells;
         if (h->storage == ORR_STORAGE_F64) {
-            check(cudaMemcpyAsync(f, h->f[h->cur], n * 8, cudaMemcpyDeviceToHost, h->stream),
-                  "population read-back");
-            check(cudaStreamSynchronize(h->stream), "population read-back");
+            const orr::HostSpan all{f, h->f[h->cur], n * 8};
+            orr::copy_to_host(&all, 1, h->stream, h->device);
             return ORR_OK;
         }
         std::vector<unsigned char> raw(n * h->sbytes);
-        check(cudaMemcpyAsync(raw.data(), h->f[h->cur], raw.size(), cudaMemcpyDeviceToHost, h->stream),
-              "population read-back");
-        check(cudaStreamSynchronize(h->stream), "population read-back");
+        const orr::HostSpan all{raw.data(), h->f[h->cur], raw.size()};
+        orr::copy_to_host(&all, 1, h->stream, h->device);
         for (int i = 0; i < d3::Q; ++i) {
             const double w = d3::w(i);
             for (std::size_t c = 0; c < cells; ++c) {

@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "common.h"
+#include "host_copy.h"
 #include "orrery_lbm.h"
 
 namespace orr::geo {
@@ -580,7 +581,8 @@ Grid grid_of(const orr_grid_spec& s) {
 struct Call {
     cudaStream_t stream = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
-    explicit Call(int device) {
+    int device;
+    explicit Call(int device) : device(device) {
         require_device(device);
         check(cudaSetDevice(device), "cudaSetDevice");
         check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
@@ -683,14 +685,11 @@ orr_status orr_voxelize(const orr_mesh* mesh, const orr_grid_spec* spec, double 
         check(cudaGetLastError(), "winding kernel");
         check(cudaEventRecord(call.t1, call.stream), "event");
         uint32_t overflow = 0;
-        check(cudaMemcpyAsync(solid, dsolid, cells, cudaMemcpyDeviceToHost, call.stream), "voxel read-back");
-        if (winding != nullptr) {
-            check(cudaMemcpyAsync(winding, dwinding, cells * sizeof(double), cudaMemcpyDeviceToHost, call.stream),
-                  "winding read-back");
-        }
         check(cudaMemcpyAsync(&overflow, d.overflow, sizeof overflow, cudaMemcpyDeviceToHost, call.stream),
               "status read-back");
-        check(cudaStreamSynchronize(call.stream), "voxelize");
+        const HostSpan out[2] = {{solid, dsolid, cells},
+                                 {winding, dwinding, winding != nullptr ? cells * sizeof(double) : 0}};
+        copy_to_host(out, 2, call.stream, call.device);
         if (overflow != 0) {
             throw Refusal{ORR_ERR_STATE, "voxelize: tree walk exceeded its stack"};
         }
@@ -752,12 +751,10 @@ orr_status orr_signed_distance_band(const orr_mesh* mesh, const orr_grid_spec* s
         check(cudaGetLastError(), "distance kernel");
         check(cudaEventRecord(call.t1, call.stream), "event");
         uint32_t overflow = 0;
-        check(cudaMemcpyAsync(distance, ddist, cells * sizeof(double), cudaMemcpyDeviceToHost, call.stream),
-              "distance read-back");
-        check(cudaMemcpyAsync(in_band, dband, cells, cudaMemcpyDeviceToHost, call.stream), "band read-back");
         check(cudaMemcpyAsync(&overflow, d.overflow, sizeof overflow, cudaMemcpyDeviceToHost, call.stream),
               "status read-back");
-        check(cudaStreamSynchronize(call.stream), "signed_distance_band");
+        const HostSpan out[2] = {{distance, ddist, cells * sizeof(double)}, {in_band, dband, cells}};
+        copy_to_host(out, 2, call.stream, call.device);
         if (overflow != 0) {
             throw Refusal{ORR_ERR_STATE, "signed_distance_band: tree walk exceeded its stack"};
         }
