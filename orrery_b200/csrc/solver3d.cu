@@ -9,8 +9,10 @@
 #include <algorithm>
 #include <array>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.h"
@@ -209,7 +211,66 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         h->ops = &ops_for(o.storage);
         h->sbytes = storage_bytes(o.storage);
         h->abytes = arithmetic_bytes(o.storage);
-        h->plan = plan3d(*config, solid, distance);
+        // The buffers whose sizes follow from the configuration alone (not
+        // from the plan's links and wall slots) are allocated on a helper
+        // thread while this one plans the lattice, when that part of the
+        // memory check fits already; the full check follows the plan, against
+        // the free memory measured before either started.
+        const std::size_t cells = static_cast<std::size_t>(config->nx) * config->ny * config->nz;
+        const bool interpolated = config->solid_wall == ORR_SOLID_INTERPOLATED;
+        orr_lbm3d* hp = h.get();
+        const auto allocate_fixed = [hp, cells, interpolated, config]() {
+            check(cudaSetDevice(hp->device), "cudaSetDevice");
+            check(cudaStreamCreateWithFlags(&hp->stream, cudaStreamNonBlocking), "stream");
+            for (int k = 0; k < 2; ++k) {
+                const std::size_t bytes = (d3::Q * cells + 2 * kPopPad) * hp->sbytes;
+                check(cudaMalloc(&hp->fbase[k], bytes), "population buffer");
+                check(cudaMemsetAsync(hp->fbase[k], 0, bytes, hp->stream), "population buffer");
+                hp->f[k] = static_cast<char*>(hp->fbase[k]) + kPopPad * hp->sbytes;
+            }
+            hp->cls = device_alloc<uint8_t>(cells + kClassPad, "node class buffer");
+            check(cudaMemsetAsync(hp->cls + cells, 0, kClassPad, hp->stream), "node class buffer");
+            hp->nmask = device_alloc<uint32_t>(cells, "bounce-back mask buffer");
+            if (interpolated) {
+                hp->nslot = device_alloc<int32_t>(cells, "wall slot buffer");
+            }
+            check(cudaMalloc(&hp->hist,
+                             static_cast<std::size_t>(d3::kOutletSlots) * config->ny * config->nz * hp->abytes),
+                  "outlet buffer");
+            check(cudaMalloc(&hp->moments, 4 * cells * hp->abytes), "moment buffer");
+            check(cudaMalloc(&hp->small, 256), "small buffer");
+            check(cudaMemsetAsync(hp->small, 0, 256, hp->stream), "small buffer");
+            check(cudaMallocHost(reinterpret_cast<void**>(&hp->host_small), 256), "pinned buffer");
+            check(cudaMalloc(&hp->table, kTableBytes), "lattice table");
+        };
+        std::size_t free_bytes = 0, total_bytes = 0;
+        check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
+        {
+            const auto fixed = memory3d(*config, 0, 0, o.storage);
+            std::exception_ptr failed;
+            std::thread helper;
+            if (fixed && *fixed <= free_bytes) {
+                helper = std::thread([&] {
+                    try {
+                        allocate_fixed();
+                    } catch (...) {
+                        failed = std::current_exception();
+                    }
+                });
+            }
+            try {
+                h->plan = plan3d(*config, solid, distance);
+            } catch (...) {
+                if (helper.joinable()) helper.join();
+                throw;
+            }
+            if (helper.joinable()) {
+                helper.join();
+                if (failed) {
+                    std::rethrow_exception(failed);
+                }
+            }
+        }
         const Plan3D& p = h->plan;
         // The memory check counts every table the solver allocates
         // (check_memory, lbm3d_gpu.cpp:129-149).
@@ -218,8 +279,6 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         if (!need) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the device memory of the lattice overflows std::size_t"};
         }
-        std::size_t free_bytes = 0, total_bytes = 0;
-        check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
         if (*need > free_bytes) {
             throw Refusal{ORR_ERR_MEMORY, "lbm3d gpu: the lattice needs " + mebibytes(*need) +
                                               " of device memory, " + mebibytes(free_bytes) +
@@ -258,32 +317,15 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         fill_phys(h->phys64, *config, false);
         h->smag = config->smagorinsky_enabled != 0 &&
                   (binary32 ? h->phys32.smag_c2 > 0.0f : true);
-        // Streams and device tables.
-        check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
-        const std::size_t cells = p.cells;
-        for (int k = 0; k < 2; ++k) {
-            const std::size_t bytes = (d3::Q * cells + 2 * kPopPad) * h->sbytes;
-            check(cudaMalloc(&h->fbase[k], bytes), "population buffer");
-            check(cudaMemsetAsync(h->fbase[k], 0, bytes, h->stream), "population buffer");
-            h->f[k] = static_cast<char*>(h->fbase[k]) + kPopPad * h->sbytes;
-        }
-        h->cls = device_alloc<uint8_t>(cells + kClassPad, "node class buffer");
-        check(cudaMemsetAsync(h->cls + cells, 0, kClassPad, h->stream), "node class buffer");
-        h->nmask = device_alloc<uint32_t>(cells, "bounce-back mask buffer");
-        if (!p.nslot.empty()) {
-            h->nslot = device_alloc<int32_t>(cells, "wall slot buffer");
+        // Streams and device tables (the plan-sized ones here; the others
+        // unless the helper made them).
+        if (h->stream == nullptr) {
+            allocate_fixed();
         }
         check(cudaMalloc(&h->wall_q, std::max<std::size_t>(slots, 1) * d3::Q * h->abytes), "wall buffer");
-        check(cudaMalloc(&h->hist, static_cast<std::size_t>(d3::kOutletSlots) * config->ny * config->nz * h->abytes),
-              "outlet buffer");
-        check(cudaMalloc(&h->moments, 4 * cells * h->abytes), "moment buffer");
         h->lcell = device_alloc<uint32_t>(p.link_cell.size(), "link buffer");
         h->ldir = device_alloc<uint32_t>(p.link_cell.size(), "link buffer");
         h->lq = device_alloc<double>(p.link_cell.size(), "link buffer");
-        check(cudaMalloc(&h->small, 256), "small buffer");
-        check(cudaMemsetAsync(h->small, 0, 256, h->stream), "small buffer");
-        check(cudaMallocHost(reinterpret_cast<void**>(&h->host_small), 256), "pinned buffer");
-        check(cudaMalloc(&h->table, kTableBytes), "lattice table");
         // Uploads.
         cudaStream_t s = h->stream;
         {
