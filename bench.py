@@ -347,28 +347,37 @@ def main(argv=None) -> int:
     if args.e2e_steps >= 10 and args.e2e_repeats >= 1:
         import numpy as np
         samples = args.e2e_steps // 10
-        times = []
+        times, phases = [], []
         for _ in range(args.e2e_repeats):
             barrier()
             t0 = time.perf_counter()
             s2 = S.make_gpu_solver(w.config, w.mask, storage=args.storage, device=local_rank, block_x=args.block,
                                    kernel=args.kernel, stages=args.stages, nodes_per_thread=args.npt)
+            t1 = time.perf_counter()
             s2.initialize(w.rho, w.ux, w.uy, w.uz)
+            t2 = time.perf_counter()
             for _ in range(samples):
                 s2.step(10)
                 s2.force()
+            t3 = time.perf_counter()
             fields = s2.macroscopic()
             torch.cuda.synchronize()
-            times.append(slowest_rank(time.perf_counter() - t0, dist))
+            t4 = time.perf_counter()
+            times.append(slowest_rank(t4 - t0, dist))
+            # this rank's phases (the whole solve above is the slowest rank's)
+            phases.append({"create": (t1 - t0) * 1e3, "initialize": (t2 - t1) * 1e3,
+                           "steps_and_forces": (t3 - t2) * 1e3, "macroscopic": (t4 - t3) * 1e3})
             del fields
             s2.close()
         e2e_s = float(np.median(times))
+        mid = phases[int(np.argsort(times)[len(times) // 2])]
         k = samples * 10
         h2d = w.cells * (1 + 4 * 8) + 8 * 3  # mask, four initial fields, inlet velocity
         d2h = samples * 48 + 4 * 8 * w.cells
         e2e = {"value": w.cells * k * world / e2e_s / 1e6, "unit": "MLUPS",
                "h2d_bytes_per_step": h2d / k, "d2h_bytes_per_step": d2h / k,
                "steps": k, "seconds": e2e_s, "seconds_each": times,
+               "phases_ms": {key: round(v, 2) for key, v in mid.items()},
                "note": f"whole solves per rank, median of {len(times)}: create (plan + upload), initialise from "
                        "host fields, steps with the force read back every 10 steps, moments read back"}
 

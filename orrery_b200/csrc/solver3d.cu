@@ -493,11 +493,18 @@ orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
         if (links > 0) {
             ++h->launches;
         }
-        check(cudaMemcpyAsync(h->host_small + 8, h->acc(), 6 * sizeof(double), cudaMemcpyDeviceToHost,
-                              h->stream),
+        // One read-back: the six sums (64 bytes into the small buffer) and,
+        // for the persistent step, its status word (kStatusOffset).
+        static_assert(kStatusOffset >= 64 + 6 * sizeof(double) && kStatusOffset + 4 <= 64 + 192);
+        const std::size_t bytes = h->persistent ? kStatusOffset + 4 - 64 : 6 * sizeof(double);
+        check(cudaMemcpyAsync(h->host_small + 8, h->acc(), bytes, cudaMemcpyDeviceToHost, h->stream),
               "force read-back");
         check(cudaStreamSynchronize(h->stream), "force read-back");
-        h->check_status();
+        if (h->persistent) {
+            uint32_t word = 0;
+            std::memcpy(&word, reinterpret_cast<const char*>(h->host_small + 8) + (kStatusOffset - 64), 4);
+            orr_lbm3d::raise_status(word);
+        }
         std::memcpy(force_moment, h->host_small + 8, 6 * sizeof(double));
         return ORR_OK;
     });

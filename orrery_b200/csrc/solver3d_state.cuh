@@ -220,7 +220,10 @@ struct orr_lbm3d {
         check(cudaMemcpyAsync(word, status(), sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
               "status read-back");
         check(cudaStreamSynchronize(stream), "status read-back");
-        if (*word != 0u) {
+        raise_status(*word);
+    }
+    static void raise_status(uint32_t word) {
+        if (word != 0u) {
             throw Refusal{ORR_ERR_TIMEOUT, "lbm3d gpu: a staged step gave up waiting for its row copies; "
                                         "the populations are invalid until initialize"};
         }
