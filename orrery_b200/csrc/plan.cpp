@@ -393,10 +393,9 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
     // z order, which is the scan order of the whole lattice.
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const long workers = p.cells >= (std::size_t{1} << 20) ? std::min<long>({static_cast<long>(hw), 32L, nz}) : 1L;
-    // Rows (y, z) holding a solid node.  An interior row whose 3 x 3 block of
-    // neighbouring rows holds none is bulk from end to end with no link (its
-    // x-edge sources are in the same rows, or an inlet / outlet), so it is
-    // skipped; the others are classified node by node, in scan order.
+    // Rows (y, z) holding a solid node.  A row whose source rows hold none
+    // (`quiet` below) is classified whole: bulk from end to end inside, face
+    // nodes on a y or z face, no link; the others node by node, in scan order.
     std::vector<uint8_t> row_solid(static_cast<std::size_t>(ny * nz), 0);
     const auto scan_rows = [&](long r0, long r1) {
         for (long r = r0; r < r1; ++r) {
@@ -405,10 +404,31 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
                 std::any_of(row, row + nx, [](uint8_t s) { return s != 0; }) ? 1 : 0;
         }
     };
+    // The row a source index s of an axis of n rows reads after the side
+    // rules of bounces3d (periodic wrap, free-slip mirror onto the node's
+    // own row `own`), or -1 across a no-slip domain wall, which makes no link.
+    const auto source_row = [](long s, long n, const orr_wall& lo, const orr_wall& hi, long own) -> long {
+        if (s >= 0 && s < n) {
+            return s;
+        }
+        const orr_wall& w = s < 0 ? lo : hi;
+        if (w.kind == ORR_WALL_PERIODIC) {
+            return (s + n) % n;
+        }
+        return w.kind == ORR_WALL_SLIP ? own : -1;
+    };
+    // A row none of whose source rows (y - c_y, z - c_z after the side rules;
+    // x sources stay in those rows or leave through the inlet or outlet)
+    // holds a solid node has no solid node and no link.
     const auto quiet = [&](long y, long z) {
         for (long dz = -1; dz <= 1; ++dz) {
+            const long sz = source_row(z + dz, nz, c.z_low, c.z_high, z);
+            if (sz < 0) {
+                continue;
+            }
             for (long dy = -1; dy <= 1; ++dy) {
-                if (row_solid[static_cast<std::size_t>((y + dy) + ny * (z + dz))] != 0) {
+                const long sy = source_row(y + dy, ny, c.y_low, c.y_high, y);
+                if (sy >= 0 && row_solid[static_cast<std::size_t>(sy + ny * sz)] != 0) {
                     return false;
                 }
             }
@@ -431,8 +451,15 @@ Plan3D plan3d(const orr_lbm3d_config& c, const uint8_t* solid, const double* dis
         }
         for (long z = z0; z < z1; ++z) {
             for (long y = 0; y < ny; ++y) {
-                if (y > 0 && y + 1 < ny && z > 0 && z + 1 < nz && quiet(y, z)) {
+                if (quiet(y, z)) {
+                    // Interior rows stay bulk from end to end; every node of a
+                    // face row takes the face path.
                     s.fluid += static_cast<std::size_t>(nx);
+                    if (y == 0 || z == 0 || y + 1 == ny || z + 1 == nz) {
+                        const std::size_t r = static_cast<std::size_t>(nx * (y + ny * z));
+                        std::fill(p.cls.begin() + r, p.cls.begin() + r + nx, kFace);
+                        s.general += static_cast<std::size_t>(nx);
+                    }
                     continue;
                 }
                 for (long x = 0; x < nx; ++x) {
