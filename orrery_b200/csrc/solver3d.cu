@@ -211,11 +211,11 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         h->ops = &ops_for(o.storage);
         h->sbytes = storage_bytes(o.storage);
         h->abytes = arithmetic_bytes(o.storage);
-        // The buffers whose sizes follow from the configuration alone (not
-        // from the plan's links and wall slots) are allocated on a helper
-        // thread while this one plans the lattice, when that part of the
-        // memory check fits already; the full check follows the plan, against
-        // the free memory measured before either started.
+        // A helper thread reads the free device memory (a query that has
+        // taken milliseconds) and, when the part of the memory check that
+        // follows from the configuration alone fits, allocates those buffers,
+        // while this thread plans the lattice; the full check, with the plan's
+        // links and wall slots, follows against the free memory it read.
         const std::size_t cells = static_cast<std::size_t>(config->nx) * config->ny * config->nz;
         const bool interpolated = config->solid_wall == ORR_SOLID_INTERPOLATED;
         orr_lbm3d* hp = h.get();
@@ -244,31 +244,29 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             check(cudaMalloc(&hp->table, kTableBytes), "lattice table");
         };
         std::size_t free_bytes = 0, total_bytes = 0;
-        check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
         {
             const auto fixed = memory3d(*config, 0, 0, o.storage);
             std::exception_ptr failed;
-            std::thread helper;
-            if (fixed && *fixed <= free_bytes) {
-                helper = std::thread([&] {
-                    try {
+            std::thread helper([&] {
+                try {
+                    check(cudaSetDevice(hp->device), "cudaSetDevice");
+                    check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
+                    if (fixed && *fixed <= free_bytes) {
                         allocate_fixed();
-                    } catch (...) {
-                        failed = std::current_exception();
                     }
-                });
-            }
+                } catch (...) {
+                    failed = std::current_exception();
+                }
+            });
             try {
                 h->plan = plan3d(*config, solid, distance);
             } catch (...) {
-                if (helper.joinable()) helper.join();
+                helper.join();
                 throw;
             }
-            if (helper.joinable()) {
-                helper.join();
-                if (failed) {
-                    std::rethrow_exception(failed);
-                }
+            helper.join();
+            if (failed) {
+                std::rethrow_exception(failed);
             }
         }
         const Plan3D& p = h->plan;
