@@ -109,6 +109,21 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
     h->upload_inlet(v);
 }
 
+// Unshifted binary64 populations of directions [i0, i0 + gridDim.y) from a
+// shifted storage (value + w_i, the host's decode), written direction-major
+// where the host copies them from.
+template <class S>
+__global__ void widen_populations_kernel(const S* __restrict__ f, double* __restrict__ out, uint64_t cells, int i0) {
+    const int i = i0 + static_cast<int>(blockIdx.y);
+    const double w = d3::w(i);
+    const S* src = f + static_cast<uint64_t>(i) * cells;
+    double* dst = out + static_cast<uint64_t>(blockIdx.y) * cells;
+    for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < cells;
+         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        dst[c] = static_cast<double>(Storage<S>::value(src[c])) + w;
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -571,29 +586,31 @@ orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
             orr::copy_to_host(&all, 1, h->stream, h->device);
             return ORR_OK;
         }
-        std::vector<unsigned char> raw(n * h->sbytes);
-        const orr::HostSpan all{raw.data(), h->f[h->cur], raw.size()};
-        orr::copy_to_host(&all, 1, h->stream, h->device);
-        for (int i = 0; i < d3::Q; ++i) {
-            const double w = d3::w(i);
-            for (std::size_t c = 0; c < cells; ++c) {
-                const std::size_t k = static_cast<std::size_t>(i) * cells + c;
-                double v;
-                if (h->storage == ORR_STORAGE_F32) {
-                    float x;
-                    std::memcpy(&x, raw.data() + 4 * k, 4);
-                    v = x;
-                } else if (h->storage == ORR_STORAGE_F16) {
-                    __half x;
-                    std::memcpy(&x, raw.data() + 2 * k, 2);
-                    v = static_cast<double>(__half2float(x));
-                } else {
-                    __nv_bfloat16 x;
-                    std::memcpy(&x, raw.data() + 2 * k, 2);
-                    v = static_cast<double>(__bfloat162float(x));
-                }
-                f[k] = v + w;
+        // The shifted values are widened on the device into the idle
+        // population buffer (which the next step overwrites whole), as many
+        // directions at a time as it holds in binary64, and each pass is
+        // copied straight into the caller's array.
+        const int per_pass = static_cast<int>(d3::Q * h->sbytes / 8);
+        double* wide = static_cast<double*>(h->f[1 - h->cur]);
+        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((cells + 255) / 256, 1184));
+        for (int i0 = 0; i0 < d3::Q; i0 += per_pass) {
+            const int count = std::min(per_pass, d3::Q - i0);
+            const dim3 grid(blocks, static_cast<unsigned>(count));
+            if (h->storage == ORR_STORAGE_F32) {
+                widen_populations_kernel<<<grid, 256, 0, h->stream>>>(static_cast<const float*>(h->f[h->cur]), wide,
+                                                                      cells, i0);
+            } else if (h->storage == ORR_STORAGE_F16) {
+                widen_populations_kernel<<<grid, 256, 0, h->stream>>>(static_cast<const __half*>(h->f[h->cur]),
+                                                                      wide, cells, i0);
+            } else {
+                widen_populations_kernel<<<grid, 256, 0, h->stream>>>(
+                    static_cast<const __nv_bfloat16*>(h->f[h->cur]), wide, cells, i0);
             }
+            check(cudaGetLastError(), "population widening");
+            ++h->launches;
+            const orr::HostSpan part{f + static_cast<std::size_t>(i0) * cells, wide,
+                                     static_cast<std::size_t>(count) * cells * 8};
+            orr::copy_to_host(&part, 1, h->stream, h->device);
         }
         return ORR_OK;
     });

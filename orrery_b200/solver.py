@@ -204,13 +204,36 @@ class CudaLbm3D:
         self._check(self._lib.orr_lbm3d_inlet_velocity(self._h, ptr(v, _dp)))
         return v
 
-    def macroscopic(self) -> MacroFields3D:
-        out = [np.empty(self.cells) for _ in range(4)]
-        self._check(self._lib.orr_lbm3d_macroscopic(self._h, *[ptr(a, _dp) for a in out]))
-        return MacroFields3D(self.config.nx, self.config.ny, self.config.nz, *out, self._solid.copy())
+    def macroscopic(self, out: MacroFields3D | None = None) -> MacroFields3D:
+        """Density and velocity of every node.  With `out` (the fields of an
+        earlier call on a lattice of this size) the values are written into
+        its arrays, which saves the page faults of fresh ones when fields
+        are read back repeatedly."""
+        if out is None:
+            planes = [np.empty(self.cells) for _ in range(4)]
+        else:
+            planes = [out.density, out.velocity_x, out.velocity_y, out.velocity_z]
+            if any(a.dtype != np.float64 or a.size != self.cells or not a.flags.c_contiguous or not a.flags.writeable
+                   for a in planes):
+                raise LbmError(abi.ORR_ERR_INVALID, "lbm3d: macroscopic(out) needs four writable contiguous "
+                                                    "float64 arrays of nx*ny*nz values")
+        self._check(self._lib.orr_lbm3d_macroscopic(self._h, *[ptr(a, _dp) for a in planes]))
+        if out is not None:
+            return out
+        return MacroFields3D(self.config.nx, self.config.ny, self.config.nz, *planes, self._solid.copy())
 
-    def populations(self) -> np.ndarray:
-        f = np.empty(self.q * self.cells)
+    def populations(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The 19 populations of every node (unshifted), direction-major; into
+        `out` (a writable contiguous float64 array of 19*nx*ny*nz values)
+        when given."""
+        if out is None:
+            f = np.empty(self.q * self.cells)
+        else:
+            f = out
+            if f.dtype != np.float64 or f.size != self.q * self.cells or not f.flags.c_contiguous or \
+                    not f.flags.writeable:
+                raise LbmError(abi.ORR_ERR_INVALID, "lbm3d: populations(out) needs a writable contiguous "
+                                                    "float64 array of 19*nx*ny*nz values")
         self._check(self._lib.orr_lbm3d_populations(self._h, ptr(f, _dp)))
         return f
 

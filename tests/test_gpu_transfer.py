@@ -89,3 +89,31 @@ def test_mask_upload_of_a_full_size_lattice():
     assert np.array_equal(f[:, ~fluid], np.repeat(W[:, None], (~fluid).sum(), 1))
     assert np.all(m.velocity_x[~fluid] == 0.0)
     assert abs(f[:, fluid].sum() - rho[fluid].sum()) < 1e-9 * fluid.sum()
+
+
+def test_read_back_into_earlier_arrays():
+    """macroscopic(out=...) and populations(out=...) write into the arrays of an
+    earlier call (no fresh pages) and give the same bits; arrays of the wrong
+    size or type are refused before anything is copied."""
+    nx, ny, nz = SHAPE
+    cfg = periodic_box(nx, ny, nz, 0.8)
+    mask = SolidMask3D(nx, ny, nz, np.zeros(nx * ny * nz, np.uint8), None)
+    rho, (ux, uy, uz) = _fields(10)
+    with S.make_gpu_solver(cfg, mask) as s:
+        s.initialize(rho, ux, uy, uz)
+        m = s.macroscopic()
+        f = s.populations()
+        s.step(3)
+        m2 = s.macroscopic(out=m)
+        f2 = s.populations(out=f)
+        assert m2 is m and f2 is f
+        fresh, fresh_f = s.macroscopic(), s.populations()
+        for a, b in ((m.density, fresh.density), (m.velocity_x, fresh.velocity_x),
+                     (m.velocity_y, fresh.velocity_y), (m.velocity_z, fresh.velocity_z), (f, fresh_f)):
+            assert np.array_equal(a, b)
+        with pytest.raises(S.LbmError):
+            s.populations(out=np.empty(10))
+        bad = S.MacroFields3D(nx, ny, nz, m.density.astype(np.float32), m.velocity_x, m.velocity_y,
+                              m.velocity_z, m.solid)
+        with pytest.raises(S.LbmError):
+            s.macroscopic(out=bad)
