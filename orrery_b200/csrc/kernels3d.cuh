@@ -1039,14 +1039,21 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
     finish3<S, kSmag>(g, p, b, f, x, y, z, here, dst);
 }
 
-template <class S> constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : 4;
+// Resident 256-thread blocks per SM the row step is compiled for: 48
+// registers for the binary32-arithmetic flat step, 64 for the general one,
+// 128 for binary64.  The flat step fits 48 without spills, and the extra
+// resident warps hide more of the memory latency: 45.5 against 42.8 GLUPS for
+// binary16 storage in 128-thread blocks, 41.4 against 39.9 for binary32 in
+// 256-thread blocks (256 x 128 x 128 sphere channel).
+template <class S, bool kFlat>
+constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : (kFlat ? 5 : 4);
 
 // Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B)
 // of row (y, z).
 // kFlat: the lattice has g.flat set (the independent-load gather; the
 // general one otherwise).
 template <class S, bool kSmag, bool kFlat>
-__global__ void __launch_bounds__(256, kStepMinBlocks<S>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
+__global__ void __launch_bounds__(256, kStepMinBlocks<S, kFlat>) step3d_kernel(Geom3D g, Phys3D<typename Storage<S>::A> p,
                                                         const S* __restrict__ src,
                                                         S* __restrict__ dst, StepBuffers3D b) {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;

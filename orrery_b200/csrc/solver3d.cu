@@ -222,7 +222,12 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         h->device = o.device;
         h->storage = o.storage;
         h->allow_high_mach = o.allow_high_mach != 0;
-        h->block = o.block_x > 0 ? static_cast<uint32_t>(o.block_x) : kDefaultBlock;
+        // Default row tile: 256 nodes for binary32 storage when they divide
+        // the rows (the row step is memory bound there and longer tiles read
+        // a little faster), else 128.
+        h->block = o.block_x > 0 ? static_cast<uint32_t>(o.block_x)
+                   : (o.storage == ORR_STORAGE_F32 && config->nx % 256 == 0) ? 256u
+                                                                              : kDefaultBlock;
         h->ops = &ops_for(o.storage);
         h->sbytes = storage_bytes(o.storage);
         h->abytes = arithmetic_bytes(o.storage);
