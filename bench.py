@@ -104,6 +104,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_reference_mlups(workload, seconds: float, threads: int | None = None, use_reference=True):
     """Times a CPU solver of the path on the host cores on a bounded sample of
     the workload: the reference's own CpuLbm3D when built (oracle/_ref), else
@@ -126,11 +139,12 @@ def cpu_reference_mlups(workload, seconds: float, threads: int | None = None, us
         solver.step(1)
         steps += 1
         elapsed = time.perf_counter() - t0
-        if elapsed >= seconds or steps >= 1000:
+        if elapsed >= seconds or steps >= 2000:
             break
     mlups = steps * workload.cells / elapsed / 1e6
     sample = (f"{steps} steps of the full {workload.config.nx}x{workload.config.ny}x{workload.config.nz} "
-              f"lattice after 1 warm-up step, {elapsed:.1f} s wall, {threads} threads")
+              f"lattice after 1 warm-up step, {elapsed:.1f} s wall, {threads} threads of "
+              f"{os.cpu_count()} ({cpu_model()})")
     solver.close()
     return mlups, threads, kind, sample, steps
 
@@ -165,7 +179,8 @@ def run_reference_arm(args, rank: int):
         "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "storage": "f64 (reference CPU solver)", "seed": 1},
-        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
+                         "cpu_model": cpu_model(), "nproc": os.cpu_count()},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -196,6 +211,44 @@ def voxelize_cpu_baseline(forms, arrays, planes: int = 48) -> dict:
             "cpu_slab_matches_device": bool(np.array_equal(solid, arrays["solid"][lo:hi]) and
                                             np.array_equal(dist, arrays["distance"][lo:hi]) and
                                             np.array_equal(inb, arrays["in_band"][lo:hi]))}
+
+
+def default_forms(args) -> dict:
+    """Reduced batched and served forms for the default line (binary16
+    storage against the plain binary32 form), small enough to finish in about
+    a minute and a half together: the first 16 lattices of the 64-lattice NACA
+    batch for 1000 steps, and the first 16 requests of the sphere-cone stream
+    with a 10,000-step cap, the Cd of every converged served solve checked
+    against the binary64 form of the same solve at the same step."""
+    from orrery_b200 import forms
+    out = {}
+    t0 = time.perf_counter()
+    b = forms.run_batched(storage="f16", count=16, steps=1000, plain=True, warmup=4)
+    out["batched"] = {
+        "workload": "naca_batch(seed=4)[:16]: 16 NACA-wing lattices (nx 96..256, ny, nz 96..128), 1000 steps, "
+                    "force every 10 steps",
+        "storage": "f16", "nodes": b["nodes"], "solves_per_s": b["solves_per_s"], "mlups": b["mlups"],
+        "plain_f32_solves_per_s": b["plain"]["solves_per_s"], "plain_f32_mlups": b["plain"]["mlups"],
+        "speedup_vs_plain": b["speedup_vs_plain"], "schedule": b["schedule"], "gpu_launches": b["gpu_launches"],
+        "finite": b["finite"], "seconds": time.perf_counter() - t0}
+    t0 = time.perf_counter()
+    r = forms.run_serve(storage="f16", count=16, max_steps=10000, plain=True, oracle_check="converged")
+    sv, pl, ce = r["served"], r["plain"], r["cd_rel_error_vs_f64"]
+    states = {}
+    for st in sv["state"]:
+        states[st] = states.get(st, 0) + 1
+    out["served"] = {
+        "workload": "sphere_cone_requests(seed=5)[:16] at 20 req/s: 64^3..320x160x160, Re 100..2000, window 500, "
+                    "|dCd| < 1e-4, cap 10,000 steps, 150 GB budget, 64 slots",
+        "storage": "f16", "solves_per_s": sv["solves_per_s"], "latency_p50_s": sv["latency_p50_s"],
+        "latency_p99_s": sv["latency_p99_s"], "states": states, "mlups": sv["mlups"],
+        "plain_f32_solves_per_s": pl["solves_per_s"], "plain_f32_latency_p99_s": pl["latency_p99_s"],
+        "speedup_vs_plain": r["speedup_vs_plain"],
+        "cd_rel_error_vs_f64": {"converged_checked": ce["n"], "max": ce["max"], "per_request": ce["per_request"],
+                                "requests": ce["requests"], "steps": ce["steps"],
+                                "within_0.5pct": all(e <= 5e-3 for e in ce["per_request"])},
+        "seconds": time.perf_counter() - t0}
+    return out
 
 
 def run_form(args, rank: int) -> int:
@@ -268,6 +321,8 @@ def main(argv=None) -> int:
                     help="serve form: parallel graph branches of per-lattice launches (0: one launch / stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1000)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain form: leave out the reduced batched and served forms of the default line")
     ap.add_argument("--e2e-repeats", type=int, default=3,
                     help="whole solves timed end to end; the line reports their median")
     args = ap.parse_args(argv)
@@ -302,7 +357,8 @@ def main(argv=None) -> int:
     kinfo = solver.kernel_info()
     solver.initialize(w.rho, w.ux, w.uy, w.uz)
     stream = torch.cuda.ExternalStream(solver.stream(), device=torch.device("cuda", local_rank))
-    solver.step(max(args.warmup, 3))
+    warmup = max(args.warmup, 3)
+    solver.step(warmup)
     torch.cuda.synchronize()
 
     def barrier():
@@ -328,10 +384,6 @@ def main(argv=None) -> int:
     ms_per_step = ms / args.steps
     mlups = whole_job_rate(w.cells, args.steps, ms, world)
 
-    # Force sanity and the coefficient at the end of the timed run.
-    f = solver.force()
-    coeff = W.coefficients3d(f.force, f.moment, w.config.inlet_ux, w.reference_area, w.reference_length)
-
     # Roofline of the step (bulk + boundary kernels): algorithmic bytes per
     # step over the device time of a step.
     bytes_per_step = BYTES_PER_UPDATE[args.storage] * w.cells
@@ -347,7 +399,7 @@ def main(argv=None) -> int:
     if args.e2e_steps >= 10 and args.e2e_repeats >= 1:
         import numpy as np
         samples = args.e2e_steps // 10
-        times, phases = [], []
+        times, phases, fx = [], [], []
         for _ in range(args.e2e_repeats):
             barrier()
             t0 = time.perf_counter()
@@ -356,10 +408,12 @@ def main(argv=None) -> int:
             t1 = time.perf_counter()
             s2.initialize(w.rho, w.ux, w.uy, w.uz)
             t2 = time.perf_counter()
+            fx_run = []
             for _ in range(samples):
                 s2.step(10)
-                s2.force()
+                fx_run.append(s2.force().force[0])
             t3 = time.perf_counter()
+            fx = fx_run
             fields = s2.macroscopic()
             torch.cuda.synchronize()
             t4 = time.perf_counter()
@@ -380,17 +434,30 @@ def main(argv=None) -> int:
                "phases_ms": {key: round(v, 2) for key, v in mid.items()},
                "note": f"whole solves per rank, median of {len(times)}: create (plan + upload), initialise from "
                        "host fields, steps with the force read back every 10 steps, moments read back"}
+        # The drag coefficient the reference adapter reports: the mean of the
+        # last 50 force samples (every 10 steps) over 1/2 rho U^2 A.
+        window = fx[-50:]
+        u = w.config.inlet_ux
+        e2e["cd_window_mean"] = float(np.mean(window)) / (0.5 * u * u * w.reference_area)
+        e2e["cd_window"] = (f"mean Fx of the last {len(window)} force samples of the last solve "
+                            f"(steps {k - 10 * (len(window) - 1)}..{k}) over 1/2 rho U^2 A, A = pi D^2 / 4; "
+                            "impulsive start from noisy uniform flow, so not yet the steady drag")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        secs = float(os.environ.get("ORR_CPU_BASELINE_SECONDS", "15"))
+        secs = float(os.environ.get("ORR_CPU_BASELINE_SECONDS", "30"))
         mlups_cpu, cores, kind, sample, _ = cpu_reference_mlups(w, secs)
-        cpu = {"value": mlups_cpu, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample}
+        cpu = {"value": mlups_cpu, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
+               "cpu_model": cpu_model(), "nproc": os.cpu_count()}
+
+    forms_out = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms_out = default_forms(args)
 
     if rank == 0:
         line = {
             "metric": "D3Q19 MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+            "steps": args.steps, "warmup": warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f32": "f32", "f16": "f16-storage/f32-math", "bf16": "bf16-storage/f32-math",
                       "f64": "f64"}[args.storage],
@@ -407,8 +474,9 @@ def main(argv=None) -> int:
             "clocks": clock_info,
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "cd": coeff["cd"], "cl": coeff["cl"],
         }
+        if forms_out is not None:
+            line["forms"] = forms_out
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -235,6 +235,15 @@ ORR_API orr_status orr_lbm3d_node_counts(const orr_lbm3d* solver, uint64_t* flui
 ORR_API orr_status orr_lbm3d_stream(const orr_lbm3d* solver, void** stream);
 /* Kernels launched by this handle since creation (step, force, moments, ...). */
 ORR_API orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches);
+/* Test hook of the staged step's bounded waits (no counterpart in the
+ * reference, whose GL kernels do not wait on copies): the next staged launch's
+ * CTA `cta` withholds the copies of its first span, so its consumers' wait
+ * runs out (about 1.3 s), the launch ends early and the next read-back returns
+ * ORR_ERR_TIMEOUT, as after a copy that never lands; the populations are then
+ * invalid until orr_lbm3d_initialize, which also cancels a request no launch
+ * has taken.  Refused (ORR_ERR_INVALID) unless the solver runs the staged step
+ * and that CTA has a staged span. */
+ORR_API orr_status orr_lbm3d_request_stall(orr_lbm3d* solver, uint32_t cta);
 
 /* ---- D3Q19 batches ------------------------------------------------------ */
 

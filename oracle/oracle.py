@@ -34,13 +34,25 @@ _restated = None
 _reference = None
 
 
+def reference_tree(reference: str | None = None) -> str | None:
+    """The reference source tree: `reference`, else $ORR_REFERENCE, else a
+    checkout named ``reference`` beside this repository; None when none of
+    them holds the LBM sources."""
+    candidates = [reference, os.environ.get("ORR_REFERENCE"),
+                  os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for ref in candidates:
+        if ref and os.path.isdir(os.path.join(ref, "src", "aero", "lbm3d")):
+            return os.path.abspath(ref)
+    return None
+
+
 def build(reference: str | None = None) -> None:
     """Builds the restatement, and the reference libraries when the reference
-    tree exists (the adapter harness after the product library)."""
+    tree is found (the adapter harness after the product library)."""
     env = dict(os.environ)
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True, env=env)
-    ref = reference or os.environ.get("ORR_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src", "aero", "lbm3d")):
+    ref = reference_tree(reference)
+    if ref is not None:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True, env=env)
         subprocess.run(["make", "-s", "-C", HERE, "adapter", f"REF={ref}"], check=True, env=env)
 

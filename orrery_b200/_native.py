@@ -51,6 +51,7 @@ SIGNATURES = {
     "orr_lbm3d_node_counts": (_st, [_vp, _u64p, _u64p]),
     "orr_lbm3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
     "orr_lbm3d_launch_count": (_st, [_vp, _u64p]),
+    "orr_lbm3d_request_stall": (_st, [_vp, ctypes.c_uint32]),
     "orr_lbm3d_kernel_info": (_st, [_vp, ctypes.POINTER(abi.CKernelInfo)]),
     "orr_lbm3d_force_static": (_st, [ctypes.POINTER(abi.CForceLinks), _dp]),
     "orr_lbm2d_validate": (_st, [_c2, _u8p, _opt, ctypes.c_char_p, ctypes.c_size_t]),

@@ -80,8 +80,9 @@ orr_status orr_batch3d_create(int32_t device, orr_batch3d** out) {
         check(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
         check(cudaEventCreate(&b->t0), "batch event");
         check(cudaEventCreate(&b->t1), "batch event");
-        check(cudaMalloc(&b->status, sizeof(uint32_t)), "batch status");
-        check(cudaMemsetAsync(b->status, 0, sizeof(uint32_t), b->stream), "batch status");
+        // The status word and the staged step's stall-request word.
+        check(cudaMalloc(&b->status, 2 * sizeof(uint32_t)), "batch status");
+        check(cudaMemsetAsync(b->status, 0, 2 * sizeof(uint32_t), b->stream), "batch status");
         check(cudaStreamSynchronize(b->stream), "batch create");
         *out = b.release();
         return ORR_OK;

@@ -268,7 +268,10 @@ struct orr_server {
         bool finite = true;
         for (int v = 0; v < 6; ++v) finite = finite && std::isfinite(sums[v]);
         if (!finite) {
-            finish(a, ORR_SOLVE_FAILED, 0, 0, 0, 0, nullptr, "serve: the force is not finite (the solve diverged)");
+            // The reference adapter's warning for the same event
+            // (lbm_aero_solver3d.cpp:585-588).
+            finish(a, ORR_SOLVE_FAILED, 0, 0, 0, 0, nullptr,
+                   "lbm.diverged: the lattice state is no longer finite (numerical instability)");
             return true;
         }
         if (a.window_steps < q.window) {

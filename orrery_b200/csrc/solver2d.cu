@@ -90,6 +90,28 @@ struct orr_lbm2d {
         ++launches;
     }
 
+    // Captures kGraphSteps2 steps (buffer 0 -> 1 -> ... -> 0) as one graph.
+    void build_graph() {
+        cudaGraph_t captured = nullptr;
+        const uint64_t before = launches;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+        try {
+            for (uint32_t k = 0; k < kGraphSteps2; ++k) {
+                launch_step(static_cast<int>(k & 1u));
+            }
+        } catch (...) {
+            cudaStreamEndCapture(stream, &captured);
+            if (captured) cudaGraphDestroy(captured);
+            launches = before;
+            throw;
+        }
+        launches = before;
+        check(cudaStreamEndCapture(stream, &captured), "graph capture");
+        const cudaError_t e = cudaGraphInstantiate(&graph, captured, 0);
+        cudaGraphDestroy(captured);
+        check(e, "graph instantiate");
+    }
+
     void run(uint64_t count) {
         uint64_t left = count;
         if (left >= kGraphSteps2) {
@@ -99,24 +121,7 @@ struct orr_lbm2d {
                 --left;
             }
             if (!graph) {
-                cudaGraph_t captured = nullptr;
-                const uint64_t before = launches;
-                check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-                try {
-                    for (uint32_t k = 0; k < kGraphSteps2; ++k) {
-                        launch_step(static_cast<int>(k & 1u));
-                    }
-                } catch (...) {
-                    cudaStreamEndCapture(stream, &captured);
-                    if (captured) cudaGraphDestroy(captured);
-                    launches = before;
-                    throw;
-                }
-                launches = before;
-                check(cudaStreamEndCapture(stream, &captured), "graph capture");
-                const cudaError_t e = cudaGraphInstantiate(&graph, captured, 0);
-                cudaGraphDestroy(captured);
-                check(e, "graph instantiate");
+                build_graph();
             }
             while (left >= kGraphSteps2) {
                 check(cudaGraphLaunch(graph, stream), "graph launch");
@@ -293,6 +298,8 @@ orr_status orr_lbm2d_create(const orr_lbm2d_config* config, const uint8_t* solid
                   "link upload");
         }
         initialize2(h.get(), nullptr, nullptr, nullptr);
+        // The step graph is captured here, not inside a later step() call.
+        h->build_graph();
         h->plan.cls.clear();
         h->plan.cls.shrink_to_fit();
         *out = h.release();

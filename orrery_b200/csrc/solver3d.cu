@@ -100,7 +100,8 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
                           h->stream),
           "population copy");
     check(h->ops->history(h->g, h->f[0], h->hist, h->stream), "history kernel");
-    check(cudaMemsetAsync(h->status(), 0, sizeof(uint32_t), h->stream), "status reset");
+    // The status word and the stall-request word after it.
+    check(cudaMemsetAsync(h->status(), 0, 2 * sizeof(uint32_t), h->stream), "status reset");
     ++h->epoch;
     h->launches += 2;
     h->cur = 0;
@@ -418,6 +419,10 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             h->row_npt = 2;
         }
         initialize_state(h.get(), nullptr, nullptr, nullptr, nullptr);
+        // Capture the step graph now, so that no step() call, the first
+        // included, does host capture or instantiation work between its
+        // launches.
+        h->build_graph();
         check(cudaStreamSynchronize(s), "create");
         // The per-node tables are on the device now; keep the links.
         h->plan.cls.clear();
@@ -718,6 +723,25 @@ orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches) {
     }
     *launches = solver->launches;
     return ORR_OK;
+}
+
+orr_status orr_lbm3d_request_stall(orr_lbm3d* solver, uint32_t cta) {
+    return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
+        orr_lbm3d* h = handle_of(solver);
+        if (!h->persistent) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d: a stall request needs the staged step"};
+        }
+        const uint64_t ctas = std::min<uint64_t>(h->shape.grid, h->items.staged);
+        if (cta >= ctas) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d: the stall request names a CTA without staged spans"};
+        }
+        uint32_t* word = reinterpret_cast<uint32_t*>(h->host_small + 31);
+        *word = cta + 1u;
+        check(cudaMemcpyAsync(h->status() + 1, word, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream),
+              "stall request");
+        check(cudaStreamSynchronize(h->stream), "stall request");
+        return ORR_OK;
+    });
 }
 
 } // extern "C"

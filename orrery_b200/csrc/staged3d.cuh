@@ -41,6 +41,11 @@
 // sets kStatusWaitTimeout in the status word and the CTA's abort word, every
 // warp leaves its loop, and the CTA waits (bounded again) for the copies it
 // still has in flight before it returns.
+//
+// The word after the status word is the stall request that tests of this
+// path set (0 when none): a CTA whose index + 1 it holds, and that has a
+// staged span, clears it and withholds the copies of its first span, so that
+// its consumers' bounded wait runs out exactly as when a copy never lands.
 #pragma once
 
 #include <cstdint>
@@ -310,6 +315,13 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
 
     if (warp == kConsumerWarps) {
         // ---- producer warp
+        // A stall request naming this CTA is claimed by one launch only.
+        uint32_t claim = 0u;
+        if (status != nullptr && lane == 0 && count > 0u &&
+            *reinterpret_cast<volatile uint32_t*>(status + 1) == blockIdx.x + 1u) {
+            claim = atomicCAS(status + 1, blockIdx.x + 1u, 0u) == blockIdx.x + 1u ? 1u : 0u;
+        }
+        const bool withhold = __shfl_sync(0xffffffffu, claim, 0) != 0u;
         uint32_t s = 0, phase = 0;
         for (uint32_t j = 0; j < count; ++j) {
             if (j >= stages) {
@@ -334,12 +346,16 @@ __global__ void __launch_bounds__(kStagedThreads<B>, kStagedMinBlocks<S, B>)
             const uint64_t c0 = static_cast<uint64_t>(z) * L.g.plane + static_cast<uint64_t>(nx) * y0 + x0;
             const uint32_t bar = smem_u32(full + s);
             unsigned char* stage = ring + s * STAGE;
-            if (lane == 0) {
+            if (withhold && j == 0u) {
+                // The stall request: this stage is never armed or filled.
+            } else if (lane == 0) {
                 info[s] = make_uint4(l, x0, y0, z);
                 mbar_expect_tx(bar, STAGE);
             }
             __syncwarp();
-            if (lane < static_cast<uint32_t>(d3::Q)) {
+            if (withhold && j == 0u) {
+                // no copies
+            } else if (lane < static_cast<uint32_t>(d3::Q)) {
                 int cx, cy, cz;
                 c_rt(static_cast<int>(lane), cx, cy, cz);
                 const S* src = static_cast<const S*>(L.f[L.parity ^ flip]);

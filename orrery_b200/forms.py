@@ -15,8 +15,8 @@ serve     the sphere-cone request stream of ``workloads.sphere_cone_requests``
           every solve runs until its window-mean Cd settles or its step cap.
           Reported: solves/s, p50 / p99 latency from arrival to result, and
           the plain form (binary32, one slot: the same requests one after
-          another), optionally the Cd error of the first requests against the
-          binary64 form of the same solves.
+          another), optionally the Cd error of the first requests (or of every
+          converged solve) against the binary64 form of the same solves.
 
 Both return plain dictionaries (bench.py prints them as its JSON line).
 """
@@ -140,13 +140,13 @@ def _serve_once(requests, workloads, storage, max_active, memory_budget, window,
             "peak_device_gb": stats["peak_device_bytes"] / 1e9,
             "mlups": stats["lattice_updates"] / max(stats["busy_seconds"], 1e-9) / 1e6,
             "steps": [r["steps"] for r in results], "cd": [r["cd"] for r in results],
-            "worker_message": stats["message"]}
+            "state": [r["state"] for r in results], "worker_message": stats["message"]}
 
 
 def run_serve(storage: str = "f16", count: int = 48, rate: float = 20.0, seed: int = 5,
               window: int = 500, tolerance: float = 1e-4, max_steps: int = 20000,
               memory_budget: float = 150e9, max_active: int = 64, chunk_steps: int = 100,
-              plain: bool = True, oracle_check: int = 0, kernel: str = "auto", branches: int = 0) -> dict:
+              plain: bool = True, oracle_check=0, kernel: str = "auto", branches: int = 0) -> dict:
     requests = W.sphere_cone_requests(seed=seed, count=count, rate=rate)
     t0 = time.perf_counter()
     workloads = []
@@ -170,22 +170,38 @@ def run_serve(storage: str = "f16", count: int = 48, rate: float = 20.0, seed: i
         out["plain"] = _serve_once(requests, workloads, "f32", 1, memory_budget, window, tolerance,
                                    max_steps, chunk_steps, "rows", 0)
         out["speedup_vs_plain"] = out["served"]["solves_per_s"] / max(out["plain"]["solves_per_s"], 1e-12)
-    if oracle_check > 0:
-        # Cd of the first requests against the binary64 form of the same
-        # solves at the same step: each binary64 solve is capped at the step
-        # its served solve ended on, with a tolerance that never stops it, so
-        # both window means cover the same steps.
-        n = min(oracle_check, count)
-        caps = out["served"]["steps"][:n]
-        ref = _serve_once(requests[:n], workloads[:n], "f64", max_active, memory_budget, window, 1e-300,
-                          caps, chunk_steps)
-        errs = []
-        for k in range(n):
-            cd, cd64 = out["served"]["cd"][k], ref["cd"][k]
-            errs.append(abs(cd - cd64) / abs(cd64) if cd64 else math.inf)
-        out["cd_rel_error_vs_f64"] = {"max": max(errs), "mean": float(np.mean(errs)), "n": n,
-                                      "per_request": errs, "steps": caps, "steps_f64": ref["steps"]}
+    if oracle_check == "converged" or (isinstance(oracle_check, int) and oracle_check > 0):
+        # Cd against the binary64 form of the same solves at the same step:
+        # each binary64 solve is capped at the step its served solve ended
+        # on, with a tolerance that never stops it, so both window means
+        # cover the same steps.  "converged": every solve that converged;
+        # n > 0: the first n requests.
+        if oracle_check == "converged":
+            pick = [k for k, st in enumerate(out["served"]["state"]) if st == "converged"]
+        else:
+            pick = list(range(min(oracle_check, count)))
+        out["cd_rel_error_vs_f64"] = oracle_errors(out["served"], [requests[k] for k in pick],
+                                                   [workloads[k] for k in pick], pick, max_active,
+                                                   memory_budget, window, chunk_steps)
     return out
+
+
+def oracle_errors(served: dict, requests, workloads, pick, max_active, memory_budget, window,
+                  chunk_steps) -> dict:
+    """Relative Cd error of the served solves `pick` against binary64 solves
+    of the same requests capped at the same steps."""
+    if not pick:
+        return {"n": 0, "max": None, "mean": None, "per_request": [], "requests": [], "steps": [],
+                "steps_f64": [], "cd_f64": []}
+    caps = [served["steps"][k] for k in pick]
+    ref = _serve_once(requests, workloads, "f64", max_active, memory_budget, window, 1e-300, caps,
+                      chunk_steps)
+    errs = []
+    for j, k in enumerate(pick):
+        cd, cd64 = served["cd"][k], ref["cd"][j]
+        errs.append(abs(cd - cd64) / abs(cd64) if cd64 else math.inf)
+    return {"n": len(pick), "max": max(errs), "mean": float(np.mean(errs)), "requests": pick,
+            "per_request": errs, "steps": caps, "steps_f64": ref["steps"], "cd_f64": ref["cd"]}
 
 
 def voxelize_workload():

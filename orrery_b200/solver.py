@@ -272,6 +272,12 @@ class CudaLbm3D:
         self._check(self._lib.orr_lbm3d_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    def request_stall(self, cta: int = 0) -> None:
+        """Test hook of the staged step's bounded waits: the next staged
+        launch's CTA `cta` withholds its first span's copies, so the next
+        read-back raises the timeout error until initialize()."""
+        self._check(self._lib.orr_lbm3d_request_stall(self._h, int(cta)))
+
     def kernel_info(self) -> dict:
         """The step kernel this solver runs and its launch shape."""
         k = abi.CKernelInfo()

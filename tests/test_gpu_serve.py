@@ -100,13 +100,23 @@ def test_memory_budget_admission():
     assert res[0]["state"] == "failed" and "budget" in res[0]["message"]
 
 
-def test_fp16_served_close_to_fp32():
+def test_served_16bit_and_binary32_within_bar_of_binary64():
+    """Cd of a converged served solve in binary16 and binary32 storage against
+    the binary64 form of the same request capped at the same step (so both
+    window means cover the same steps): within 0.5% relative, always
+    asserted."""
     w = small(41)
-    r32, _ = serve([w], storage="f32")
-    r16, _ = serve([w], storage="f16")
-    assert r16[0]["state"] != "failed"
-    if r16[0]["steps"] == r32[0]["steps"]:
-        assert abs(r16[0]["cd"] - r32[0]["cd"]) / abs(r32[0]["cd"]) < 5e-3
+    for storage in ("f16", "f32"):
+        r, _ = serve([w], storage=storage)
+        r = r[0]
+        assert r["state"] in ("converged", "capped"), (storage, r["state"], r["message"])
+        with Server(storage="f64", chunk_steps=CHUNK, sample_every=10) as srv:
+            i = srv.submit(w, window=WINDOW, tolerance=1e-300, max_steps=r["steps"])
+            srv.drain(timeout=600)
+            r64 = srv.poll(i)
+        assert r64["steps"] == r["steps"]
+        err = abs(r["cd"] - r64["cd"]) / abs(r64["cd"])
+        assert err <= 5e-3, (storage, r["cd"], r64["cd"], err)
 
 
 def test_refusals():
