@@ -216,9 +216,9 @@ def voxelize_cpu_baseline(forms, arrays, planes: int = 48) -> dict:
 def default_forms(args) -> dict:
     """Reduced batched and served forms for the default line (binary16
     storage against the plain binary32 form), small enough to finish in about
-    a minute and a half together: the first 16 lattices of the 64-lattice NACA
+    two minutes together: the first 16 lattices of the 64-lattice NACA
     batch for 1000 steps, and the first 16 requests of the sphere-cone stream
-    with a 10,000-step cap, the Cd of every converged served solve checked
+    with a 20,000-step cap, the Cd of every converged served solve checked
     against the binary64 form of the same solve at the same step."""
     from orrery_b200 import forms
     out = {}
@@ -232,14 +232,14 @@ def default_forms(args) -> dict:
         "speedup_vs_plain": b["speedup_vs_plain"], "schedule": b["schedule"], "gpu_launches": b["gpu_launches"],
         "finite": b["finite"], "seconds": time.perf_counter() - t0}
     t0 = time.perf_counter()
-    r = forms.run_serve(storage="f16", count=16, max_steps=10000, plain=True, oracle_check="converged")
+    r = forms.run_serve(storage="f16", count=16, max_steps=20000, plain=True, oracle_check="converged")
     sv, pl, ce = r["served"], r["plain"], r["cd_rel_error_vs_f64"]
     states = {}
     for st in sv["state"]:
         states[st] = states.get(st, 0) + 1
     out["served"] = {
         "workload": "sphere_cone_requests(seed=5)[:16] at 20 req/s: 64^3..320x160x160, Re 100..2000, window 500, "
-                    "|dCd| < 1e-4, cap 10,000 steps, 150 GB budget, 64 slots",
+                    "|dCd| < 1e-4, cap 20,000 steps, 150 GB budget, 64 slots",
         "storage": "f16", "solves_per_s": sv["solves_per_s"], "latency_p50_s": sv["latency_p50_s"],
         "latency_p99_s": sv["latency_p99_s"], "states": states, "mlups": sv["mlups"],
         "plain_f32_solves_per_s": pl["solves_per_s"], "plain_f32_latency_p99_s": pl["latency_p99_s"],

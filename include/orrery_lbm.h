@@ -360,20 +360,39 @@ typedef struct orr_solve_request {
     int32_t allow_high_mach;
     uint32_t sample_every;            /* 0 or the server's */
     uint32_t window;                  /* steps per window, a multiple of chunk_steps */
-    uint32_t reserved;
-    double tolerance;                 /* on |delta Cd| between consecutive window means */
-    uint64_t max_steps;               /* step cap (0: none) */
+    uint32_t mode;                    /* ORR_RUN_UNTIL_SETTLED or ORR_RUN_FIXED_STEPS */
+    double tolerance;                 /* on |delta Cd| between consecutive window means (until settled) */
+    uint64_t max_steps;               /* step cap (0: none); the run's length when fixed */
     double reference_area;            /* Cd = Fx / (1/2 rho U^2 A) */
     double reference_length;          /* Cm = Mz / (1/2 rho U^2 A L) */
     double moment_centre[3];
+    /* Gradual start (LbmAeroSolver3D::step, src/aero/lbm3d/lbm_aero_solver3d.cpp:
+     * 398-412): when positive the solve starts at rest (rho 1, u 0, initial
+     * fields not allowed) and its inlet velocity is the configured one times
+     * (1 - cos(pi s / ramp_steps)) / 2 while s < ramp_steps, where s is the
+     * first step of each sampling interval (held over the interval), and the
+     * configured one after.  0: no ramp. */
+    double ramp_steps;
 } orr_solve_request;
+
+/* Run modes of a served solve.  Until settled: windows of `window` steps
+ * until |delta Cd| < tolerance or max_steps.  Fixed steps: exactly max_steps
+ * steps (max_steps and max_steps - window multiples of chunk_steps), the
+ * result the means over the last `window` steps, as the reference adapter's
+ * moving average over a run of fixed duration (lbm_aero_solver3d.cpp:464-481);
+ * the tolerance is not used. */
+enum {
+    ORR_RUN_UNTIL_SETTLED = 0,
+    ORR_RUN_FIXED_STEPS = 1
+};
 
 enum {
     ORR_SOLVE_QUEUED = 0,
     ORR_SOLVE_RUNNING = 1,
     ORR_SOLVE_CONVERGED = 2,
     ORR_SOLVE_CAPPED = 3,
-    ORR_SOLVE_FAILED = 4
+    ORR_SOLVE_FAILED = 4,
+    ORR_SOLVE_COMPLETED = 5           /* a fixed-steps solve ran its steps */
 };
 
 typedef struct orr_solve_result {

@@ -623,3 +623,96 @@ def reference_adapter_run(vertices, triangles, backend: str = "cpu", storage: in
         result["cp"] = cp[:nc.value]
         result["velocity"] = vel[:nv_.value].reshape(-1, 3)
     return result
+
+
+def _adapter_lib():
+    if ADAPTER_SO not in _adapter:
+        lib = ctypes.CDLL(ADAPTER_SO)
+        lib.ref_adapter_run.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_int,
+                                        ctypes.c_int, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        _adapter[ADAPTER_SO] = lib
+    lib = _adapter[ADAPTER_SO]
+    lib.ref_cd_table.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_double, _dp,
+                                 ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _dp, ctypes.c_char_p,
+                                 ctypes.c_size_t]
+    lib.ref_cd_point_problem.argtypes = [_dp, ctypes.c_uint64, _u32p, ctypes.c_uint64, _dp, ctypes.c_double,
+                                         ctypes.c_double, ctypes.POINTER(abi.CLbm3DConfig), _u8p, _dp, _dp,
+                                         ctypes.c_char_p, ctypes.c_size_t]
+    return lib
+
+
+_TABLE_OUT = ["mach", "cd", "solver_steps", "converged", "within_envelope", "seconds", "table_cd", "table_seconds"]
+
+
+def reference_cd_table(vertices, triangles, mach, temperature: float = 288.15, max_steps: int = 100000,
+                       storage: int = 0, **params) -> list[dict]:
+    """The reference's atmo::sample_cd_table (src/atmo/cd_sampling.cpp:98-120)
+    with the lattice Boltzmann solver forced and a factory of the reference's
+    LbmAeroSolver3D on the CUDA solver (ORR_STORAGE_* `storage`): one adapter
+    solve per Mach number, one after another.  `params` as for
+    reference_adapter_run (the speed is Mach times the speed of sound of
+    `temperature`).  One dict per point."""
+    lib = _adapter_lib()
+    p = dict(ADAPTER_DEFAULTS)
+    p.update(params)
+    arr = np.array([float(p[k]) for k in _ADAPTER_ORDER])
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    m = np.ascontiguousarray(mach, np.float64)
+    out = np.zeros(len(m) * len(_TABLE_OUT))
+    msg = ctypes.create_string_buffer(2048)
+    if lib.ref_cd_table(_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(arr, _dp), float(temperature),
+                        _ptr(m, _dp), len(m), int(max_steps), int(storage), _ptr(out, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return [dict(zip(_TABLE_OUT, row.tolist())) for row in out.reshape(len(m), len(_TABLE_OUT))]
+
+
+_PROBLEM_META = ["nx", "ny", "nz", "total_steps", "window_samples", "ramp_steps", "dx", "area_lattice",
+                 "length_lattice", "lattice_velocity", "sample_every", "has_distance"]
+
+
+def reference_cd_point_problem(vertices, triangles, mach: float, temperature: float = 288.15, **params) -> dict:
+    """The lattice problem the reference adapter's setup builds for one Mach
+    point of reference_cd_table: "config" (abi.CLbm3DConfig), "solid",
+    "distance" (or None), and the run lengths and lattice reference values of
+    _PROBLEM_META."""
+    lib = _adapter_lib()
+    p = dict(ADAPTER_DEFAULTS)
+    p.update(params)
+    arr = np.array([float(p[k]) for k in _ADAPTER_ORDER])
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    cfg = abi.CLbm3DConfig()
+    meta = np.zeros(len(_PROBLEM_META))
+    msg = ctypes.create_string_buffer(2048)
+    args = (_ptr(v, _dp), len(v), _ptr(t, _u32p), len(t), _ptr(arr, _dp), float(temperature), float(mach),
+            ctypes.byref(cfg))
+    if lib.ref_cd_point_problem(*args, None, None, _ptr(meta, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    cells = int(meta[0]) * int(meta[1]) * int(meta[2])
+    solid = np.zeros(cells, np.uint8)
+    dist = np.zeros(cells) if meta[11] else None
+    if lib.ref_cd_point_problem(*args, _ptr(solid, _u8p), _ptr(dist, _dp), _ptr(meta, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    out = dict(zip(_PROBLEM_META, meta.tolist()))
+    out.update({"config": cfg, "solid": solid, "distance": dist})
+    return out
+
+
+def reference_cd_lookup(samples, query, area: float = 1.0):
+    """The reference's AeroCoefficientTable::create + lookup
+    (src/atmo/aero_table.cpp:47-83): (cd, clamped) at every query Mach, or
+    ReferenceError_ with the refusal's text."""
+    lib = _adapter_lib()
+    lib.ref_cd_table_lookup.argtypes = [_dp, _dp, ctypes.c_uint64, ctypes.c_double, _dp, ctypes.c_uint64, _dp,
+                                        _u8p, ctypes.c_char_p, ctypes.c_size_t]
+    m = np.ascontiguousarray([s[0] for s in samples], np.float64)
+    c = np.ascontiguousarray([s[1] for s in samples], np.float64)
+    q = np.ascontiguousarray(query, np.float64)
+    out = np.zeros(max(len(q), 1))
+    clamped = np.zeros(max(len(q), 1), np.uint8)
+    msg = ctypes.create_string_buffer(1024)
+    if lib.ref_cd_table_lookup(_ptr(m, _dp), _ptr(c, _dp), len(m), float(area), _ptr(q, _dp),
+                               len(q), _ptr(out, _dp), _ptr(clamped, _u8p), msg, 1024) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return out[:len(q)], clamped[:len(q)].astype(bool)

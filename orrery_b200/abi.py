@@ -113,14 +113,16 @@ class CSolveRequest(ctypes.Structure):
                 ("distance", ctypes.POINTER(ctypes.c_double)), ("rho", ctypes.POINTER(ctypes.c_double)),
                 ("ux", ctypes.POINTER(ctypes.c_double)), ("uy", ctypes.POINTER(ctypes.c_double)),
                 ("uz", ctypes.POINTER(ctypes.c_double)), ("allow_high_mach", ctypes.c_int32),
-                ("sample_every", ctypes.c_uint32), ("window", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("sample_every", ctypes.c_uint32), ("window", ctypes.c_uint32), ("mode", ctypes.c_uint32),
                 ("tolerance", ctypes.c_double), ("max_steps", ctypes.c_uint64),
                 ("reference_area", ctypes.c_double), ("reference_length", ctypes.c_double),
-                ("moment_centre", ctypes.c_double * 3)]
+                ("moment_centre", ctypes.c_double * 3), ("ramp_steps", ctypes.c_double)]
 
 
+ORR_RUN_UNTIL_SETTLED, ORR_RUN_FIXED_STEPS = 0, 1
 ORR_SOLVE_QUEUED, ORR_SOLVE_RUNNING, ORR_SOLVE_CONVERGED, ORR_SOLVE_CAPPED, ORR_SOLVE_FAILED = 0, 1, 2, 3, 4
-SOLVE_STATES = {0: "queued", 1: "running", 2: "converged", 3: "capped", 4: "failed"}
+ORR_SOLVE_COMPLETED = 5
+SOLVE_STATES = {0: "queued", 1: "running", 2: "converged", 3: "capped", 4: "failed", 5: "completed"}
 
 
 class CSolveResult(ctypes.Structure):

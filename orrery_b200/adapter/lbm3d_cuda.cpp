@@ -49,6 +49,14 @@ orr_lbm3d_config config_of(const Lbm3DConfig& c) {
     return o;
 }
 
+} // namespace
+
+orr_lbm3d_config c_config(const Lbm3DConfig& config) {
+    return config_of(config);
+}
+
+namespace {
+
 class CudaLbm3D final : public Lbm3DSolver {
 public:
     CudaLbm3D(orr_lbm3d* handle, const Lbm3DConfig& config, SolidMask3D mask)

@@ -22,4 +22,7 @@ namespace orrery::aero::lbm {
 make_cuda_solver(const Lbm3DConfig& config, SolidMask3D mask, std::int32_t storage = ORR_STORAGE_F32,
                  std::int32_t device = 0);
 
+// The C ABI's configuration record of a reference configuration.
+[[nodiscard]] orr_lbm3d_config c_config(const Lbm3DConfig& config);
+
 } // namespace orrery::aero::lbm

@@ -23,7 +23,11 @@
 //              window of `window` steps differs from the previous window's
 //              by less than `tolerance` (converged), when it reaches
 //              `max_steps` (capped), or when its force stops being finite
-//              (failed).
+//              (failed); a fixed-steps solve when it has run `max_steps`
+//              steps (completed, the means over its last window).
+//   ramp       a solve with ramp_steps > 0 starts at rest and its inlet
+//              velocity follows the reference adapter's gradual start, set
+//              on the device before every sampling interval (batch3d).
 //
 // Each solve's populations and force sums are exactly those it would have
 // alone (batch members do not interact, and the force sums have a fixed
@@ -61,8 +65,10 @@ struct Request {
     std::vector<double> fields;   // rho, ux, uy, uz (4 cells) or empty
     int32_t allow_high_mach = 0;
     uint32_t window = 500;
+    uint32_t mode = ORR_RUN_UNTIL_SETTLED;
     double tolerance = 1e-4;
     uint64_t max_steps = 0;
+    double ramp_steps = 0.0;      // gradual start (0: none)
     double area = 1.0, length = 1.0;
     double centre[3] = {0.0, 0.0, 0.0};
     uint64_t estimate = 0;        // device bytes before planning
@@ -196,6 +202,23 @@ struct orr_server {
                                       q->fields.data() + 3 * n);
             if (st != ORR_OK) why = orr_lbm3d_last_error(s);
         }
+        if (st == ORR_OK && q->ramp_steps > 0.0) {
+            // Gradual start: at rest, the inlet velocity planned by the batch
+            // before every sampling interval.
+            try {
+                initialize_at_rest(s);
+                s->ramp_steps = q->ramp_steps;
+                s->ramp_u[0] = q->config.inlet_ux;
+                s->ramp_u[1] = q->config.inlet_uy;
+                s->ramp_u[2] = q->config.inlet_uz;
+            } catch (const Refusal& r) {
+                st = r.status;
+                why = r.text;
+            } catch (const CudaError& e) {
+                st = ORR_ERR_CUDA;
+                why = describe(e);
+            }
+        }
         if (st != ORR_OK) {
             if (s) orr_lbm3d_destroy(s);
             Active none;
@@ -261,10 +284,16 @@ struct orr_server {
     // Window bookkeeping after a chunk; returns true when the solve is done.
     bool update(Active& a, const double* sums, uint64_t samples, uint64_t steps) {
         const Request& q = *a.req;
+        const uint64_t chunk_first = a.steps;
         a.steps += steps;
-        a.window_steps += steps;
-        for (int v = 0; v < 6; ++v) a.window_sum[v] += sums[v];
-        a.window_samples += samples;
+        // A fixed-steps solve sums only its last window (whose first step is
+        // a chunk boundary).
+        const bool counted = q.mode != ORR_RUN_FIXED_STEPS || chunk_first >= q.max_steps - q.window;
+        if (counted) {
+            a.window_steps += steps;
+            for (int v = 0; v < 6; ++v) a.window_sum[v] += sums[v];
+            a.window_samples += samples;
+        }
         bool finite = true;
         for (int v = 0; v < 6; ++v) finite = finite && std::isfinite(sums[v]);
         if (!finite) {
@@ -273,6 +302,9 @@ struct orr_server {
             finish(a, ORR_SOLVE_FAILED, 0, 0, 0, 0, nullptr,
                    "lbm.diverged: the lattice state is no longer finite (numerical instability)");
             return true;
+        }
+        if (q.mode == ORR_RUN_FIXED_STEPS && a.steps < q.max_steps) {
+            return false;
         }
         if (a.window_steps < q.window) {
             return false;
@@ -285,6 +317,10 @@ struct orr_server {
         const double qa = 0.5 * u * u * q.area;
         const double mz = mean[5] - (q.centre[0] * mean[1] - q.centre[1] * mean[0]);
         const double cd = mean[0] / qa, cl = mean[1] / qa, cm = mz / (qa * q.length);
+        if (q.mode == ORR_RUN_FIXED_STEPS) {
+            finish(a, ORR_SOLVE_COMPLETED, cd, cl, cm, 0.0, mean, "");
+            return true;
+        }
         const double delta = a.have_previous ? std::abs(cd - a.previous_cd) : INFINITY;
         a.have_previous = true;
         a.previous_cd = cd;
@@ -483,8 +519,19 @@ orr_status orr_serve_submit(orr_server* server, const orr_solve_request* request
         if (r.sample_every != 0 && r.sample_every != s->opt.sample_every) {
             throw Refusal{ORR_ERR_INVALID, "serve: the request's sampling differs from the server's"};
         }
-        if (!(r.tolerance > 0.0) || !(r.reference_area > 0.0) || !(r.reference_length > 0.0)) {
+        if (r.mode != ORR_RUN_UNTIL_SETTLED && r.mode != ORR_RUN_FIXED_STEPS) {
+            throw Refusal{ORR_ERR_INVALID, "serve: unknown run mode"};
+        }
+        const bool fixed = r.mode == ORR_RUN_FIXED_STEPS;
+        if ((!fixed && !(r.tolerance > 0.0)) || !(r.reference_area > 0.0) || !(r.reference_length > 0.0)) {
             throw Refusal{ORR_ERR_INVALID, "serve: tolerance, area and length must be positive"};
+        }
+        if (fixed && (r.max_steps < r.window || r.max_steps % s->opt.chunk_steps != 0)) {
+            throw Refusal{ORR_ERR_INVALID, "serve: a fixed-steps solve needs max_steps a multiple of chunk_steps "
+                                           "and at least one window"};
+        }
+        if (!(r.ramp_steps >= 0.0) || !std::isfinite(r.ramp_steps)) {
+            throw Refusal{ORR_ERR_INVALID, "serve: ramp_steps must be finite and not negative"};
         }
         if (c.x_boundary != ORR_X_INFLOW_OUTFLOW || !(c.inlet_ux != 0.0)) {
             throw Refusal{ORR_ERR_INVALID, "serve: drag solves need an inflow with a non-zero inlet speed"};
@@ -497,6 +544,9 @@ orr_status orr_serve_submit(orr_server* server, const orr_solve_request* request
         const bool all = r.rho && r.ux && r.uy && r.uz;
         if (any && !all) {
             throw Refusal{ORR_ERR_INVALID, "serve: initial fields need all four arrays or none"};
+        }
+        if (any && r.ramp_steps > 0.0) {
+            throw Refusal{ORR_ERR_INVALID, "serve: a ramped solve starts at rest (no initial fields)"};
         }
         auto q = std::make_shared<Request>();
         q->config = c;
@@ -512,8 +562,10 @@ orr_status orr_serve_submit(orr_server* server, const orr_solve_request* request
         }
         q->allow_high_mach = r.allow_high_mach;
         q->window = r.window;
+        q->mode = r.mode;
         q->tolerance = r.tolerance;
         q->max_steps = r.max_steps ? r.max_steps : UINT64_MAX;
+        q->ramp_steps = r.ramp_steps;
         q->area = r.reference_area;
         q->length = r.reference_length;
         std::memcpy(q->centre, r.moment_centre, sizeof(q->centre));

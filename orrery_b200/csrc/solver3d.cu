@@ -75,7 +75,7 @@ void copy_message(const std::string& text, char* message, size_t capacity) {
 }
 
 void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const double* uy,
-                      const double* uz) {
+                      const double* uz, bool at_rest = false) {
     const auto& c = h->plan.c;
     const std::size_t cells = h->plan.cells;
     double* staged[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -91,7 +91,7 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
         }
         orr::copy_to_device(spans, 4, h->stream, h->device);
     }
-    const bool inflow = c.x_boundary == ORR_X_INFLOW_OUTFLOW;
+    const bool inflow = c.x_boundary == ORR_X_INFLOW_OUTFLOW && !at_rest;
     check(h->ops->init(h->g, h->cls, staged[0], staged[1], staged[2], staged[3], 1.0,
                        inflow ? c.inlet_ux : 0.0, inflow ? c.inlet_uy : 0.0,
                        inflow ? c.inlet_uz : 0.0, h->f[0], h->stream),
@@ -106,7 +106,7 @@ void initialize_state(orr_lbm3d* h, const double* rho, const double* ux, const d
     h->launches += 2;
     h->cur = 0;
     h->steps = 0;
-    const double v[3] = {c.inlet_ux, c.inlet_uy, c.inlet_uz};
+    const double v[3] = {at_rest ? 0.0 : c.inlet_ux, at_rest ? 0.0 : c.inlet_uy, at_rest ? 0.0 : c.inlet_uz};
     h->upload_inlet(v);
 }
 
@@ -126,6 +126,12 @@ __global__ void widen_populations_kernel(const S* __restrict__ f, double* __rest
 }
 
 } // namespace
+
+void orr::initialize_at_rest(orr_lbm3d* h) {
+    check(cudaSetDevice(h->device), "cudaSetDevice");
+    initialize_state(h, nullptr, nullptr, nullptr, nullptr, true);
+    check(cudaStreamSynchronize(h->stream), "initialize");
+}
 
 extern "C" {
 

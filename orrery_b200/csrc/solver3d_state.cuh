@@ -41,6 +41,13 @@ struct orr_lbm3d;
 void orr_batch3d_forget(orr_batch3d* batch, orr_lbm3d* solver) noexcept;
 
 namespace orr {
+// Initialises the solver at rest (rho 1, u 0 at every node) with a zero inlet
+// velocity: the start of a ramped solve (the reference adapter's gradual
+// start initialises the same state, lbm_aero_solver3d.cpp:320-329).
+void initialize_at_rest(orr_lbm3d* h);
+} // namespace orr
+
+namespace orr {
 
 constexpr uint32_t kGraphSteps = 16; // even: a graph returns to the buffer it started on
 constexpr uint32_t kDefaultBlock = 128;
@@ -126,6 +133,11 @@ struct orr_lbm3d {
     uint64_t steps = 0;
     uint64_t launches = 0;
     double inlet[3] = {0.0, 0.0, 0.0};
+    // Gradual start applied by a batch's sampled runs (served drag solves):
+    // ramp_steps > 0 sets the inlet velocity to ramp_u times the ramp
+    // fraction before every sampling interval.
+    double ramp_steps = 0.0;
+    double ramp_u[3] = {0.0, 0.0, 0.0};
     std::string error;
 
     const void* phys() const {

@@ -87,6 +87,18 @@ class Lbm3DConfig:
     def cells(self) -> int:
         return int(self.nx) * int(self.ny) * int(self.nz)
 
+    @classmethod
+    def from_c(cls, c: abi.CLbm3DConfig) -> "Lbm3DConfig":
+        """The configuration of a C ABI record (the inverse of to_c)."""
+        walls = {name: Wall(WallKind(getattr(c, name).kind), getattr(c, name).velocity_x)
+                 for name in ("y_low", "y_high", "z_low", "z_high")}
+        return cls(nx=c.nx, ny=c.ny, nz=c.nz, tau=c.tau, x_boundary=XBoundary(c.x_boundary),
+                   outlet=Outlet(c.outlet), inlet_ux=c.inlet_ux, inlet_uy=c.inlet_uy, inlet_uz=c.inlet_uz,
+                   body_force_x=c.body_force_x, body_force_y=c.body_force_y, body_force_z=c.body_force_z,
+                   smagorinsky=Smagorinsky(bool(c.smagorinsky_enabled), c.smagorinsky_constant),
+                   sponge=Sponge(c.sponge_strength, c.sponge_inlet, c.sponge_outlet, c.sponge_sides),
+                   solid_wall=SolidWall(c.solid_wall), **walls)
+
     def to_c(self) -> abi.CLbm3DConfig:
         c = abi.CLbm3DConfig()
         c.nx, c.ny, c.nz = int(self.nx), int(self.ny), int(self.nz)

@@ -72,14 +72,18 @@ class Server:
         self.close()
 
     def submit(self, w: Workload3D, window: int = 500, tolerance: float = 1e-4, max_steps: int = 0,
-               initial_state: bool = True, moment_centre=(0.0, 0.0, 0.0)) -> int:
+               initial_state: bool = True, moment_centre=(0.0, 0.0, 0.0), fixed_steps: bool = False,
+               ramp_steps: float = 0.0) -> int:
         """Queues the solve of workload `w`; returns its id.  Without
-        `initial_state` the solve starts from the uniform inlet state."""
+        `initial_state` the solve starts from the uniform inlet state.
+        `fixed_steps`: run exactly `max_steps` steps and report the means over
+        the last `window` steps.  `ramp_steps` > 0: start at rest with the
+        reference adapter's gradual start of the inlet velocity."""
         c = w.config.to_c()
         solid = np.ascontiguousarray(w.mask.solid, np.uint8).reshape(-1)
         dist = None if w.mask.distance is None else np.ascontiguousarray(w.mask.distance, np.float64).reshape(-1)
         fields = [np.ascontiguousarray(a, np.float64).reshape(-1) for a in (w.rho, w.ux, w.uy, w.uz)] \
-            if initial_state and w.rho is not None else [None] * 4
+            if initial_state and w.rho is not None and not ramp_steps > 0 else [None] * 4
         r = abi.CSolveRequest()
         r.config = ctypes.pointer(c)
         r.solid = ptr(solid, _u8p)
@@ -93,6 +97,8 @@ class Server:
         r.reference_area = float(w.reference_area)
         r.reference_length = float(w.reference_length)
         r.moment_centre = (ctypes.c_double * 3)(*[float(v) for v in moment_centre])
+        r.mode = abi.ORR_RUN_FIXED_STEPS if fixed_steps else abi.ORR_RUN_UNTIL_SETTLED
+        r.ramp_steps = float(ramp_steps)
         out = ctypes.c_uint64()
         self._check(self._lib.orr_serve_submit(self._h, ctypes.byref(r), ctypes.byref(out)))
         return out.value
