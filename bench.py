@@ -305,7 +305,7 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
     ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rows", "staged", "tiled"])
     ap.add_argument("--stages", type=int, default=0)
     ap.add_argument("--npt", type=int, default=0, help="nodes per thread of a staged span, or of the row kernel (2: the pair step)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "serve", "voxelize"])

@@ -125,7 +125,7 @@ typedef struct orr_solver_options {
  * periodic or free-slip sides and halfway walls (and refuses others).  AUTO picks STAGED for the binary16
  * and bfloat16 forms when the lattice qualifies, ROWS otherwise.  Both give
  * the same result bit for bit. */
-enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2 };
+enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2, ORR_KERNEL_TILED = 3 };
 
 typedef struct orr_lbm3d orr_lbm3d;
 typedef struct orr_lbm2d orr_lbm2d;
@@ -161,11 +161,12 @@ ORR_API void orr_lbm3d_destroy(orr_lbm3d* solver);
 ORR_API const char* orr_lbm3d_last_error(const orr_lbm3d* solver);
 
 /* The step kernel a solver runs and its launch shape (no counterpart in the
- * reference, whose GL backend has one dispatch shape): kernel ORR_KERNEL_ROWS
- * or ORR_KERNEL_STAGED, threads per CTA, pipeline stages and shared bytes
- * per CTA (staged), CTAs per launch, resident CTAs per SM (staged),
- * registers per thread, nodes per consumer thread of a staged span, and the
- * staged / per-node work items. */
+ * reference, whose GL backend has one dispatch shape): kernel ORR_KERNEL_ROWS,
+ * ORR_KERNEL_STAGED or ORR_KERNEL_TILED, threads per CTA (consumer threads of
+ * the persistent steps), pipeline stages and shared bytes per CTA, CTAs per
+ * launch, resident CTAs per SM, registers per thread, nodes per consumer
+ * thread of a staged span or tile, and the staged spans or tiles and the
+ * per-node work items. */
 typedef struct orr_kernel_info {
     int32_t kernel;
     uint32_t block;
@@ -458,7 +459,11 @@ typedef struct orr_force_links {
  * device, using as scratch a fixed 192 KiB array compiled into the library
  * (held by every GPU that loads the library until exit), so it calls no
  * cudaMalloc or cudaFree.  More than ORR_FORCE_STATIC_MAX_LINKS links are
- * refused with ORR_ERR_INVALID.  The first call on a device looks up the
+ * refused with ORR_ERR_INVALID, and so is a call whose tables hold a link
+ * outside the lattice (a cell beyond nx*ny*nz, a direction outside 1..18 or
+ * an interpolation source beyond the lattice: the caller owns the tables,
+ * and such links are skipped on the device, never read through).  The
+ * first call on a device looks up the
  * array's device address (make it before any stream capture).  All calls
  * share the array: calls whose work overlaps on the GPU race and must be
  * serialised by the caller.  Blocks until the result is in force_moment. */

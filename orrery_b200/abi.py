@@ -74,8 +74,9 @@ class CForceLinks(ctypes.Structure):
 ORR_FORCE_STATIC_MAX_LINKS = 8388608
 
 
-ORR_KERNEL_AUTO, ORR_KERNEL_ROWS, ORR_KERNEL_STAGED = 0, 1, 2
-KERNEL_NAMES = {"auto": ORR_KERNEL_AUTO, "rows": ORR_KERNEL_ROWS, "staged": ORR_KERNEL_STAGED}
+ORR_KERNEL_AUTO, ORR_KERNEL_ROWS, ORR_KERNEL_STAGED, ORR_KERNEL_TILED = 0, 1, 2, 3
+KERNEL_NAMES = {"auto": ORR_KERNEL_AUTO, "rows": ORR_KERNEL_ROWS, "staged": ORR_KERNEL_STAGED,
+                "tiled": ORR_KERNEL_TILED}
 
 
 class CKernelInfo(ctypes.Structure):

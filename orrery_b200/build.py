@@ -39,6 +39,7 @@ SOURCES = {
     "solver3d.cu": [],
     "solver2d.cu": [],
     "force_static.cu": [],
+    "tiles.cu": [],
     "batch3d.cu": [],
     "serve3d.cu": [],
     "voxel.cu": ["-fmad=false"],

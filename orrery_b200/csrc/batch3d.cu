@@ -30,6 +30,7 @@
 
 #include "batch3d_state.cuh"
 #include "common.h"
+#include "trace.h"
 #include "solver3d_state.cuh"
 
 using namespace orr;
@@ -44,46 +45,7 @@ orr_batch3d* batch_of(orr_batch3d* b) {
     return b;
 }
 
-// The inlet velocities of one sampling interval of a ramp plan (one block;
-// every thread reads the interval before thread 0 advances it).
-template <class A>
-__global__ void apply_inlets_kernel(const A* __restrict__ plan, A* const* __restrict__ inlets, uint32_t n,
-                                    uint32_t intervals, uint32_t* __restrict__ counter) {
-    const uint32_t j = *counter;
-    if (j < intervals) {
-        for (uint32_t r = threadIdx.x; r < n; r += blockDim.x) {
-            const A* v = plan + (static_cast<uint64_t>(j) * n + r) * 3;
-            A* dst = inlets[r];
-            dst[0] = v[0];
-            dst[1] = v[1];
-            dst[2] = v[2];
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && j < intervals) {
-        *counter = j + 1;
-    }
-}
-
 } // namespace
-
-cudaError_t orr::launch_apply_inlets(int32_t storage, const void* plan, void* const* inlets, uint32_t n,
-                                     uint32_t intervals, uint32_t* counter, cudaStream_t s) {
-    if (n == 0) {
-        return cudaSuccess;
-    }
-    const uint32_t threads = std::min<uint32_t>(256u, (n + 31u) / 32u * 32u);
-    if (storage == ORR_STORAGE_F64) {
-        apply_inlets_kernel<double><<<1, threads, 0, s>>>(static_cast<const double*>(plan),
-                                                          reinterpret_cast<double* const*>(inlets), n, intervals,
-                                                          counter);
-    } else {
-        apply_inlets_kernel<float><<<1, threads, 0, s>>>(static_cast<const float*>(plan),
-                                                         reinterpret_cast<float* const*>(inlets), n, intervals,
-                                                         counter);
-    }
-    return cudaGetLastError();
-}
 
 // Called by orr_lbm3d_destroy for a member that is still in a batch.
 void orr_batch3d_forget(orr_batch3d* b, orr_lbm3d* m) noexcept {
@@ -255,6 +217,7 @@ orr_status orr_batch3d_schedule(const orr_batch3d* batch, orr_batch_schedule* sc
 }
 
 orr_status orr_batch3d_step(orr_batch3d* batch, uint64_t count) {
+    orr::Zone zone("batch_step");
     return orr::guarded(batch ? &batch->error : nullptr, [&]() -> orr_status {
         orr_batch3d* b = batch_of(batch);
         b->run(count, 0);
@@ -264,6 +227,7 @@ orr_status orr_batch3d_step(orr_batch3d* batch, uint64_t count) {
 
 orr_status orr_batch3d_step_sampled(orr_batch3d* batch, uint64_t count, uint32_t sample_every,
                                     double* sums) {
+    orr::Zone zone("batch_step");
     return orr::guarded(batch ? &batch->error : nullptr, [&]() -> orr_status {
         orr_batch3d* b = batch_of(batch);
         if (sample_every == 0 || sample_every % 2 != 0 || count % sample_every != 0) {

@@ -8,7 +8,6 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
-#include <numbers>
 #include <string>
 #include <vector>
 
@@ -35,13 +34,6 @@ inline constexpr Candidate kCandidates[] = {
     {ORR_KERNEL_ROWS, 128, 0, 2, 0},    {ORR_KERNEL_ROWS, 128, 0, 2, 64},
     {ORR_KERNEL_ROWS, 64, 0, 0, 0},     {ORR_KERNEL_ROWS, 64, 0, 0, 64},
 };
-
-// Copies sampling interval `*counter` of `plan` ([interval][member][3]
-// inlet velocity values in the arithmetic type of `storage`, `intervals`
-// intervals of n members) into the members' inlet buffers `inlets[m]` and
-// advances the counter; past the last interval it copies nothing.  One block.
-cudaError_t launch_apply_inlets(int32_t storage, const void* plan, void* const* inlets, uint32_t n,
-                                uint32_t intervals, uint32_t* counter, cudaStream_t s);
 
 } // namespace orr
 
@@ -102,22 +94,6 @@ struct orr_batch3d {
     uint64_t chunks = 0;
     std::vector<ForceJob> host_jobs;
 
-    // Gradual start of the members with ramp_steps > 0 (served drag
-    // solves): a sampled run plans every member's inlet velocity for each of
-    // its sampling intervals on the host (the reference adapter's rule, in
-    // binary64, then rounded to the arithmetic type as an inlet upload is),
-    // uploads the plan, and one small kernel at the start of every sampling
-    // interval copies that interval's values into the members' inlet buffers.
-    std::vector<uint32_t> ramp_members;        // indices into members
-    void* ramp_inlets = nullptr;               // device table of their inlet buffers
-    std::size_t ramp_inlets_bytes = 0;
-    void* ramp_plan = nullptr;                 // [interval][ramp member][3]
-    std::size_t ramp_plan_bytes = 0;
-    uint32_t* ramp_counter = nullptr;          // the next interval of the plan
-    uint32_t ramp_intervals = 0;               // intervals of the current plan
-    std::vector<unsigned char> ramp_host;
-    bool graph_ramp = false;                   // the graph holds the interval kernels
-
     uint64_t launches = 0;
     std::string error;
 
@@ -139,12 +115,9 @@ struct orr_batch3d {
         if (fork_event) cudaEventDestroy(fork_event);
         fork_event = nullptr;
         for (void* p : {table, static_cast<void*>(status), jobs, static_cast<void*>(partial),
-                        static_cast<void*>(sums), ramp_inlets, ramp_plan, static_cast<void*>(ramp_counter)}) {
+                        static_cast<void*>(sums)}) {
             if (p) cudaFree(p);
         }
-        ramp_inlets = ramp_plan = nullptr;
-        ramp_counter = nullptr;
-        ramp_inlets_bytes = ramp_plan_bytes = 0;
         if (done) cudaEventDestroy(done);
         if (t0) cudaEventDestroy(t0);
         if (t1) cudaEventDestroy(t1);
@@ -292,95 +265,8 @@ struct orr_batch3d {
               "batch force table upload");
         grow(partial, partial_count, std::max<uint64_t>(chunks, 1) * 6, "batch force partials");
         grow(sums, sums_count, members.size() * 6, "batch force sums");
-        // Ramped members and their inlet buffers.
-        ramp_members.clear();
-        std::vector<void*> inlets;
-        for (std::size_t k = 0; k < members.size(); ++k) {
-            if (members[k]->ramp_steps > 0.0) {
-                ramp_members.push_back(static_cast<uint32_t>(k));
-                inlets.push_back(members[k]->inlet_dev());
-            }
-        }
-        if (!inlets.empty()) {
-            grow_bytes(ramp_inlets, ramp_inlets_bytes, inlets.size() * sizeof(void*), "batch inlet table");
-            check(cudaMemcpyAsync(ramp_inlets, inlets.data(), inlets.size() * sizeof(void*), cudaMemcpyHostToDevice,
-                                  stream),
-                  "batch inlet table upload");
-            if (ramp_counter == nullptr) {
-                check(cudaMalloc(reinterpret_cast<void**>(&ramp_counter), sizeof(uint32_t)), "batch ramp counter");
-            }
-        }
         check(cudaStreamSynchronize(stream), "batch force table upload");
         dirty = false;
-    }
-
-    // Plans the inlet velocities of the ramped members for the `count /
-    // sample` sampling intervals of a run (each from the interval's first
-    // step, held over the interval: LbmAeroSolver3D::step,
-    // lbm_aero_solver3d.cpp:398-412) and uploads the plan.
-    void plan_ramp(uint64_t count, uint32_t sample) {
-        const std::size_t n = ramp_members.size();
-        const uint64_t intervals = count / sample;
-        const std::size_t bytes_per = storage == ORR_STORAGE_F64 ? sizeof(double) : sizeof(float);
-        const std::size_t need = static_cast<std::size_t>(intervals) * n * 3 * bytes_per;
-        if (need > ramp_plan_bytes || ramp_plan == nullptr) {
-            drop_graph(); // the graph holds the plan's address
-            grow_bytes(ramp_plan, ramp_plan_bytes, need, "batch inlet plan");
-        }
-        ramp_host.resize(need);
-        for (uint64_t j = 0; j < intervals; ++j) {
-            for (std::size_t r = 0; r < n; ++r) {
-                const orr_lbm3d* m = members[ramp_members[r]];
-                const uint64_t now = m->steps + j * sample;
-                const double start = static_cast<double>(now - now % sample);
-                const double fraction =
-                    start >= m->ramp_steps ? 1.0 : 0.5 * (1.0 - std::cos(std::numbers::pi * start / m->ramp_steps));
-                for (int d = 0; d < 3; ++d) {
-                    const double v = fraction * m->ramp_u[d];
-                    unsigned char* at = ramp_host.data() + ((j * n + r) * 3 + static_cast<std::size_t>(d)) * bytes_per;
-                    if (bytes_per == sizeof(double)) {
-                        std::memcpy(at, &v, sizeof v);
-                    } else {
-                        const float f = to_f32(v);
-                        std::memcpy(at, &f, sizeof f);
-                    }
-                }
-            }
-        }
-        // From pageable memory: the call returns once the host array is
-        // staged, so it may be refilled by the next run.
-        check(cudaMemcpyAsync(ramp_plan, ramp_host.data(), need, cudaMemcpyHostToDevice, stream), "batch inlet plan");
-        check(cudaMemsetAsync(ramp_counter, 0, sizeof(uint32_t), stream), "batch ramp counter");
-        ramp_intervals = static_cast<uint32_t>(intervals);
-    }
-
-    // After a ramped run: the members' host copies of their inlet velocity
-    // (the values of their last interval).
-    void settle_ramp(uint64_t count, uint32_t sample) {
-        const std::size_t n = ramp_members.size();
-        const uint64_t last = count / sample - 1;
-        const std::size_t bytes_per = storage == ORR_STORAGE_F64 ? sizeof(double) : sizeof(float);
-        for (std::size_t r = 0; r < n; ++r) {
-            orr_lbm3d* m = members[ramp_members[r]];
-            for (int d = 0; d < 3; ++d) {
-                const unsigned char* at =
-                    ramp_host.data() + ((last * n + r) * 3 + static_cast<std::size_t>(d)) * bytes_per;
-                if (bytes_per == sizeof(double)) {
-                    std::memcpy(&m->inlet[d], at, sizeof(double));
-                } else {
-                    float f;
-                    std::memcpy(&f, at, sizeof f);
-                    m->inlet[d] = static_cast<double>(f);
-                }
-            }
-        }
-    }
-
-    void launch_ramp() {
-        check(launch_apply_inlets(storage, ramp_plan, static_cast<void* const*>(ramp_inlets),
-                                  static_cast<uint32_t>(ramp_members.size()), ramp_intervals, ramp_counter, stream),
-              "batch inlet kernel");
-        ++launches;
     }
 
     bool branched() const { return branches > 0; }
@@ -519,7 +405,7 @@ struct orr_batch3d {
 
     // kGraphSteps steps, with a force sample after every `sample` steps
     // when sample > 0 (kGraphSteps is then a multiple of it).
-    void build_graph(uint32_t sample, uint32_t steps, bool ramp = false) {
+    void build_graph(uint32_t sample, uint32_t steps) {
         drop_graph();
         cudaGraph_t captured = nullptr;
         const uint64_t before = launches;
@@ -528,9 +414,6 @@ struct orr_batch3d {
         try {
             if (sample > 0) {
                 for (uint32_t k = 0; k < steps; k += sample) {
-                    if (ramp) {
-                        launch_ramp();
-                    }
                     launch_steps(sample);
                     launch_sample(true);
                 }
@@ -552,9 +435,7 @@ struct orr_batch3d {
         check(e, "batch graph instantiate");
         graph_sample = sample;
         graph_steps = steps;
-        graph_ramp = ramp;
-        graph_launches = launches_per_step() * steps +
-                         (sample > 0 ? (steps / sample) * ((chunks > 0 ? 2 : 1) + (ramp ? 1 : 0)) : 0);
+        graph_launches = launches_per_step() * steps + (sample > 0 ? (steps / sample) * (chunks > 0 ? 2 : 1) : 0);
     }
     uint32_t graph_steps = 0;
     uint64_t graph_launches = 0;
@@ -594,21 +475,12 @@ struct orr_batch3d {
         if (sample > 0) {
             check(cudaMemsetAsync(sums, 0, members.size() * 6 * sizeof(double), stream), "batch sums");
         }
-        // Ramped members (sampled runs only; `count` is then a multiple of
-        // `sample`).
-        const bool ramp = sample > 0 && !ramp_members.empty();
-        if (ramp) {
-            plan_ramp(count, sample);
-        }
         // Graphs cover whole sampling periods: the largest multiple of
         // `sample` up to kGraphSteps (at least one period).
         const uint32_t period = sample > 0 ? std::max<uint32_t>(1u, kGraphSteps / sample) * sample
                                            : kGraphSteps;
         uint64_t done_steps = 0;
         const auto single = [&]() {
-            if (ramp && done_steps % sample == 0) {
-                launch_ramp();
-            }
             launch_steps(1);
             ++done_steps;
             if (sample > 0 && done_steps % sample == 0) {
@@ -619,8 +491,8 @@ struct orr_batch3d {
             single();
         }
         if (count - done_steps >= period) {
-            if (!graph || graph_sample != sample || graph_steps != period || graph_ramp != ramp) {
-                build_graph(sample, period, ramp);
+            if (!graph || graph_sample != sample || graph_steps != period) {
+                build_graph(sample, period);
             }
             while (count - done_steps >= period) {
                 check(cudaGraphLaunch(graph, stream), "batch graph launch");
@@ -631,11 +503,20 @@ struct orr_batch3d {
         while (done_steps < count) {
             single();
         }
-        if (ramp) {
-            settle_ramp(count, sample);
-        }
         release_members(count);
     }
+
+    // The serving loop's use of the batch (serve3d.cu): before capturing one
+    // sampling period of `sample` (even) steps as the body of its device
+    // loop, the tables of the current members; after a launch that ran
+    // `count` steps, the members' step counts and stream order.
+    void prepare_loop(uint32_t sample) {
+        (void)sample;
+        if (stale() || flip != 0) {
+            rebuild();
+        }
+    }
+    void finish_loop(uint64_t count) { release_members(count); }
 
     void check_status() {
         uint32_t word = 0;
@@ -665,7 +546,7 @@ struct orr_batch3d {
     }
 
     void run_graph_only() {
-        if (!graph || graph_sample != 0 || graph_steps != kGraphSteps || graph_ramp) {
+        if (!graph || graph_sample != 0 || graph_steps != kGraphSteps) {
             build_graph(0, kGraphSteps);
         }
         check(cudaGraphLaunch(graph, stream), "batch graph launch");

@@ -14,10 +14,13 @@
 //           and writes its six partial sums to slot b of the scratch array;
 //   pass 2  one block adds the partial sums of all slots in slot order and
 //           writes the six totals to the last slot.
-// Every slot pass 2 reads is written by pass 1 of the same call, so nothing
-// has to be cleared between calls; a call's contents stay in the array until
-// the next call overwrites them.  Calls that overlap on the GPU race on the
-// array; callers serialise them (one stream, or one call at a time).
+// Every slot pass 2 reads is written by pass 1 of the same call; the one
+// value that must start at zero, the flag a link outside the lattice raises
+// (such links are skipped: the tables come from the caller), is cleared by a
+// memset of the array at the start of each call.  A call's contents stay in
+// the array until the next call overwrites them.  Calls that overlap on the
+// GPU race on the array; callers serialise them (one stream, or one call at
+// a time).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -41,8 +44,10 @@ constexpr uint64_t kChunk = 2048;                      // links per block of pas
 constexpr uint64_t kSlots = ORR_FORCE_STATIC_MAX_LINKS / kChunk;  // 4096 partial-sum slots
 static_assert(kSlots * kChunk == ORR_FORCE_STATIC_MAX_LINKS, "whole chunks");
 
-// 4096 slots of 6 partial sums plus the slot of the totals: 196,656 bytes.
-__device__ __align__(256) double g_force_scratch[(kSlots + 1) * 6];
+// 4096 slots of 6 partial sums, the slot of the totals and the flag slot
+// (its first value is set when a link of the caller's tables is out of
+// range): 196,704 bytes.
+__device__ __align__(256) double g_force_scratch[(kSlots + 2) * 6];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -84,56 +89,27 @@ __device__ void block_sum6(double (&v)[6]) {
     }
 }
 
-// Pass 1: the links of chunk blockIdx.x; per link c_o (f*_o + f_j(t+1)) and
-// its moment about the origin at the wall point x - q c_j (CpuLbm3D::force,
-// lbm3d_cpu.cpp:192-203; add_link_force, lbm3d_common.cpp:213-241).
+// Pass 1: the links of chunk blockIdx.x (add_link3, the solver's per-link
+// routine, with the caller's tables checked: a link whose cell, direction or
+// interpolation source lies outside the lattice is skipped and raises the
+// flag slot).
 template <class S>
 __global__ void __launch_bounds__(kThreads) force_static_partials(
     uint64_t nx, uint64_t ny, uint64_t cells, const S* __restrict__ f,
     const uint32_t* __restrict__ lcell, const uint32_t* __restrict__ ldir,
     const double* __restrict__ lq, uint64_t links, double* __restrict__ scratch) {
-    using A = typename Storage<S>::A;
-    using T = Storage<S>;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     const uint64_t begin = static_cast<uint64_t>(blockIdx.x) * kChunk;
     const uint64_t end = begin + kChunk < links ? begin + kChunk : links;
     const uint64_t plane = nx * ny;
+    bool bad = false;
     for (uint64_t k = begin + threadIdx.x; k < end; k += kThreads) {
-        const uint64_t h = lcell[k];
-        const int j = static_cast<int>(ldir[k]);
-        const int o = opposite_rt(j);
-        int jx, jy, jz;
-        c_rt(j, jx, jy, jz);
-        const double q = lq[k];
-        const A qa = static_cast<A>(q);
-        const A leaving = T::load(f + static_cast<uint64_t>(o) * cells + h);
-        A back;
-        if (q == 0.5) {
-            back = leaving;
-        } else if (q < 0.5) {
-            const uint64_t farther = static_cast<uint64_t>(static_cast<int64_t>(h) + jx +
-                                                           static_cast<int64_t>(nx) * jy +
-                                                           static_cast<int64_t>(plane) * jz);
-            back = A(2) * qa * leaving + (A(1) - A(2) * qa) * T::load(f + static_cast<uint64_t>(o) * cells + farther);
-        } else {
-            back = (leaving + (A(2) * qa - A(1)) * T::load(f + static_cast<uint64_t>(j) * cells + h)) / (A(2) * qa);
+        if (!add_link3<S, true>(nx, plane, cells, f, lcell[k], static_cast<int>(ldir[k]), lq[k], acc)) {
+            bad = true;
         }
-        double ex = static_cast<double>(leaving) + static_cast<double>(back);
-        if (T::kShifted) {
-            ex += 2.0 * w_rt(o);
-        }
-        const double fx = -jx * ex, fy = -jy * ex, fz = -jz * ex;
-        const uint64_t z = h / plane, rest = h - z * plane;
-        const uint64_t y = rest / nx, x = rest - y * nx;
-        const double rx = static_cast<double>(x) - q * jx;
-        const double ry = static_cast<double>(y) - q * jy;
-        const double rz = static_cast<double>(z) - q * jz;
-        acc[0] += fx;
-        acc[1] += fy;
-        acc[2] += fz;
-        acc[3] += ry * fz - rz * fy;
-        acc[4] += rz * fx - rx * fz;
-        acc[5] += rx * fy - ry * fx;
+    }
+    if (bad) {
+        scratch[(kSlots + 1) * 6] = 1.0;
     }
     block_sum6(acc);
     if (threadIdx.x == 0) {
@@ -177,7 +153,10 @@ extern "C" orr_status orr_lbm3d_force_static(const orr_force_links* args, double
                               std::to_string(ORR_FORCE_STATIC_MAX_LINKS) +
                               " the fixed scratch array holds; use orr_lbm3d_force"};
         }
-        if (a.nx < 1 || a.ny < 1 || a.nz < 1 || a.nx * a.ny * a.nz > kMaxGridCells) {
+        uint64_t plane = 0, cells = 0;
+        if (a.nx < 1 || a.ny < 1 || a.nz < 1 || a.nx > kMaxGridCells || a.ny > kMaxGridCells ||
+            a.nz > kMaxGridCells || __builtin_mul_overflow(a.nx, a.ny, &plane) ||
+            __builtin_mul_overflow(plane, a.nz, &cells) || cells > kMaxGridCells) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d force_static: lattice dimensions out of range"};
         }
         if (a.storage < ORR_STORAGE_F32 || a.storage > ORR_STORAGE_F64) {
@@ -198,6 +177,9 @@ extern "C" orr_status orr_lbm3d_force_static(const orr_force_links* args, double
         }
         cudaStream_t s = static_cast<cudaStream_t>(a.stream);
         const unsigned blocks = static_cast<unsigned>((a.links + kChunk - 1) / kChunk);
+        // The flag slot starts clear; the totals and the flag come back in
+        // one copy.
+        check(cudaMemsetAsync(scratch + (kSlots + 1) * 6, 0, sizeof(double), s), "force_static flag");
         switch (a.storage) {
             case ORR_STORAGE_F16:
                 launch_partials<__half>(a, s, blocks, scratch);
@@ -215,10 +197,15 @@ extern "C" orr_status orr_lbm3d_force_static(const orr_force_links* args, double
         check(cudaGetLastError(), "force_static partial sums");
         force_static_total<<<1, kThreads, 0, s>>>(blocks, scratch);
         check(cudaGetLastError(), "force_static total");
-        check(cudaMemcpyAsync(force_moment, scratch + kSlots * 6, 6 * sizeof(double),
-                              cudaMemcpyDeviceToHost, s),
+        double result[7];
+        check(cudaMemcpyAsync(result, scratch + kSlots * 6, 7 * sizeof(double), cudaMemcpyDeviceToHost, s),
               "force_static read-back");
         check(cudaStreamSynchronize(s), "force_static read-back");
+        if (result[6] != 0.0) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d force_static: a link's cell, direction or interpolation "
+                                           "source lies outside the lattice"};
+        }
+        std::memcpy(force_moment, result, 6 * sizeof(double));
         return ORR_OK;
     });
 }

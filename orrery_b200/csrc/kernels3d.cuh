@@ -1295,71 +1295,39 @@ __device__ __forceinline__ void block_reduce_add(double (&v)[N], double* out) {
     }
 }
 
-// Momentum exchange over the boundary links, summed in binary64: force
-// sum c_o (f*_o(x) + f_j(x, t+1)) and moment sum r x F at the wall point
-// x - q c_j (CpuLbm3D::force, lbm3d_cpu.cpp:192-203; add_link_force and
-// link_wall_point, lbm3d_common.cpp:213-241; lbm_d3q19_force.comp.glsl).
-template <class S>
-__global__ void force3d_kernel(Geom3D g, const S* __restrict__ f, const uint32_t* __restrict__ lcell,
-                               const uint32_t* __restrict__ ldir, const double* __restrict__ lq,
-                               uint64_t links, double* __restrict__ out) {
-    using A = typename Storage<S>::A;
-    using T = Storage<S>;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < links;
-         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t h = lcell[k];
-        const int j = static_cast<int>(ldir[k]);
-        const int o = opposite_rt(j);
-        const double q = lq[k];
-        int jx, jy, jz;
-        c_rt(j, jx, jy, jz);
-        const A leaving = T::load(f + static_cast<uint64_t>(o) * g.cells + h);
-        A back;
-        const A qa = static_cast<A>(q);
-        if (q == 0.5) {
-            back = leaving;
-        } else if (q < 0.5) {
-            const uint64_t farther = static_cast<uint64_t>(
-                static_cast<int64_t>(h) + jx + static_cast<int64_t>(g.nx) * jy +
-                static_cast<int64_t>(g.plane) * jz);
-            back = A(2) * qa * leaving + (A(1) - A(2) * qa) * T::load(f + static_cast<uint64_t>(o) * g.cells + farther);
-        } else {
-            back = (leaving + (A(2) * qa - A(1)) * T::load(f + static_cast<uint64_t>(j) * g.cells + h)) /
-                   (A(2) * qa);
-        }
-        double ex = static_cast<double>(leaving) + static_cast<double>(back);
-        if (T::kShifted) {
-            ex += 2.0 * w_rt(o);
-        }
-        // c_o = -c_j
-        const double fx = -jx * ex, fy = -jy * ex, fz = -jz * ex;
-        const uint32_t z = static_cast<uint32_t>(h / g.plane);
-        const uint32_t rest = static_cast<uint32_t>(h - static_cast<uint64_t>(z) * g.plane);
-        const uint32_t y = rest / g.nx, x = rest - y * g.nx;
-        const double rx = static_cast<double>(x) - q * jx;
-        const double ry = static_cast<double>(y) - q * jy;
-        const double rz = static_cast<double>(z) - q * jz;
-        acc[0] += fx;
-        acc[1] += fy;
-        acc[2] += fz;
-        acc[3] += ry * fz - rz * fy;
-        acc[4] += rz * fx - rx * fz;
-        acc[5] += rx * fy - ry * fx;
-    }
-    block_reduce_add<6>(acc, out);
-}
+// One boundary link's momentum exchange c_o (f*_o(x) + f_j(x, t+1)) and its
+// moment about the origin at the wall point x - q c_j, added to acc
+// (CpuLbm3D::force, lbm3d_cpu.cpp:192-203; add_link_force and link_wall_point,
+// lbm3d_common.cpp:213-241; lbm_d3q19_force.comp.glsl).  The one per-link
+// routine of every force kernel (the solver's, the batched and the
+// allocation-free one): the population arithmetic rounds explicitly in the
+// storage's arithmetic type and the binary64 sums use unfused intrinsics, so
+// no unit contracts them differently and every kernel sums the same terms.
+// kChecked: the link comes from a caller's table, so a cell beyond the
+// lattice, a direction outside 1..18 or an interpolation source outside the
+// lattice skips the link and returns false (the plan's own links are in
+// range by construction).
+// Unfused binary64 forms of r_mul / r_sub / r_fma for the link arithmetic
+// (the binary32 ones already round explicitly); the same bits in every unit,
+// with or without FMA contraction.
+__device__ __forceinline__ float lk_mul(float a, float b) { return r_mul(a, b); }
+__device__ __forceinline__ float lk_sub(float a, float b) { return r_sub(a, b); }
+__device__ __forceinline__ float lk_fma(float a, float b, float c) { return r_fma(a, b, c); }
+__device__ __forceinline__ double lk_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double lk_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double lk_fma(double a, double b, double c) { return __dadd_rn(__dmul_rn(a, b), c); }
 
-// ------------------------------------------------------ batched forces --
-
-// One boundary link's momentum exchange and its moment about the origin,
-// added to acc (the per-link arithmetic of force3d_kernel).
-template <class S>
-__device__ __forceinline__ void add_link3(uint64_t nx, uint64_t plane, uint64_t cells,
+template <class S, bool kChecked = false>
+__device__ __forceinline__ bool add_link3(uint64_t nx, uint64_t plane, uint64_t cells,
                                           const S* __restrict__ f, uint64_t h, int j, double q,
                                           double (&acc)[6]) {
     using A = typename Storage<S>::A;
     using T = Storage<S>;
+    if constexpr (kChecked) {
+        if (h >= cells || j < 1 || j >= d3::Q || !(q >= 0.0 && q <= 1.0)) {
+            return false;
+        }
+    }
     const int o = opposite_rt(j);
     int jx, jy, jz;
     c_rt(j, jx, jy, jz);
@@ -1369,30 +1337,57 @@ __device__ __forceinline__ void add_link3(uint64_t nx, uint64_t plane, uint64_t 
     if (q == 0.5) {
         back = leaving;
     } else if (q < 0.5) {
-        const uint64_t farther = static_cast<uint64_t>(static_cast<int64_t>(h) + jx +
-                                                       static_cast<int64_t>(nx) * jy +
-                                                       static_cast<int64_t>(plane) * jz);
-        back = A(2) * qa * leaving + (A(1) - A(2) * qa) * T::load(f + static_cast<uint64_t>(o) * cells + farther);
+        const int64_t farther = static_cast<int64_t>(h) + jx + static_cast<int64_t>(nx) * jy +
+                                static_cast<int64_t>(plane) * jz;
+        if constexpr (kChecked) {
+            if (farther < 0 || static_cast<uint64_t>(farther) >= cells) {
+                return false;
+            }
+        }
+        const A t = lk_mul(A(2), qa);
+        back = lk_fma(t, leaving,
+                      lk_mul(lk_sub(A(1), t),
+                             T::load(f + static_cast<uint64_t>(o) * cells + static_cast<uint64_t>(farther))));
     } else {
-        back = (leaving + (A(2) * qa - A(1)) * T::load(f + static_cast<uint64_t>(j) * cells + h)) / (A(2) * qa);
+        const A t = lk_mul(A(2), qa);
+        back = r_div(lk_fma(lk_sub(t, A(1)), T::load(f + static_cast<uint64_t>(j) * cells + h), leaving), t);
     }
-    double ex = static_cast<double>(leaving) + static_cast<double>(back);
+    double ex = __dadd_rn(static_cast<double>(leaving), static_cast<double>(back));
     if (T::kShifted) {
-        ex += 2.0 * w_rt(o);
+        ex = __dadd_rn(ex, __dmul_rn(2.0, w_rt(o)));
     }
+    // c_o = -c_j
     const double fx = -jx * ex, fy = -jy * ex, fz = -jz * ex;
     const uint64_t z = h / plane, rest = h - z * plane;
     const uint64_t y = rest / nx, x = rest - y * nx;
-    const double rx = static_cast<double>(x) - q * jx;
-    const double ry = static_cast<double>(y) - q * jy;
-    const double rz = static_cast<double>(z) - q * jz;
-    acc[0] += fx;
-    acc[1] += fy;
-    acc[2] += fz;
-    acc[3] += ry * fz - rz * fy;
-    acc[4] += rz * fx - rx * fz;
-    acc[5] += rx * fy - ry * fx;
+    const double rx = __dsub_rn(static_cast<double>(x), __dmul_rn(q, jx));
+    const double ry = __dsub_rn(static_cast<double>(y), __dmul_rn(q, jy));
+    const double rz = __dsub_rn(static_cast<double>(z), __dmul_rn(q, jz));
+    acc[0] = __dadd_rn(acc[0], fx);
+    acc[1] = __dadd_rn(acc[1], fy);
+    acc[2] = __dadd_rn(acc[2], fz);
+    acc[3] = __dadd_rn(acc[3], __dsub_rn(__dmul_rn(ry, fz), __dmul_rn(rz, fy)));
+    acc[4] = __dadd_rn(acc[4], __dsub_rn(__dmul_rn(rz, fx), __dmul_rn(rx, fz)));
+    acc[5] = __dadd_rn(acc[5], __dsub_rn(__dmul_rn(rx, fy), __dmul_rn(ry, fx)));
+    return true;
 }
+
+// Momentum exchange over the boundary links, summed in binary64 (one thread
+// per link, add_link3; warp shuffles, a block reduction and one atomic per
+// value and block).
+template <class S>
+__global__ void force3d_kernel(Geom3D g, const S* __restrict__ f, const uint32_t* __restrict__ lcell,
+                               const uint32_t* __restrict__ ldir, const double* __restrict__ lq,
+                               uint64_t links, double* __restrict__ out) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < links;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        add_link3<S>(g.nx, g.plane, g.cells, f, lcell[k], static_cast<int>(ldir[k]), lq[k], acc);
+    }
+    block_reduce_add<6>(acc, out);
+}
+
+// ------------------------------------------------------ batched forces --
 
 // The links of one lattice for the batched force (device table entry).
 struct ForceJob {

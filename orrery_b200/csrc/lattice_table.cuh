@@ -93,4 +93,38 @@ inline StagedShape staged_shape(const Ops3D& ops, bool smag, uint32_t block, uin
     return s;
 }
 
+// Launch shape of the tiled step for tiles of `rows` rows and `block`
+// consumer threads: the most stages (up to 4) that keep the residency of one
+// stage, unless `stages` is given; npt holds the nodes per consumer thread
+// and tile.
+inline StagedShape tiled_shape(const Ops3D& ops, bool smag, uint32_t rows, uint32_t block, uint32_t stages,
+                               int device) {
+    StagedShape s;
+    s.block = block;
+    s.npt = kTileW * rows / block;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        return s;
+    }
+    if (stages != 0) {
+        s.stages = stages;
+        s.per_sm = ops.tiled_occupancy(smag, rows, block, stages);
+    } else {
+        const int best = ops.tiled_occupancy(smag, rows, block, 1);
+        s.stages = 2;
+        s.per_sm = ops.tiled_occupancy(smag, rows, block, 2);
+        for (uint32_t k = 4; k > 2; --k) {
+            const int o = ops.tiled_occupancy(smag, rows, block, k);
+            if (o == best && o > 0) {
+                s.stages = k;
+                s.per_sm = o;
+                break;
+            }
+        }
+    }
+    s.grid = static_cast<uint32_t>(std::max(s.per_sm, 0)) * static_cast<uint32_t>(sms);
+    return s;
+}
+
 } // namespace orr

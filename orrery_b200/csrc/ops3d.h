@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "tiles.h"
+
 namespace orr {
 
 struct Geom3D;
@@ -56,6 +58,18 @@ struct Ops3D {
     uint32_t (*staged_smem)(uint32_t block, uint32_t npt, uint32_t stages);
     // Registers per thread of the persistent step.
     int (*staged_registers)(bool smag, uint32_t block, uint32_t npt);
+    // Persistent tiled step of one flat lattice (tiled3d.cuh): `host_one` a
+    // host copy of its Lattice3D entry (passed by value), `maps` its tensor
+    // maps, `tg` its tile numbering for tiles of `rows` rows and `block`
+    // consumer threads (rows 8 with 512 threads, or rows 4 with 256), `grid`
+    // CTAs, `stages` pipeline stages, source buffer f[parity ^ flip].
+    cudaError_t (*tiled)(const void* host_one, const TileMaps& maps, const TileGrid& tg, uint32_t flip,
+                         uint32_t stages, bool smag, uint32_t rows, uint32_t block, uint32_t grid, uint32_t* status,
+                         cudaStream_t s);
+    // Resident CTAs per SM of the tiled step (0: cannot launch) and its
+    // registers per thread.
+    int (*tiled_occupancy)(bool smag, uint32_t rows, uint32_t block, uint32_t stages);
+    int (*tiled_registers)(bool smag, uint32_t rows, uint32_t block);
     // Momentum exchange of n lattices (device table of ForceJob, kernels3d.cuh)
     // summed in a fixed order: pass 1 over `chunks` link chunks into
     // `partial` (6 doubles per chunk), pass 2 into out[6 l ..] (added to it

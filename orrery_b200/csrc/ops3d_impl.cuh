@@ -7,6 +7,7 @@
 #include "kernels3d.cuh"
 #include "ops3d.h"
 #include "staged3d.cuh"
+#include "tiled3d.cuh"
 
 namespace orr {
 
@@ -219,6 +220,55 @@ template <class S> struct Launch3D {
         return regs;
     }
 
+    // Calls f.template operator()<kSmag, R, B>() for a supported tile shape
+    // (rows 8 with 512 consumers, rows 4 with 256); false otherwise.
+    template <class F> static bool with_tile(bool smag, uint32_t rows, uint32_t block, F&& f) {
+        const auto go = [&]<bool K>() {
+            if (rows == 8 && block == 512) { f.template operator()<K, 8, 512>(); return true; }
+            if (rows == 4 && block == 256) { f.template operator()<K, 4, 256>(); return true; }
+            if (rows == 2 && block == 256) { f.template operator()<K, 2, 256>(); return true; }
+            return false;
+        };
+        return smag ? go.template operator()<true>() : go.template operator()<false>();
+    }
+
+    static cudaError_t tiled(const void* host_one, const TileMaps& maps, const TileGrid& tg, uint32_t flip,
+                             uint32_t stages, bool smag, uint32_t rows, uint32_t block, uint32_t grid,
+                             uint32_t* status, cudaStream_t s) {
+        if (stages == 0 || stages > kMaxStages || grid == 0 || host_one == nullptr) {
+            return cudaErrorInvalidValue;
+        }
+        const auto& one = *static_cast<const Lattice3D<A>*>(host_one);
+        const bool ok = with_tile(smag, rows, block, [&]<bool K, int R, int B>() {
+            step3d_tiled_kernel<S, K, R, B><<<grid, kTiledThreads<B>, tiled_smem_bytes<S, R>(stages), s>>>(
+                one, maps, tg, flip, stages, status);
+        });
+        return ok ? cudaGetLastError() : cudaErrorInvalidValue;
+    }
+
+    static int tiled_occupancy(bool smag, uint32_t rows, uint32_t block, uint32_t stages) {
+        if (stages == 0 || stages > kMaxStages) {
+            return 0;
+        }
+        int result = 0;
+        with_tile(smag, rows, block, [&]<bool K, int R, int B>() {
+            result = occupancy_of(&step3d_tiled_kernel<S, K, R, B>, kTiledThreads<B>,
+                                  tiled_smem_bytes<S, R>(stages));
+        });
+        return result;
+    }
+
+    static int tiled_registers(bool smag, uint32_t rows, uint32_t block) {
+        int regs = -1;
+        with_tile(smag, rows, block, [&]<bool K, int R, int B>() {
+            cudaFuncAttributes a{};
+            if (cudaFuncGetAttributes(&a, &step3d_tiled_kernel<S, K, R, B>) == cudaSuccess) {
+                regs = a.numRegs;
+            }
+        });
+        return regs;
+    }
+
     static cudaError_t force_batch(const void* jobs, uint32_t n, uint64_t chunks, double* partial,
                                    double* out, bool accumulate, cudaStream_t s) {
         if (n == 0) {
@@ -235,7 +285,8 @@ template <class S> struct Launch3D {
     static const Ops3D& table() {
         static const Ops3D ops{&step,   &init,   &history,        &moments,          &force,
                                &mass,   &step_registers, &pairs_ok, &staged, &staged_occupancy,
-                               &staged_smem, &staged_registers, &force_batch};
+                               &staged_smem, &staged_registers, &tiled, &tiled_occupancy,
+                               &tiled_registers, &force_batch};
         return ops;
     }
 };

@@ -8,17 +8,23 @@
 //   submit     copies the request (configuration, solid mask, optional
 //              distances and initial fields) into a FIFO queue; returns at
 //              once with an id.
-//   worker     one thread per server.  Each round it launches a chunk of
-//              `chunk_steps` steps of every active lattice as one batch
-//              (batch3d.cu; the force sampled every `sample_every` steps by
-//              the fixed-order batched reduction), and while the device
-//              runs it admits queued requests in arrival order as long as a
-//              slot is free and the admitted lattices' device memory stays
-//              within the budget: planning, allocation, upload and
-//              initialisation of the new solvers overlap the chunk.  At the
-//              chunk's end it reads the force sums, updates each solve's
-//              window means, retires the solves that are done (freeing
-//              their memory) and adds the admitted ones to the batch.
+//   device     a device-resident loop (serve_loop.cuh): one launch of the
+//   loop       serving graph is a conditional while-loop over sampling
+//              periods of all admitted lattices as one batch (batch3d.cu:
+//              `sample_every` steps of every member, then the fixed-order
+//              batched force sample), and a kernel that keeps each solve's
+//              slot on the device: window means, the convergence rule, the
+//              gradual start.  The loop ends by itself after the period in
+//              which a solve finished, when the host asks (new solves wait
+//              to join), or after kMaxPeriods periods.
+//   worker     one thread per server.  It launches the loop and, while the
+//              device runs it, admits queued requests in arrival order as
+//              long as a slot is free and the admitted lattices' device
+//              memory stays within the budget: planning, allocation, upload
+//              and initialisation of the new solvers overlap the loop.  When
+//              the loop ends it reads the slot table back once, retires the
+//              solves that are done (freeing their memory), adds the
+//              admitted ones to the batch and launches the loop again.
 //   done       a solve is done when the mean drag coefficient of its last
 //              window of `window` steps differs from the previous window's
 //              by less than `tolerance` (converged), when it reaches
@@ -43,6 +49,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numbers>
 #include <string>
 #include <thread>
 #include <vector>
@@ -50,7 +57,9 @@
 #include "batch3d_state.cuh"
 #include "common.h"
 #include "plan.h"
+#include "serve_loop.cuh"
 #include "solver3d_state.cuh"
+#include "trace.h"
 
 namespace {
 
@@ -83,13 +92,13 @@ struct Active {
     std::shared_ptr<Request> req;
     orr_lbm3d* solver = nullptr;
     uint64_t bytes = 0;
-    uint64_t steps = 0;
-    uint64_t window_steps = 0;
-    double window_sum[6] = {0, 0, 0, 0, 0, 0};
-    uint64_t window_samples = 0;
-    bool have_previous = false;
-    double previous_cd = 0.0;
+    ServeSlot slot{};        // host copy of its slot, as of the last read-back
+    void* ramp = nullptr;    // device table of its gradual start (owned), or null
 };
+
+// Sampling periods a launch of the serving loop runs at most before the host
+// looks again (when no solve finishes and none waits to join).
+constexpr uint32_t kMaxPeriods = 1000;
 
 double seconds_since(Clock::time_point t0) {
     return std::chrono::duration<double>(Clock::now() - t0).count();
@@ -144,9 +153,11 @@ struct orr_server {
         for (auto* list : {&active, &joining}) {
             for (Active& a : *list) {
                 if (a.solver) orr_lbm3d_destroy(a.solver);
+                if (a.ramp) cudaFree(a.ramp);
             }
             list->clear();
         }
+        release_loop();
         if (batch) {
             orr_batch3d_destroy(batch);
             batch = nullptr;
@@ -158,7 +169,7 @@ struct orr_server {
         std::lock_guard<std::mutex> lock(mu);
         orr_solve_result& r = records[a.req->id].result;
         r.state = state;
-        r.steps = a.steps;
+        r.steps = a.slot.steps;
         r.cd = cd;
         r.cl = cl;
         r.cm = cm;
@@ -202,15 +213,39 @@ struct orr_server {
                                       q->fields.data() + 3 * n);
             if (st != ORR_OK) why = orr_lbm3d_last_error(s);
         }
+        void* ramp = nullptr;
+        uint32_t ramp_count = 0;
         if (st == ORR_OK && q->ramp_steps > 0.0) {
-            // Gradual start: at rest, the inlet velocity planned by the batch
-            // before every sampling interval.
+            // Gradual start: at rest, then the inlet velocity of each
+            // sampling interval from a table planned here with the reference
+            // adapter's rule (LbmAeroSolver3D::step, lbm_aero_solver3d.cpp:
+            // 398-412: the fraction (1 - cos(pi s / T)) / 2 of the interval's
+            // first step s, in binary64, rounded as an inlet upload rounds);
+            // its last entry is the full velocity.
             try {
                 initialize_at_rest(s);
-                s->ramp_steps = q->ramp_steps;
-                s->ramp_u[0] = q->config.inlet_ux;
-                s->ramp_u[1] = q->config.inlet_uy;
-                s->ramp_u[2] = q->config.inlet_uz;
+                const double every = static_cast<double>(opt.sample_every);
+                ramp_count = static_cast<uint32_t>(std::ceil(q->ramp_steps / every));
+                const std::size_t ab = s->abytes;
+                std::vector<unsigned char> table((ramp_count + 1u) * 3u * ab);
+                for (uint32_t j = 0; j <= ramp_count; ++j) {
+                    const double start = static_cast<double>(j) * every;
+                    const double fraction =
+                        start >= q->ramp_steps ? 1.0 : 0.5 * (1.0 - std::cos(std::numbers::pi * start / q->ramp_steps));
+                    const double u[3] = {q->config.inlet_ux, q->config.inlet_uy, q->config.inlet_uz};
+                    for (int d = 0; d < 3; ++d) {
+                        const double v = fraction * u[d];
+                        unsigned char* at = table.data() + (3u * j + static_cast<uint32_t>(d)) * ab;
+                        if (ab == sizeof(double)) {
+                            std::memcpy(at, &v, sizeof v);
+                        } else {
+                            const float f = to_f32(v);
+                            std::memcpy(at, &f, sizeof f);
+                        }
+                    }
+                }
+                check(cudaMalloc(&ramp, table.size()), "serve: ramp table");
+                check(cudaMemcpy(ramp, table.data(), table.size(), cudaMemcpyHostToDevice), "serve: ramp table");
             } catch (const Refusal& r) {
                 st = r.status;
                 why = r.text;
@@ -220,6 +255,7 @@ struct orr_server {
             }
         }
         if (st != ORR_OK) {
+            if (ramp) cudaFree(ramp);
             if (s) orr_lbm3d_destroy(s);
             Active none;
             none.req = q;
@@ -228,6 +264,23 @@ struct orr_server {
         }
         a.req = q;
         a.solver = s;
+        a.ramp = ramp;
+        // The slot (set_coefficients, aero_result.h:92: Cd = Fx / (1/2 rho U^2 A)).
+        ServeSlot& slot = a.slot;
+        slot = ServeSlot{};
+        const double u = q->config.inlet_ux;
+        slot.qa = 0.5 * u * u * q->area;
+        slot.length = q->length;
+        slot.centre[0] = q->centre[0];
+        slot.centre[1] = q->centre[1];
+        slot.tolerance = q->tolerance;
+        slot.window = q->window;
+        slot.max_steps = q->max_steps;
+        slot.mode = q->mode;
+        slot.ramp_count = ramp_count;
+        slot.ramp = ramp;
+        slot.inlet = s->inlet_dev();
+        slot.state = ORR_SOLVE_RUNNING;
         const std::size_t slots = s->plan.wall_q.size() / d3::Q;
         a.bytes = memory3d(q->config, s->plan.link_cell.size(), slots, opt.storage).value_or(q->estimate);
         {
@@ -281,61 +334,127 @@ struct orr_server {
         }
     }
 
-    // Window bookkeeping after a chunk; returns true when the solve is done.
-    bool update(Active& a, const double* sums, uint64_t samples, uint64_t steps) {
-        const Request& q = *a.req;
-        const uint64_t chunk_first = a.steps;
-        a.steps += steps;
-        // A fixed-steps solve sums only its last window (whose first step is
-        // a chunk boundary).
-        const bool counted = q.mode != ORR_RUN_FIXED_STEPS || chunk_first >= q.max_steps - q.window;
-        if (counted) {
-            a.window_steps += steps;
-            for (int v = 0; v < 6; ++v) a.window_sum[v] += sums[v];
-            a.window_samples += samples;
-        }
-        bool finite = true;
-        for (int v = 0; v < 6; ++v) finite = finite && std::isfinite(sums[v]);
-        if (!finite) {
+    // Records the result of a slot that is done and releases its solve.
+    void retire(Active& a) {
+        const ServeSlot& sl = a.slot;
+        if (sl.state == ORR_SOLVE_FAILED) {
             // The reference adapter's warning for the same event
             // (lbm_aero_solver3d.cpp:585-588).
             finish(a, ORR_SOLVE_FAILED, 0, 0, 0, 0, nullptr,
                    "lbm.diverged: the lattice state is no longer finite (numerical instability)");
-            return true;
+        } else {
+            finish(a, sl.state, sl.cd, sl.cl, sl.cm, sl.delta, sl.mean,
+                   sl.state == ORR_SOLVE_CAPPED ? "serve: step cap reached before convergence" : "");
         }
-        if (q.mode == ORR_RUN_FIXED_STEPS && a.steps < q.max_steps) {
-            return false;
+        orr_batch3d_remove(batch, a.solver);
+        orr_lbm3d_destroy(a.solver);
+        a.solver = nullptr;
+        if (a.ramp) {
+            cudaFree(a.ramp);
+            a.ramp = nullptr;
         }
-        if (a.window_steps < q.window) {
-            return false;
+        used_bytes -= a.bytes;
+    }
+
+    // ---- the serving graph: a conditional while-loop over sampling periods
+
+    cudaGraphExec_t loop_exec = nullptr;
+    ServeSlot* slots_dev = nullptr;
+    std::size_t slots_cap = 0;
+    uint32_t* counters_dev = nullptr;
+    uint32_t* flag_host = nullptr;   // mapped, pinned: the host asks the loop to end
+    uint32_t* flag_dev = nullptr;
+    cudaEvent_t loop_done = nullptr;
+    bool loop_stale = true;
+    std::vector<ServeSlot> slots_host;
+
+    void release_loop() noexcept {
+        if (loop_exec) cudaGraphExecDestroy(loop_exec);
+        loop_exec = nullptr;
+        if (slots_dev) cudaFree(slots_dev);
+        slots_dev = nullptr;
+        slots_cap = 0;
+        if (counters_dev) cudaFree(counters_dev);
+        counters_dev = nullptr;
+        if (flag_host) cudaFreeHost(flag_host);
+        flag_host = flag_dev = nullptr;
+        if (loop_done) cudaEventDestroy(loop_done);
+        loop_done = nullptr;
+    }
+
+    // Captures the loop for the current members: its body is one sampling
+    // period of the batch (the members' steps, the force sample) and
+    // serve_period_kernel, which ends the loop.
+    void build_loop() {
+        if (counters_dev == nullptr) {
+            check(cudaMalloc(reinterpret_cast<void**>(&counters_dev), kServeCounters * sizeof(uint32_t)),
+                  "serve: counters");
+            check(cudaHostAlloc(reinterpret_cast<void**>(&flag_host), sizeof(uint32_t), cudaHostAllocMapped),
+                  "serve: flag");
+            check(cudaHostGetDevicePointer(reinterpret_cast<void**>(&flag_dev), flag_host, 0), "serve: flag");
+            check(cudaEventCreateWithFlags(&loop_done, cudaEventDisableTiming), "serve: event");
         }
-        double mean[6];
-        for (int v = 0; v < 6; ++v) mean[v] = a.window_sum[v] / static_cast<double>(a.window_samples);
-        // Coefficients (set_coefficients, aero_result.h:92; moment about the
-        // centre, lbm_aero_solver3d.cpp:428-431).
-        const double u = q.config.inlet_ux;
-        const double qa = 0.5 * u * u * q.area;
-        const double mz = mean[5] - (q.centre[0] * mean[1] - q.centre[1] * mean[0]);
-        const double cd = mean[0] / qa, cl = mean[1] / qa, cm = mz / (qa * q.length);
-        if (q.mode == ORR_RUN_FIXED_STEPS) {
-            finish(a, ORR_SOLVE_COMPLETED, cd, cl, cm, 0.0, mean, "");
-            return true;
+        const std::size_t n = active.size();
+        if (n > slots_cap) {
+            if (slots_dev) cudaFree(slots_dev);
+            slots_dev = nullptr;
+            check(cudaMalloc(reinterpret_cast<void**>(&slots_dev), n * sizeof(ServeSlot)), "serve: slot table");
+            slots_cap = n;
         }
-        const double delta = a.have_previous ? std::abs(cd - a.previous_cd) : INFINITY;
-        a.have_previous = true;
-        a.previous_cd = cd;
-        a.window_steps = 0;
-        a.window_samples = 0;
-        std::fill(std::begin(a.window_sum), std::end(a.window_sum), 0.0);
-        if (delta < q.tolerance) {
-            finish(a, ORR_SOLVE_CONVERGED, cd, cl, cm, delta, mean, "");
-            return true;
+        batch->prepare_loop(opt.sample_every);
+        if (loop_exec) {
+            cudaGraphExecDestroy(loop_exec);
+            loop_exec = nullptr;
         }
-        if (a.steps >= q.max_steps) {
-            finish(a, ORR_SOLVE_CAPPED, cd, cl, cm, delta, mean, "serve: step cap reached before convergence");
-            return true;
+        cudaGraph_t graph = nullptr;
+        check(cudaGraphCreate(&graph, 0), "serve: loop graph");
+        try {
+            cudaGraphConditionalHandle handle{};
+            check(cudaGraphConditionalHandleCreate(&handle, graph, 1u, cudaGraphCondAssignDefault),
+                  "serve: loop condition");
+            cudaGraphNodeParams params{};
+            params.type = cudaGraphNodeTypeConditional;
+            params.conditional.handle = handle;
+            params.conditional.type = cudaGraphCondTypeWhile;
+            params.conditional.size = 1;
+            cudaGraphNode_t node = nullptr;
+            check(cudaGraphAddNode(&node, graph, nullptr, 0, &params), "serve: loop node");
+            cudaGraph_t body = params.conditional.phGraph_out[0];
+            check(cudaStreamBeginCaptureToGraph(batch->stream, body, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal),
+                  "serve: loop capture");
+            const uint64_t before = batch->launches;
+            try {
+                batch->launch_steps(opt.sample_every);
+                batch->launch_sample(false);
+                check(launch_period(handle, static_cast<uint32_t>(n)), "serve: period kernel");
+            } catch (...) {
+                cudaGraph_t dropped = nullptr;
+                cudaStreamEndCapture(batch->stream, &dropped);
+                batch->launches = before;
+                throw;
+            }
+            batch->launches = before;
+            cudaGraph_t captured = nullptr;
+            check(cudaStreamEndCapture(batch->stream, &captured), "serve: loop capture");
+            check(cudaGraphInstantiate(&loop_exec, graph, 0), "serve: loop instantiate");
+        } catch (...) {
+            cudaGraphDestroy(graph);
+            throw;
         }
-        return false;
+        cudaGraphDestroy(graph);
+        loop_stale = false;
+    }
+
+    cudaError_t launch_period(cudaGraphConditionalHandle handle, uint32_t n) {
+        if (opt.storage == ORR_STORAGE_F64) {
+            serve_period_kernel<double><<<1, 256, 0, batch->stream>>>(slots_dev, n, batch->sums, opt.sample_every,
+                                                                      kMaxPeriods, flag_dev, counters_dev, handle);
+        } else {
+            serve_period_kernel<float><<<1, 256, 0, batch->stream>>>(slots_dev, n, batch->sums, opt.sample_every,
+                                                                     kMaxPeriods, flag_dev, counters_dev, handle);
+        }
+        return cudaGetLastError();
     }
 
     static void check_status(orr_status st, const char* what) {
@@ -360,7 +479,7 @@ struct orr_server {
             if (orr_batch3d_set_schedule(batch, &sched) != ORR_OK) {
                 throw Refusal{ORR_ERR_INVALID, orr_batch3d_last_error(batch)};
             }
-            std::vector<double> sums;
+            uint32_t counters[kServeCounters] = {0, 0};
             for (;;) {
                 {
                     std::unique_lock<std::mutex> lock(mu);
@@ -369,50 +488,98 @@ struct orr_server {
                         return;
                     }
                 }
-                // New solvers join at chunk boundaries, in admission order.
+                // New solvers join between launches, in admission order.
                 for (Active& a : joining) {
                     if (orr_batch3d_add(batch, a.solver) != ORR_OK) {
                         throw Refusal{ORR_ERR_STATE, orr_batch3d_last_error(batch)};
                     }
                     active.push_back(a);
+                    loop_stale = true;
                 }
                 joining.clear();
-                const auto chunk_start = Clock::now();
-                if (!active.empty()) {
-                    batch->run(opt.chunk_steps, opt.sample_every);
-                }
-                // Admission overlaps the chunk on the device.
-                admit();
                 if (active.empty()) {
+                    orr::Zone zone("serve_admit");
+                    admit();
                     continue;
                 }
-                sums.assign(active.size() * 6, 0.0);
-                check(cudaMemcpyAsync(sums.data(), batch->sums, sums.size() * sizeof(double),
-                                      cudaMemcpyDeviceToHost, batch->stream),
-                      "serve: force sums");
-                check(cudaStreamSynchronize(batch->stream), "serve: chunk");
+                if (loop_stale) {
+                    build_loop();
+                }
+                // The slot table in member order, then the loop.
+                const std::size_t n = active.size();
+                slots_host.resize(n);
+                for (std::size_t k = 0; k < n; ++k) slots_host[k] = active[k].slot;
+                check(cudaMemcpyAsync(slots_dev, slots_host.data(), n * sizeof(ServeSlot), cudaMemcpyHostToDevice,
+                                      batch->stream),
+                      "serve: slot table");
+                check(cudaMemsetAsync(counters_dev, 0, kServeCounters * sizeof(uint32_t), batch->stream),
+                      "serve: counters");
+                *reinterpret_cast<volatile uint32_t*>(flag_host) = 0u;
+                const auto launch_start = Clock::now();
+                {
+                    orr::Zone zone("serve_loop");
+                    batch->wait_members();
+                    check(cudaGraphLaunch(loop_exec, batch->stream), "serve: loop launch");
+                    check(cudaEventRecord(loop_done, batch->stream), "serve: loop event");
+                }
+                // While the loop runs on the device, admit queued requests;
+                // once one is ready to join, ask the loop to end after its
+                // current period.  Every period ends (bounded waits inside
+                // the step kernels), and the loop after at most kMaxPeriods.
+                for (;;) {
+                    {
+                        orr::Zone zone("serve_admit");
+                        admit();
+                    }
+                    bool ask = !joining.empty();
+                    {
+                        std::lock_guard<std::mutex> lock(mu);
+                        ask = ask || stop;
+                    }
+                    if (ask) {
+                        *reinterpret_cast<volatile uint32_t*>(flag_host) = 1u;
+                    }
+                    const cudaError_t q = cudaEventQuery(loop_done);
+                    if (q == cudaSuccess) {
+                        break;
+                    }
+                    if (q != cudaErrorNotReady) {
+                        check(q, "serve: loop");
+                    }
+                    std::unique_lock<std::mutex> lock(mu);
+                    cv.wait_for(lock, std::chrono::microseconds(200), [&] { return stop; });
+                }
+                check(cudaMemcpyAsync(slots_host.data(), slots_dev, n * sizeof(ServeSlot), cudaMemcpyDeviceToHost,
+                                      batch->stream),
+                      "serve: slot table");
+                check(cudaMemcpyAsync(counters, counters_dev, sizeof counters, cudaMemcpyDeviceToHost,
+                                      batch->stream),
+                      "serve: counters");
+                check(cudaStreamSynchronize(batch->stream), "serve: loop");
+                batch->finish_loop(static_cast<uint64_t>(counters[0]) * opt.sample_every);
                 batch->check_status();
-                const double busy = std::chrono::duration<double>(Clock::now() - chunk_start).count();
+                const double busy = std::chrono::duration<double>(Clock::now() - launch_start).count();
                 double updates = 0.0;
-                for (const Active& a : active) updates += static_cast<double>(a.solver->g.cells) * opt.chunk_steps;
+                for (const Active& a : active) {
+                    updates += static_cast<double>(a.solver->g.cells) * opt.sample_every * counters[0];
+                }
                 {
                     std::lock_guard<std::mutex> lock(mu);
-                    ++chunks;
+                    chunks += counters[0];
                     busy_seconds += busy;
                     lattice_updates += updates;
-                    active_sum += static_cast<double>(active.size());
+                    active_sum += static_cast<double>(n) * counters[0];
                 }
-                // Members sit in the batch in the order of `active`.
+                // Retire the slots that are done; members sit in the batch in
+                // the order of `active`.
                 std::vector<Active> keep;
-                keep.reserve(active.size());
-                const uint64_t samples = opt.chunk_steps / opt.sample_every;
-                for (std::size_t k = 0; k < active.size(); ++k) {
+                keep.reserve(n);
+                for (std::size_t k = 0; k < n; ++k) {
                     Active& a = active[k];
-                    if (update(a, sums.data() + 6 * k, samples, opt.chunk_steps)) {
-                        orr_batch3d_remove(batch, a.solver);
-                        orr_lbm3d_destroy(a.solver);
-                        a.solver = nullptr;
-                        used_bytes -= a.bytes;
+                    a.slot = slots_host[k];
+                    if (a.slot.state != ORR_SOLVE_RUNNING) {
+                        retire(a);
+                        loop_stale = true;
                     } else {
                         keep.push_back(a);
                     }

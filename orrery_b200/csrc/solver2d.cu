@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.h"
+#include "trace.h"
 #include "kernels2d.cuh"
 #include "lattice.h"
 #include "ops2d.h"
@@ -329,6 +330,7 @@ orr_status orr_lbm2d_initialize(orr_lbm2d* solver, const double* rho, const doub
 }
 
 orr_status orr_lbm2d_step(orr_lbm2d* solver, uint64_t count) {
+    orr::Zone zone("lbm_step");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         handle2_of(solver)->run(count);
         return ORR_OK;

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.h"
+#include "trace.h"
 #include "host_copy.h"
 #include "kernels3d.cuh"
 #include "lattice.h"
@@ -194,6 +195,7 @@ orr_status orr_lbm3d_plan(const orr_lbm3d_config* config, const uint8_t* solid,
 orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid,
                             const double* distance, const orr_solver_options* options,
                             orr_lbm3d** out) {
+    orr::Zone zone("lbm_create");
     if (out == nullptr) {
         return orr::fail(ORR_ERR_INVALID, "null output handle");
     }
@@ -209,10 +211,12 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             !problem.empty()) {
             throw Refusal{ORR_ERR_INVALID, problem};
         }
-        if (o.block_x < 0 || o.block_x > 256 || (o.block_x % 32) != 0) {
-            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: block_x must be 0 or a multiple of 32 up to 256"};
+        const bool tiled_block = o.kernel == ORR_KERNEL_TILED && (o.block_x == 256 || o.block_x == 512);
+        if (!tiled_block && (o.block_x < 0 || o.block_x > 256 || (o.block_x % 32) != 0)) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: block_x must be 0 or a multiple of 32 up to 256 "
+                                           "(256 or 512 consumer threads for the tiled step)"};
         }
-        if (o.kernel < ORR_KERNEL_AUTO || o.kernel > ORR_KERNEL_STAGED) {
+        if (o.kernel < ORR_KERNEL_AUTO || o.kernel > ORR_KERNEL_TILED) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: unknown step kernel"};
         }
         if (o.kernel == ORR_KERNEL_STAGED && o.block_x != 0 && o.block_x != 128 && o.block_x != 256) {
@@ -232,7 +236,7 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
         // Default row tile: 256 nodes for binary32 storage when they divide
         // the rows (the row step is memory bound there and longer tiles read
         // a little faster), else 128.
-        h->block = o.block_x > 0 ? static_cast<uint32_t>(o.block_x)
+        h->block = o.block_x > 0 && o.block_x <= 256 ? static_cast<uint32_t>(o.block_x)
                    : (o.storage == ORR_STORAGE_F32 && config->nx % 256 == 0) ? 256u
                                                                               : kDefaultBlock;
         h->ops = &ops_for(o.storage);
@@ -390,9 +394,41 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step needs periodic or free-slip sides "
                                            "and halfway walls"};
         }
-        const bool want = o.kernel == ORR_KERNEL_STAGED ||
-                          (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && g.flat && stageable(g) &&
-                           (o.block_x == 0 || o.block_x == 128 || o.block_x == 256));
+        if (o.kernel == ORR_KERNEL_TILED && !tileable(g)) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the tiled step needs periodic or free-slip sides, "
+                                           "halfway walls and rows of a multiple of 16 nodes"};
+        }
+        // The tiled step: when asked for (512 consumer threads and tiles of
+        // 8 rows, or 256 and 4).
+        if (o.kernel == ORR_KERNEL_TILED) {
+            const uint32_t tblock = o.block_x == 256 ? 256u : 512u;
+            // Rows per tile: two nodes per consumer thread (the default), or
+            // one with nodes_per_thread 1.
+            const uint32_t rows = tblock * (o.nodes_per_thread == 1 ? 1u : 2u) / kTileW;
+            h->shape = tiled_shape(*h->ops, h->smag, rows, tblock, static_cast<uint32_t>(o.stages), o.device);
+            if (h->shape.per_sm <= 0) {
+                throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the tiled step cannot launch with " +
+                                                   std::to_string(h->shape.stages) + " stages"};
+            }
+            if (std::string why = encode_tile_maps(h->tmaps, g, h->f[0], h->f[1], h->cls, h->sbytes, rows);
+                !why.empty()) {
+                throw Refusal{ORR_ERR_CUDA, "lbm3d gpu: " + why};
+            }
+            h->tiled = true;
+            h->tile_rows = rows;
+            if (binary32) {
+                h->upload_table(h->phys32);
+            } else {
+                h->upload_table(h->phys64);
+            }
+            h->tgrid = tile_grid(g, rows, tblock);
+            const uint64_t most = std::max<uint64_t>({h->tgrid.tiles, h->tgrid.direct, 1});
+            h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
+        }
+        const bool want = !h->tiled &&
+                          (o.kernel == ORR_KERNEL_STAGED ||
+                           (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && g.flat && stageable(g) &&
+                            (o.block_x == 0 || o.block_x == 128 || o.block_x == 256)));
         if (want) {
             const uint32_t sblock = o.block_x == 128 ? 128u : 256u;
             const uint32_t npt = o.nodes_per_thread > 0 ? static_cast<uint32_t>(o.nodes_per_thread)
@@ -415,7 +451,7 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
                 h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
             }
         }
-        if (!h->persistent && o.nodes_per_thread == 2) {
+        if (!h->persistent && !h->tiled && o.nodes_per_thread == 2) {
             // Row-tile step with two neighbouring nodes per thread.
             if (!h->ops->pairs_ok(g, h->block)) {
                 throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: two nodes per thread of the row step need 2-byte "
@@ -455,6 +491,7 @@ const char* orr_lbm3d_last_error(const orr_lbm3d* solver) {
 
 orr_status orr_lbm3d_initialize(orr_lbm3d* solver, const double* rho, const double* ux,
                                 const double* uy, const double* uz) {
+    orr::Zone zone("lbm_initialize");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
         const bool any = rho || ux || uy || uz;
@@ -469,6 +506,7 @@ orr_status orr_lbm3d_initialize(orr_lbm3d* solver, const double* rho, const doub
 }
 
 orr_status orr_lbm3d_step(orr_lbm3d* solver, uint64_t count) {
+    orr::Zone zone("lbm_step");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
         if (h->batch != nullptr) {
@@ -511,6 +549,7 @@ orr_status orr_lbm3d_inlet_velocity(const orr_lbm3d* solver, double velocity[3])
 }
 
 orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
+    orr::Zone zone("lbm_force");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
         if (force_moment == nullptr) {
@@ -525,11 +564,12 @@ orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
         // One read-back: the six sums (64 bytes into the small buffer) and,
         // for the persistent step, its status word (kStatusOffset).
         static_assert(kStatusOffset >= 64 + 6 * sizeof(double) && kStatusOffset + 4 <= 64 + 192);
-        const std::size_t bytes = h->persistent ? kStatusOffset + 4 - 64 : 6 * sizeof(double);
+        const bool watched = h->persistent || h->tiled;
+        const std::size_t bytes = watched ? kStatusOffset + 4 - 64 : 6 * sizeof(double);
         check(cudaMemcpyAsync(h->host_small + 8, h->acc(), bytes, cudaMemcpyDeviceToHost, h->stream),
               "force read-back");
         check(cudaStreamSynchronize(h->stream), "force read-back");
-        if (h->persistent) {
+        if (watched) {
             uint32_t word = 0;
             std::memcpy(&word, reinterpret_cast<const char*>(h->host_small + 8) + (kStatusOffset - 64), 4);
             orr_lbm3d::raise_status(word);
@@ -555,6 +595,7 @@ __global__ void widen_moments_kernel(const float* __restrict__ m, double* __rest
 
 orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, double* uy,
                                  double* uz) {
+    orr::Zone zone("lbm_macroscopic");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
         h->check_status();
@@ -589,6 +630,7 @@ orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, dou
 }
 
 orr_status orr_lbm3d_populations(orr_lbm3d* solver, double* f) {
+    orr::Zone zone("lbm_populations");
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
         if (f == nullptr) {
@@ -699,7 +741,18 @@ orr_status orr_lbm3d_kernel_info(const orr_lbm3d* solver, orr_kernel_info* info)
     return orr::guarded(nullptr, [&]() -> orr_status {
         check(cudaSetDevice(solver->device), "cudaSetDevice");
         orr_kernel_info k{};
-        if (solver->persistent) {
+        if (solver->tiled) {
+            k.kernel = ORR_KERNEL_TILED;
+            k.block = solver->shape.block;
+            k.stages = solver->shape.stages;
+            k.grid = solver->shape.grid;
+            k.ctas_per_sm = solver->shape.per_sm;
+            k.registers = solver->ops->tiled_registers(solver->smag, solver->tile_rows, solver->shape.block);
+            k.shared_bytes = 0;
+            k.nodes_per_thread = solver->shape.npt;
+            k.staged_items = solver->tgrid.tiles;
+            k.direct_items = solver->tgrid.direct;
+        } else if (solver->persistent) {
             k.kernel = ORR_KERNEL_STAGED;
             k.block = solver->shape.block;
             k.stages = solver->shape.stages;
@@ -734,10 +787,10 @@ orr_status orr_lbm3d_launch_count(const orr_lbm3d* solver, uint64_t* launches) {
 orr_status orr_lbm3d_request_stall(orr_lbm3d* solver, uint32_t cta) {
     return orr::guarded(solver ? &solver->error : nullptr, [&]() -> orr_status {
         orr_lbm3d* h = handle_of(solver);
-        if (!h->persistent) {
-            throw Refusal{ORR_ERR_INVALID, "lbm3d: a stall request needs the staged step"};
+        if (!h->persistent && !h->tiled) {
+            throw Refusal{ORR_ERR_INVALID, "lbm3d: a stall request needs the staged or tiled step"};
         }
-        const uint64_t ctas = std::min<uint64_t>(h->shape.grid, h->items.staged);
+        const uint64_t ctas = std::min<uint64_t>(h->shape.grid, h->tiled ? h->tgrid.tiles : h->items.staged);
         if (cta >= ctas) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d: the stall request names a CTA without staged spans"};
         }

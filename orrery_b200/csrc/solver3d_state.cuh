@@ -114,6 +114,10 @@ struct orr_lbm3d {
     void* f[2] = {nullptr, nullptr};
     int cur = 0;
     bool persistent = false;  // the staged persistent step runs the steps
+    bool tiled = false;       // the tiled step runs the steps (shape as the staged one's)
+    TileMaps tmaps{};
+    TileGrid tgrid{};
+    uint32_t tile_rows = 8;
     StagedShape shape{};
     ItemCounts items{};
     void* table = nullptr;
@@ -133,11 +137,6 @@ struct orr_lbm3d {
     uint64_t steps = 0;
     uint64_t launches = 0;
     double inlet[3] = {0.0, 0.0, 0.0};
-    // Gradual start applied by a batch's sampled runs (served drag solves):
-    // ramp_steps > 0 sets the inlet velocity to ramp_u times the ramp
-    // fraction before every sampling interval.
-    double ramp_steps = 0.0;
-    double ramp_u[3] = {0.0, 0.0, 0.0};
     std::string error;
 
     const void* phys() const {
@@ -211,7 +210,11 @@ struct orr_lbm3d {
 
     // One step src -> dst on `stream` (one kernel launch).
     void launch_step(int from) {
-        if (persistent) {
+        if (tiled) {
+            check(ops->tiled(host_table, tmaps, tgrid, static_cast<uint32_t>(from), shape.stages, smag, tile_rows,
+                             shape.block, shape.grid, status(), stream),
+                  "step kernel");
+        } else if (persistent) {
             check(ops->staged(host_table, table, 1, items.staged, items.direct, static_cast<uint32_t>(from),
                               shape.stages, smag, shape.block, shape.npt, shape.grid, status(), stream),
                   "step kernel");
@@ -225,7 +228,7 @@ struct orr_lbm3d {
     // The persistent step's status word (a wait that timed out makes the
     // populations invalid until the next initialize).
     void check_status() {
-        if (!persistent) {
+        if (!persistent && !tiled) {
             return;
         }
         uint32_t* word = reinterpret_cast<uint32_t*>(host_small + 30);

@@ -74,17 +74,25 @@ def test_members_equal_alone(storage, schedule):
         assert np.array_equal(a.populations(), b.populations())
 
 
-def test_sampled_forces_alone_and_in_mix():
-    """Fixed-order force sums: a lattice alone and in a mix of four agree bit for bit."""
-    mixed = solvers("f32")
+@pytest.mark.parametrize("general", [False, True], ids=["halfway", "interpolated"])
+def test_sampled_forces_alone_and_in_mix(general):
+    """Fixed-order force sums: a lattice alone and in a mix of four agree bit
+    for bit (with `general`, one member has an interpolated wall: links with
+    q != 1/2)."""
+    rows = ("rows", 128, 0, 0, 0)
+    mixed = solvers("f32", general)
     batch = CudaBatch3D()
     for s in mixed:
         batch.add(s)
+    if general:
+        batch.set_schedule(*rows)
     sums_mix = batch.step_sampled(100, 10)
-    for k, (c, m) in enumerate(lattices()):
+    for k, (c, m) in enumerate(lattices(general)):
         solo = S.make_gpu_solver(c, m, storage="f32")
         b1 = CudaBatch3D()
         b1.add(solo)
+        if general:
+            b1.set_schedule(*rows)
         sums_solo = b1.step_sampled(100, 10)
         assert np.array_equal(sums_solo[0], sums_mix[k])
         # and the same populations

@@ -1,7 +1,8 @@
 """Failure detection made to fire, without a GPU fault.
 
-* The staged step's bounded mbarrier waits: a stall request makes one CTA
-  withhold the copies of its first span (a copy that never lands); its
+* The staged and tiled steps' bounded mbarrier waits: a stall request makes
+  one CTA withhold the copies of its first span or tile (a copy that never
+  lands); its
   consumers' bounded wait must give up, the launch must end, and every
   read-back must report ORR_ERR_TIMEOUT until initialize, after which the
   solver steps and reads back exactly like a fresh one.
@@ -30,10 +31,11 @@ def small(seed, nx=64, ny=32, nz=32, reynolds=60.0):
     return W.sphere3d(seed=seed, nx=nx, ny=ny, nz=nz, diameter=8.0, reynolds=reynolds)
 
 
-def test_staged_wait_runs_out_and_is_reported():
+@pytest.mark.parametrize("kernel", ["staged", "tiled"])
+def test_staged_wait_runs_out_and_is_reported(kernel):
     w = small(81)
-    s = S.make_gpu_solver(w.config, w.mask, storage="f16", kernel="staged")
-    assert s.kernel_info()["kernel"] == "staged"
+    s = S.make_gpu_solver(w.config, w.mask, storage="f16", kernel=kernel)
+    assert s.kernel_info()["kernel"] == kernel
     s.initialize(w.rho, w.ux, w.uy, w.uz)
     s.step(4)
     s.force()
@@ -54,11 +56,13 @@ def test_staged_wait_runs_out_and_is_reported():
         s.populations()
     s.initialize(w.rho, w.ux, w.uy, w.uz)
     s.step(6)
-    fresh = S.make_gpu_solver(w.config, w.mask, storage="f16", kernel="staged")
+    fresh = S.make_gpu_solver(w.config, w.mask, storage="f16", kernel=kernel)
     fresh.initialize(w.rho, w.ux, w.uy, w.uz)
     fresh.step(6)
     assert np.array_equal(s.populations(), fresh.populations())
-    assert np.array_equal(s.force().force, fresh.force().force)
+    # (the binary64 link sum adds with atomics: equal to its last bits' order)
+    fa, fb = s.force().force, fresh.force().force
+    assert np.allclose(fa, fb, rtol=0, atol=1e-12 * np.max(np.abs(fb)))
     # Requests the step cannot take are refused.
     with pytest.raises(LbmError):
         s.request_stall(1 << 30)
