@@ -469,6 +469,62 @@ typedef struct orr_force_links {
  * serialised by the caller.  Blocks until the result is in force_moment. */
 ORR_API orr_status orr_lbm3d_force_static(const orr_force_links* args, double force_moment[6]);
 
+/* ---- The reference's compute-backend kernels --------------------------- */
+
+/* The three D3Q19 kernels the reference's GPU driver, GpuLbm3D, dispatches
+ * through its IComputeBackend (lbm_d3q19_step, lbm_d3q19_moments,
+ * lbm_d3q19_force: src/aero/lbm3d/lbm3d_gpu.cpp:37-44, 158-189, 333-436,
+ * IComputeBackend::dispatch of compute_backend.h:94-129), run on device
+ * buffers in that driver's layout: binary32 populations shifted by their
+ * weights (19 * nx*ny*nz, the layout of ORR_STORAGE_F32), node codes (uint32:
+ * 0 solid, 1 bulk, 2 boundary, 3 + wall slot), 19 binary32 wall fractions per
+ * slot, the convective-outlet history (5 * ny*nz), the moments (rho - 1, ux,
+ * uy, uz planes) and the links (cell, direction pairs).  A CUDA
+ * IComputeBackend (orrery_b200/adapter/compute_backend_cuda.cpp) maps the
+ * driver's dispatches onto these calls.  Population buffers need
+ * orr_gl3d_buffer_slack() bytes of addressable slack before and after them
+ * (the step reads past the lattice at its edges and never uses those values).
+ * Calls are ordered on `stream` (a cudaStream_t; NULL is the legacy stream). */
+typedef struct orr_gl3d_params {   /* the driver's uniforms (lbm3d_gpu.cpp:158-189) */
+    uint32_t nx, ny, nz;           /* u_nx, u_ny, u_nz */
+    uint32_t x_mode;               /* u_x_mode: 1 inflow / outflow, 0 periodic */
+    uint32_t wall_kind[4];         /* u_{y_low,y_high,z_low,z_high}_kind: 0 periodic, 1 slip, 2 no-slip */
+    float wall_ux[4];              /* u_{y_low,y_high,z_low,z_high}_ux */
+    float inlet[3];                /* u_inlet_ux, u_inlet_uy, u_inlet_uz */
+    float tau;                     /* u_tau */
+    float smagorinsky_c2;          /* u_smagorinsky_c2: the closure is on when positive */
+    float force[3];                /* u_force_x, u_force_y, u_force_z */
+    uint32_t outlet_mode;          /* u_outlet_mode: 1 extrapolation, 0 convective */
+    float outlet_speed;            /* u_outlet_speed */
+    float sponge_strength;         /* u_sponge_strength */
+    uint32_t sponge_inlet, sponge_outlet, sponge_sides; /* u_sponge_* */
+    uint32_t link_count;           /* u_link_count */
+} orr_gl3d_params;
+
+typedef struct orr_gl3d orr_gl3d;  /* the tables derived from one node-code buffer */
+
+/* Bytes of slack a population buffer needs before and after it. */
+ORR_API uint64_t orr_gl3d_buffer_slack(void);
+/* Tables for the lattice of `params` whose node codes are `class_codes` (host,
+ * nx*ny*nz values): this library's node classes, bounce-back masks and wall
+ * slots, on `device`.  The lattice is validated as the driver's make_gpu_solver
+ * validates it. */
+ORR_API orr_status orr_gl3d_create(const orr_gl3d_params* params, const uint32_t* class_codes, int32_t device,
+                                   orr_gl3d** out);
+ORR_API void orr_gl3d_destroy(orr_gl3d* tables);
+ORR_API const char* orr_gl3d_last_error(const orr_gl3d* tables);
+/* lbm_d3q19_step: binding 0 (src) -> binding 2 (dst), binding 6 (outlet
+ * history, updated), binding 7 (wall fractions; may be NULL without slots). */
+ORR_API orr_status orr_gl3d_step(orr_gl3d* tables, const orr_gl3d_params* params, const float* src, float* dst,
+                                 float* outlet, const float* wall, void* stream);
+/* lbm_d3q19_moments: binding 0 (src) -> binding 3 (moments). */
+ORR_API orr_status orr_gl3d_moments(orr_gl3d* tables, const orr_gl3d_params* params, const float* src,
+                                    float* moments, void* stream);
+/* lbm_d3q19_force: binding 0 (src), 4 (links), 7 (wall) -> binding 5 (per link
+ * the shifted sum f*_o + f_j; a link outside the lattice gives 0). */
+ORR_API orr_status orr_gl3d_link_force(orr_gl3d* tables, const orr_gl3d_params* params, const float* src,
+                                       const uint32_t* links, float* link_force, const float* wall, void* stream);
+
 /* ---- D2Q9 -------------------------------------------------------------- */
 
 /* validate (lbm2d.h:85-86; lbm2d_common.cpp:31-77) plus the binary32 checks

@@ -55,6 +55,7 @@ def build(reference: str | None = None) -> None:
     if ref is not None:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True, env=env)
         subprocess.run(["make", "-s", "-C", HERE, "adapter", f"REF={ref}"], check=True, env=env)
+        subprocess.run(["make", "-s", "-C", HERE, "backend", f"REF={ref}"], check=True, env=env)
 
 
 def _ptr(a, t):
@@ -716,3 +717,151 @@ def reference_cd_lookup(samples, query, area: float = 1.0):
                                len(q), _ptr(out, _dp), _ptr(clamped, _u8p), msg, 1024) != 0:
         raise ReferenceError_(msg.value.decode())
     return out[:len(q)], clamped[:len(q)].astype(bool)
+
+
+# ---- the reference's GPU driver (GpuLbm3D) on the CUDA compute backend ----
+
+BACKEND_SO = os.path.join(os.path.dirname(REFERENCE_SO), "libref_backend.so")
+_backend = None
+
+
+def backend_available() -> bool:
+    return os.path.exists(BACKEND_SO)
+
+
+def _backend_lib():
+    global _backend
+    if _backend is None:
+        lib = ctypes.CDLL(BACKEND_SO)
+        lib.ref_backend_solve.argtypes = [ctypes.POINTER(abi.CLbm3DConfig), _u8p, _dp, _dp, _dp, _dp, _dp,
+                                          ctypes.c_uint64, _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_refusals.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        _backend = lib
+    return _backend
+
+
+def reference_gpu_driver_solve(config, solid, distance=None, fields=None, steps: int = 0) -> dict:
+    """One solve of the reference's own GPU driver (make_gpu_solver of
+    src/aero/lbm3d/lbm3d_gpu.cpp) on the CUDA compute backend: initial fields
+    (rho, ux, uy, uz) or the uniform inlet state, `steps` steps; returns the
+    populations, the moments (density, ux, uy, uz), force and moment, and the
+    backend's dispatch count and node-code tables built."""
+    lib = _backend_lib()
+    c = config.to_c()
+    n = config.cells
+    s = np.ascontiguousarray(solid, np.uint8).reshape(-1)
+    d = None if distance is None else np.ascontiguousarray(distance, np.float64).reshape(-1)
+    f = [None] * 4 if fields is None else [np.ascontiguousarray(a, np.float64).reshape(-1) for a in fields]
+    pops = np.zeros(19 * n)
+    mom = np.zeros(4 * n)
+    force = np.zeros(6)
+    meta = np.zeros(4)
+    msg = ctypes.create_string_buffer(2048)
+    rc = lib.ref_backend_solve(ctypes.byref(c), _ptr(s, _u8p), _ptr(d, _dp), *[_ptr(a, _dp) for a in f],
+                               int(steps), _ptr(pops, _dp), _ptr(mom, _dp), _ptr(force, _dp), _ptr(meta, _dp),
+                               msg, 2048)
+    if rc != 0:
+        raise ReferenceError_(msg.value.decode())
+    return {"populations": pops, "density": mom[:n], "ux": mom[n:2 * n], "uy": mom[2 * n:3 * n],
+            "uz": mom[3 * n:], "force": force[:3], "moment": force[3:], "dispatches": int(meta[0]),
+            "tables_built": int(meta[1]), "executes_kernels": bool(meta[2]), "steps": int(meta[3])}
+
+
+def reference_backend_refusals():
+    """(refusals of the CUDA backend's five bad calls, the last refusal's text)."""
+    msg = ctypes.create_string_buffer(1024)
+    n = _backend_lib().ref_backend_refusals(msg, 1024)
+    return n, msg.value.decode()
+
+
+# ---- binary32 restatement of the reference's GPU step (GLSL kernels) ----
+
+RESTATED32_SO = os.path.join(HERE, "_build", "liblbm_oracle32.so")
+_restated32 = None
+
+
+def restated32_lib():
+    global _restated32
+    if _restated32 is None:
+        if not os.path.exists(RESTATED32_SO):
+            build()
+        lib = ctypes.CDLL(RESTATED32_SO)
+        _fp = ctypes.POINTER(ctypes.c_float)
+        lib.lo32_create.restype = _vp
+        lib.lo32_create.argtypes = [ctypes.POINTER(abi.CLbm3DConfig), _u8p, _fp]
+        lib.lo32_destroy.argtypes = [_vp]
+        lib.lo32_initialize.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp]
+        lib.lo32_set_inlet.argtypes = [_vp, _dp]
+        lib.lo32_step.argtypes = [_vp, ctypes.c_uint64]
+        lib.lo32_populations.argtypes = [_vp, _dp]
+        lib.lo32_force.argtypes = [_vp, _u32p, _u32p, _dp, ctypes.c_uint64, _dp]
+        lib.lo32_steps.restype = ctypes.c_uint64
+        lib.lo32_steps.argtypes = [_vp]
+        _restated32 = lib
+    return _restated32
+
+
+class Restated32:
+    """The binary32 restatement of the reference's GLSL step
+    (oracle/lbm_oracle32.c).  `links` are the lattice's boundary links (cell,
+    direction, q), from the reference planner; their fractions fill the wall
+    table of an interpolated wall."""
+
+    def __init__(self, config, solid, links):
+        self.lib = restated32_lib()
+        self.config = config
+        self.cells = config.cells
+        self._c = config.to_c()
+        self.solid = np.ascontiguousarray(solid, np.uint8).reshape(-1)
+        cell, direction, q = links
+        self.cell = np.ascontiguousarray(cell, np.uint32)
+        self.direction = np.ascontiguousarray(direction, np.uint32)
+        self.q = np.ascontiguousarray(q, np.float64)
+        wall = None
+        if int(config.solid_wall) == abi.ORR_SOLID_INTERPOLATED:
+            wall = np.full(19 * self.cells, 0.5, np.float32)
+            wall[self.cell.astype(np.int64) * 19 + self.direction] = self.q.astype(np.float32)
+        self._wall = wall
+        self.h = self.lib.lo32_create(ctypes.byref(self._c), _ptr(self.solid, _u8p),
+                                      None if wall is None else wall.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        if not self.h:
+            raise MemoryError("lo32_create")
+
+    def close(self):
+        if self.h:
+            self.lib.lo32_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def initialize(self, rho=None, ux=None, uy=None, uz=None):
+        c = self.config
+        n = self.cells
+        inflow = int(c.x_boundary) == abi.ORR_X_INFLOW_OUTFLOW
+        if rho is None:
+            rho = np.ones(n)
+            ux = np.full(n, c.inlet_ux if inflow else 0.0)
+            uy = np.full(n, c.inlet_uy if inflow else 0.0)
+            uz = np.full(n, c.inlet_uz if inflow else 0.0)
+        arrs = [np.ascontiguousarray(a, np.float64).reshape(-1) for a in (rho, ux, uy, uz)]
+        inlet = np.array([c.inlet_ux, c.inlet_uy, c.inlet_uz], np.float64)
+        self.lib.lo32_initialize(self.h, *[_ptr(a, _dp) for a in arrs], _ptr(inlet, _dp))
+
+    def step(self, n):
+        self.lib.lo32_step(self.h, int(n))
+
+    def set_inlet_velocity(self, u):
+        v = np.ascontiguousarray(u, np.float64)
+        self.lib.lo32_set_inlet(self.h, _ptr(v, _dp))
+
+    def populations(self):
+        f = np.empty(19 * self.cells)
+        self.lib.lo32_populations(self.h, _ptr(f, _dp))
+        return f
+
+    def force(self):
+        out = np.empty(6)
+        self.lib.lo32_force(self.h, _ptr(self.cell, _u32p), _ptr(self.direction, _u32p), _ptr(self.q, _dp),
+                            len(self.cell), _ptr(out, _dp))
+        return out

@@ -1,0 +1,145 @@
+// The reference's own GPU driver, GpuLbm3D (src/aero/lbm3d/lbm3d_gpu.cpp,
+// make_gpu_solver), compiled unmodified from the reference sources in place
+// by oracle/Makefile into oracle/_ref/libref_backend.so, running its
+// lbm_d3q19_* dispatches on the CUDA compute backend of
+// orrery_b200/adapter/compute_backend_cuda.cpp: the backend seam
+// (IComputeBackend, src/aero/compute/include/orrery/aero/compute/
+// compute_backend.h:94-129) end to end on the B200 library.
+//
+// TEST INFRASTRUCTURE ONLY: the check of the backend seam (the reference's
+// "GPU and CPU D3Q19 agree" comparisons, tests/aero/lbm3d/test_lbm3d_gpu.cpp,
+// with the CUDA backend in place of the GL one).  The product never links or
+// loads it.
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "compute_backend_cuda.h"
+#include "orrery/aero/lbm3d/lbm3d.h"
+#include "orrery_lbm.h"
+#include "ref_convert.h"
+
+namespace lbm = orrery::aero::lbm;
+namespace compute = orrery::aero::compute;
+
+extern "C" {
+
+// One solve of the reference's GPU driver on the CUDA backend: make_gpu_solver
+// on (config, solid, distance), initialise from the four fields (or the
+// uniform inlet state when rho is null), `steps` steps, then the read-backs
+// whose outputs are not null: populations (19 cells, unshifted), moments
+// (density, ux, uy, uz planes of cells each) and force (force, moment).
+// meta (4): dispatches the backend served, node-code tables it built, and
+// whether it executes kernels; the driver's lattice step count.  0 on
+// success; -1 with the error's text.
+int ref_backend_solve(const orr_lbm3d_config* config, const uint8_t* solid, const double* distance,
+                      const double* rho, const double* ux, const double* uy, const double* uz, uint64_t steps,
+                      double* populations, double* moments, double* force, double* meta, char* message,
+                      size_t capacity) {
+    try {
+        compute::CudaComputeBackend backend(0);
+        const lbm::Lbm3DConfig c = ref_convert::config3d_of(*config);
+        auto made = lbm::make_gpu_solver(backend, c, ref_convert::mask3d_of(*config, solid, distance));
+        if (!made) {
+            ref_convert::copy_message(made.error(), message, capacity);
+            return -1;
+        }
+        std::unique_ptr<lbm::Lbm3DSolver> solver = std::move(made).value();
+        if (rho != nullptr) {
+            const std::size_t nx = c.nx, ny = c.ny;
+            const auto state = [=](std::size_t x, std::size_t y, std::size_t z) {
+                const std::size_t k = x + nx * (y + ny * z);
+                return lbm::d3q19::Moments{rho[k], ux[k], uy[k], uz[k]};
+            };
+            if (auto done = solver->initialize(state); !done) {
+                ref_convert::copy_message(done.error(), message, capacity);
+                return -1;
+            }
+        }
+        if (auto done = solver->step(steps); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        const std::size_t cells = c.nx * c.ny * c.nz;
+        if (populations != nullptr) {
+            auto f = solver->populations();
+            if (!f) {
+                ref_convert::copy_message(f.error(), message, capacity);
+                return -1;
+            }
+            std::memcpy(populations, f.value().data(), f.value().size() * sizeof(double));
+        }
+        if (moments != nullptr) {
+            auto m = solver->macroscopic();
+            if (!m) {
+                ref_convert::copy_message(m.error(), message, capacity);
+                return -1;
+            }
+            const lbm::MacroFields3D& v = m.value();
+            std::memcpy(moments, v.density.data(), cells * sizeof(double));
+            std::memcpy(moments + cells, v.velocity_x.data(), cells * sizeof(double));
+            std::memcpy(moments + 2 * cells, v.velocity_y.data(), cells * sizeof(double));
+            std::memcpy(moments + 3 * cells, v.velocity_z.data(), cells * sizeof(double));
+        }
+        if (force != nullptr) {
+            auto f = solver->force();
+            if (!f) {
+                ref_convert::copy_message(f.error(), message, capacity);
+                return -1;
+            }
+            for (int k = 0; k < 3; ++k) {
+                force[k] = f.value().force[k];
+                force[3 + k] = f.value().moment[k];
+            }
+        }
+        if (meta != nullptr) {
+            meta[0] = static_cast<double>(backend.dispatches());
+            meta[1] = static_cast<double>(backend.tables_built());
+            meta[2] = backend.info().executes_kernels ? 1.0 : 0.0;
+            meta[3] = static_cast<double>(solver->steps());
+        }
+        solver.reset();
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The backend's refusals through the seam, for the tests of its contract:
+// an unknown kernel, an empty dispatch, a uniform of the wrong type, an
+// unknown buffer, an upload outside a buffer.  Returns how many of the five
+// were refused (each must be), with the last refusal's text.
+int ref_backend_refusals(char* message, size_t capacity) {
+    compute::CudaComputeBackend backend(0);
+    int refused = 0;
+    std::string last;
+    const auto note = [&](const compute::Status& s) {
+        if (!s) {
+            ++refused;
+            last = s.error();
+        }
+    };
+    auto made = backend.create_buffer(64);
+    if (!made) {
+        ref_convert::copy_message(made.error(), message, capacity);
+        return -1;
+    }
+    const compute::BufferId id = made.value();
+    note(backend.dispatch({"lbm_d3q19_missing", {1, 1, 1}, {}, {}}));
+    note(backend.dispatch({"lbm_d3q19_step", {0, 1, 1}, {}, {}}));
+    const compute::Uniform wrong{"u_tau", std::uint32_t{1}};
+    note(backend.dispatch({"lbm_d3q19_step", {1, 1, 1}, std::span<const compute::Uniform>(&wrong, 1), {}}));
+    const compute::BufferBinding unknown{0, compute::BufferId{9999}};
+    note(backend.dispatch({"lbm_d3q19_step", {1, 1, 1}, {}, std::span<const compute::BufferBinding>(&unknown, 1)}));
+    std::vector<std::byte> bytes(65);
+    note(backend.upload(id, 0, bytes));
+    backend.release_buffer(id);
+    ref_convert::copy_message(last, message, capacity);
+    return refused;
+}
+
+} // extern "C"

@@ -52,6 +52,13 @@ SIGNATURES = {
     "orr_lbm3d_stream": (_st, [_vp, ctypes.POINTER(_vp)]),
     "orr_lbm3d_launch_count": (_st, [_vp, _u64p]),
     "orr_lbm3d_request_stall": (_st, [_vp, ctypes.c_uint32]),
+    "orr_gl3d_buffer_slack": (ctypes.c_uint64, []),
+    "orr_gl3d_create": (_st, [_vp, _u32p, ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "orr_gl3d_destroy": (None, [_vp]),
+    "orr_gl3d_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_gl3d_step": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "orr_gl3d_moments": (_st, [_vp, _vp, _vp, _vp, _vp]),
+    "orr_gl3d_link_force": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "orr_lbm3d_kernel_info": (_st, [_vp, ctypes.POINTER(abi.CKernelInfo)]),
     "orr_lbm3d_force_static": (_st, [ctypes.POINTER(abi.CForceLinks), _dp]),
     "orr_lbm2d_validate": (_st, [_c2, _u8p, _opt, ctypes.c_char_p, ctypes.c_size_t]),

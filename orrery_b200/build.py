@@ -40,6 +40,7 @@ SOURCES = {
     "solver2d.cu": [],
     "force_static.cu": [],
     "tiles.cu": [],
+    "gl3d.cu": [],
     "batch3d.cu": [],
     "serve3d.cu": [],
     "voxel.cu": ["-fmad=false"],

@@ -104,6 +104,8 @@ __global__ void __launch_bounds__(kTiledThreads<B>, kTiledMinBlocks<B>)
     constexpr uint32_t DIR = BOX / sizeof(S);   // values between consecutive directions' boxes
     constexpr uint32_t POP = kTilePop<S, R>;
     constexpr uint32_t STAGE = kTileStage<S, R>;
+    // Bytes the copies of a stage bring (the boxes without their padding).
+    constexpr uint32_t TX = d3::Q * kTileBox<S, R> + R * kTileW;
     constexpr uint32_t kConsumerWarps = B / 32;
     constexpr uint32_t kRowsPerPass = B / kTileW;
     constexpr int NPT = static_cast<int>(kTileW) * R / B;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kTiledThreads<B>, kTiledMinBlocks<B>)
             const bool skip = withhold && j == 0u;   // the stall request: never armed or filled
             if (!skip && lane == 0) {
                 info[s] = make_uint4(x0, y0, z, 0u);
-                mbar_expect_tx(bar, STAGE);
+                mbar_expect_tx(bar, TX);
             }
             __syncwarp();
             if (!skip && lane < static_cast<uint32_t>(d3::Q)) {
