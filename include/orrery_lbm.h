@@ -374,6 +374,16 @@ typedef struct orr_solve_request {
      * first step of each sampling interval (held over the interval), and the
      * configured one after.  0: no ramp. */
     double ramp_steps;
+    /* Steady test of the settle rule (until settled only): when positive, a
+     * window settles only if, besides |delta Cd| < tolerance, the ranges
+     * (max - min) of the x, y and z force samples over the window are each
+     * within steady_range times |mean x force| - the reference adapter's
+     * steady criterion (forces_settled_3d, src/aero/lbm3d/
+     * lbm_aero_solver3d.cpp:61-80, kSteadyResidual = 1e-3 at :25), so that
+     * an oscillating wake is not taken as settled when two window means
+     * happen to agree.  The ranges are of the lattice-axis components, the
+     * wind axes for an inlet along x.  0: off. */
+    double steady_range;
 } orr_solve_request;
 
 /* Run modes of a served solve.  Until settled: windows of `window` steps

@@ -117,7 +117,8 @@ class CSolveRequest(ctypes.Structure):
                 ("sample_every", ctypes.c_uint32), ("window", ctypes.c_uint32), ("mode", ctypes.c_uint32),
                 ("tolerance", ctypes.c_double), ("max_steps", ctypes.c_uint64),
                 ("reference_area", ctypes.c_double), ("reference_length", ctypes.c_double),
-                ("moment_centre", ctypes.c_double * 3), ("ramp_steps", ctypes.c_double)]
+                ("moment_centre", ctypes.c_double * 3), ("ramp_steps", ctypes.c_double),
+                ("steady_range", ctypes.c_double)]
 
 
 ORR_RUN_UNTIL_SETTLED, ORR_RUN_FIXED_STEPS = 0, 1

@@ -8,7 +8,8 @@
 // steps of every member (sample_every steps), the fixed-order force sums of
 // that period's sample, and serve_period_kernel.  The kernel folds each
 // running slot's sample into its window, applies the slot's rule (windows
-// until |delta Cd| < tolerance or the cap, or a fixed run length), writes the
+// until |delta Cd| < tolerance - and, when asked, force ranges within the
+// reference's steady bound - or the cap, or a fixed run length), writes the
 // slot's inlet velocity for the next period while its gradual start lasts,
 // and ends the loop after the period in which a slot finished, after a bound
 // on periods per launch, or when the host raised its flag (new solves wait
@@ -34,6 +35,7 @@ struct ServeSlot {
     double length;          // reference length: Cm = Mz / (qa L)
     double centre[2];       // moment centre (x, y) of the pitching moment about z
     double tolerance;       // on |delta Cd| between consecutive windows
+    double steady_range;    // > 0: window force ranges within steady_range |mean Fx| to settle
     uint64_t window;        // steps per window
     uint64_t max_steps;     // step cap, or the run's length (fixed steps)
     uint32_t mode;          // ORR_RUN_*
@@ -46,6 +48,8 @@ struct ServeSlot {
     uint64_t window_steps;
     uint64_t window_samples;
     double window_sum[6];
+    double window_lo[3];    // force sample extremes of the window (x, y, z)
+    double window_hi[3];
     double previous_cd;
     uint32_t have_previous;
     int32_t state;          // ORR_SOLVE_RUNNING until the slot is done
@@ -78,6 +82,11 @@ __global__ void serve_period_kernel(ServeSlot* __restrict__ slots, uint32_t n, c
         if (counted) {
             s.window_steps += period;
             for (int v = 0; v < 6; ++v) s.window_sum[v] = __dadd_rn(s.window_sum[v], f[v]);
+            for (int v = 0; v < 3; ++v) {
+                const bool first_sample = s.window_samples == 0;
+                s.window_lo[v] = first_sample ? f[v] : fmin(s.window_lo[v], f[v]);
+                s.window_hi[v] = first_sample ? f[v] : fmax(s.window_hi[v], f[v]);
+            }
             s.window_samples += 1;
         }
         bool finite = true;
@@ -107,7 +116,16 @@ __global__ void serve_period_kernel(ServeSlot* __restrict__ slots, uint32_t n, c
                 s.have_previous = 1u;
                 s.previous_cd = cd;
                 s.delta = delta;
-                if (delta < s.tolerance) {
+                // The reference adapter's steady test: every force range of
+                // the window within steady_range |mean drag force|.
+                bool steady = true;
+                if (s.steady_range > 0.0) {
+                    const double bound = __dmul_rn(s.steady_range, fabs(mean[0]));
+                    for (int v = 0; v < 3; ++v) {
+                        steady = steady && __dsub_rn(s.window_hi[v], s.window_lo[v]) <= bound;
+                    }
+                }
+                if (delta < s.tolerance && steady) {
                     s.state = ORR_SOLVE_CONVERGED;
                     done = true;
                 } else if (s.steps >= s.max_steps) {

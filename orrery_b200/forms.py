@@ -196,12 +196,23 @@ def oracle_errors(served: dict, requests, workloads, pick, max_active, memory_bu
     caps = [served["steps"][k] for k in pick]
     ref = _serve_once(requests, workloads, "f64", max_active, memory_budget, window, 1e-300, caps,
                       chunk_steps)
-    errs = []
-    for j, k in enumerate(pick):
-        cd, cd64 = served["cd"][k], ref["cd"][j]
-        errs.append(abs(cd - cd64) / abs(cd64) if cd64 else math.inf)
-    return {"n": len(pick), "max": max(errs), "mean": float(np.mean(errs)), "requests": pick,
-            "per_request": errs, "steps": caps, "steps_f64": ref["steps"], "cd_f64": ref["cd"]}
+
+    def rel(a, b):
+        return abs(a - b) / abs(b) if b else math.inf
+
+    errs = [rel(served["cd"][k], ref["cd"][j]) for j, k in enumerate(pick)]
+    out = {"n": len(pick), "max": max(errs), "mean": float(np.mean(errs)), "requests": pick,
+           "per_request": errs, "steps": caps, "steps_f64": ref["steps"], "cd_f64": ref["cd"]}
+    if served.get("storage") != "f32":
+        # The binary32 form of the same solves over the same steps: where the
+        # served storage's error matches binary32's, the spread is the
+        # trajectories of an unsteady wake parting, not the storage's
+        # rounding.
+        r32 = _serve_once(requests, workloads, "f32", max_active, memory_budget, window, 1e-300, caps,
+                          chunk_steps)
+        out["f32_per_request"] = [rel(r32["cd"][j], ref["cd"][j]) for j in range(len(pick))]
+        out["cd_f32"] = r32["cd"]
+    return out
 
 
 def voxelize_workload():

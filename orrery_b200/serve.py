@@ -29,6 +29,12 @@ def _result(r: abi.CSolveResult) -> dict:
             "device_bytes": r.device_bytes, "message": r.message.decode(errors="replace")}
 
 
+# The reference adapter's steady criterion: every force range over the
+# window within 1e-3 of the mean drag (kSteadyResidual,
+# src/aero/lbm3d/lbm_aero_solver3d.cpp:25, forces_settled_3d at :61-80).
+STEADY_RANGE = 1e-3
+
+
 class Server:
     def __init__(self, storage: str = "f32", device: int = 0, memory_budget: float = 150e9,
                  max_active: int = 64, chunk_steps: int = 100, sample_every: int = 10,
@@ -73,12 +79,15 @@ class Server:
 
     def submit(self, w: Workload3D, window: int = 500, tolerance: float = 1e-4, max_steps: int = 0,
                initial_state: bool = True, moment_centre=(0.0, 0.0, 0.0), fixed_steps: bool = False,
-               ramp_steps: float = 0.0) -> int:
+               ramp_steps: float = 0.0, steady_range: float = STEADY_RANGE) -> int:
         """Queues the solve of workload `w`; returns its id.  Without
         `initial_state` the solve starts from the uniform inlet state.
         `fixed_steps`: run exactly `max_steps` steps and report the means over
         the last `window` steps.  `ramp_steps` > 0: start at rest with the
-        reference adapter's gradual start of the inlet velocity."""
+        reference adapter's gradual start of the inlet velocity.
+        `steady_range`: a window settles only when its force ranges are within
+        this fraction of the mean drag force as well (the reference adapter's
+        steady test, 1e-3 there); 0 leaves only the |delta Cd| rule."""
         c = w.config.to_c()
         solid = np.ascontiguousarray(w.mask.solid, np.uint8).reshape(-1)
         dist = None if w.mask.distance is None else np.ascontiguousarray(w.mask.distance, np.float64).reshape(-1)
@@ -99,6 +108,7 @@ class Server:
         r.moment_centre = (ctypes.c_double * 3)(*[float(v) for v in moment_centre])
         r.mode = abi.ORR_RUN_FIXED_STEPS if fixed_steps else abi.ORR_RUN_UNTIL_SETTLED
         r.ramp_steps = float(ramp_steps)
+        r.steady_range = float(steady_range)
         out = ctypes.c_uint64()
         self._check(self._lib.orr_serve_submit(self._h, ctypes.byref(r), ctypes.byref(out)))
         return out.value

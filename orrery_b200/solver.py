@@ -219,6 +219,14 @@ class CudaLbm3D:
                                                     "float64 arrays of nx*ny*nz values")
         self._check(self._lib.orr_lbm3d_macroscopic(self._h, *[ptr(a, _dp) for a in planes]))
         if out is not None:
+            # the shape and mask of this solver, whichever solver of as many
+            # nodes filled `out` before
+            out.nx, out.ny, out.nz = self.config.nx, self.config.ny, self.config.nz
+            if isinstance(out.solid, np.ndarray) and out.solid.shape == self._solid.shape \
+                    and out.solid.dtype == self._solid.dtype and out.solid.flags.writeable:
+                np.copyto(out.solid, self._solid)
+            else:
+                out.solid = self._solid.copy()
             return out
         return MacroFields3D(self.config.nx, self.config.ny, self.config.nz, *planes, self._solid.copy())
 

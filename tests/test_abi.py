@@ -130,3 +130,14 @@ def test_memory_estimate_counts_every_table():
     assert f64 > f32
     with pytest.raises(_native.LbmError):
         S.memory_bytes(Lbm3DConfig(nx=4, ny=4, nz=(1 << 60) + 1), 0, 0)
+
+
+def test_server_refuses_bfloat16_before_touching_a_device():
+    """Served solves promise Cd within 0.5% of binary64, which bfloat16
+    storage misses; the refusal comes before any device call, so it holds
+    without a GPU."""
+    from orrery_b200.serve import Server
+    with pytest.raises(_native.LbmError) as e:
+        Server(storage="bf16")
+    assert e.value.status == abi.ORR_ERR_INVALID
+    assert "bfloat16" in str(e.value) and "0.5%" in str(e.value)

@@ -81,3 +81,37 @@ def test_sphere_256_binary64_bitwise_20_steps(workload):
     # open boundaries: the mass changes only by the inlet/outlet fluxes,
     # which are small over 20 steps
     assert math.isfinite(g.mass()) and abs(g.mass() - m0) / m0 < 1e-3
+
+
+def test_sphere_256_binary32_drag_history_vs_two_oracles(workload):
+    """The instantaneous drag of the binary32 CUDA path, sampled every 10
+    steps over 1000 steps, against two committed CPU histories of the same
+    run (tests/golden/oracle32_sphere3d_256x128x128.npz, made by
+    tests/golden/make_oracle32_golden.py): the reference's binary64 CpuLbm3D
+    and the binary32 restatement of the reference's GLSL step.  The start
+    is impulsive, so the instantaneous Cd swings through zero; the spread
+    is taken in Cd units.  Two binary32 evaluations of one step round
+    differently, so the CUDA path passes when its distance from binary64
+    stays within three times the GLSL form's own."""
+    import os
+    w = workload
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle32_sphere3d_256x128x128.npz"))
+    q = float(gold["q"])
+    g = S.make_gpu_solver(w.config, w.mask)
+    g.initialize(w.rho, w.ux, w.uy, w.uz)
+    sg = sampled_run(g, lambda s: np.concatenate([s.force().force, s.force().moment]), 1000)
+    g.close()
+    cd_g, cd64, cd32 = sg[:, 0] / q, gold["f64"][:, 0] / q, gold["b32"][:, 0] / q
+    d_g, d_32 = np.abs(cd_g - cd64), np.abs(cd32 - cd64)
+    print(f"measured: 256x128x128 instantaneous Cd over 1000 steps (every 10): max |CUDA f32 - f64| "
+          f"{d_g.max():.3e}, max |GLSL b32 - f64| {d_32.max():.3e}; at step 1000 CUDA {cd_g[-1]:.8f}, "
+          f"b32 {cd32[-1]:.8f}, f64 {cd64[-1]:.8f}")
+    assert np.all(np.isfinite(cd_g))
+    assert d_g.max() <= 3.0 * d_32.max()
+    # At step 1000 the instantaneous Cd passes near a minimum of the pressure
+    # waves (0.24 against a window mean of 1.08), so the two binary32 forms
+    # are compared on the scale of the window-mean drag: within 1e-4 of it.
+    scale = abs(cd64[-50:].mean())
+    print(f"measured: |CUDA f32 - GLSL b32| at step 1000 {abs(cd_g[-1] - cd32[-1]) / scale:.2e} of the "
+          f"window-mean Cd {scale:.6f}; series max {np.abs(cd_g - cd32).max() / scale:.2e}")
+    assert abs(cd_g[-1] - cd32[-1]) <= 1e-4 * scale

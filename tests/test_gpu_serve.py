@@ -14,7 +14,7 @@ import pytest
 from orrery_b200 import solver as S
 from orrery_b200 import workloads as W
 from orrery_b200.lbm3d import XBoundary
-from orrery_b200.serve import Server
+from orrery_b200.serve import STEADY_RANGE, Server
 
 pytestmark = pytest.mark.gpu
 
@@ -28,13 +28,13 @@ def small(seed, nx=64, ny=32, nz=32, reynolds=60.0, diameter=8.0):
     return W.sphere3d(seed=seed, nx=nx, ny=ny, nz=nz, diameter=diameter, reynolds=reynolds)
 
 
-def serve(workloads, storage="f32", delays=None, **opts):
+def serve(workloads, storage="f32", delays=None, steady_range=STEADY_RANGE, **opts):
     with Server(storage=storage, chunk_steps=CHUNK, sample_every=10, **opts) as srv:
         ids = []
         for k, w in enumerate(workloads):
             if delays is not None:
                 time.sleep(delays[k])
-            ids.append(srv.submit(w, window=WINDOW, tolerance=TOL, max_steps=CAP))
+            ids.append(srv.submit(w, window=WINDOW, tolerance=TOL, max_steps=CAP, steady_range=steady_range))
         srv.drain(timeout=600)
         return [srv.poll(i) for i in ids], srv.stats()
 
@@ -57,32 +57,47 @@ def test_results_alone_and_in_mix_are_identical():
     assert stats["solves_per_second"] > 0
 
 
-def test_window_rule_matches_a_plain_solver_loop():
+@pytest.mark.parametrize("steady_range", [0.0, STEADY_RANGE, 1e-9])
+def test_window_rule_matches_a_plain_solver_loop(steady_range):
     """The served steps and window-mean Cd follow the rule run by hand on a
-    plain solver (force every 10 steps, window means, |delta Cd| < tol)."""
+    plain solver (force every 10 steps, window means, |delta Cd| < tol and,
+    with a steady range, every force range of the window within that
+    fraction of the mean drag force, the reference adapter's steady test).
+    A range of 1e-9 holds no window of this flow steady, so that solve runs
+    to the cap."""
     w = small(21)
-    served, _ = serve([w])
+    served, _ = serve([w], steady_range=steady_range)
     r = served[0]
     s = S.make_gpu_solver(w.config, w.mask)
     s.initialize(w.rho, w.ux, w.uy, w.uz)
     q = 0.5 * w.config.inlet_ux ** 2 * w.reference_area
     steps, prev, cd, state = 0, None, None, None
     while state is None:
-        acc = np.zeros(6)
+        samples = []
         for _ in range(WINDOW // 10):
             s.step(10)
             f = s.force()
-            acc += np.concatenate([f.force, f.moment])
+            samples.append(np.concatenate([f.force, f.moment]))
+        samples = np.array(samples)
+        acc = np.zeros(6)
+        for v in samples:
+            acc += v
         steps += WINDOW
         cd = acc[0] / (WINDOW // 10) / q
-        if prev is not None and abs(cd - prev) < TOL:
+        mean_fx = acc[0] / (WINDOW // 10)
+        ranges = samples[:, :3].max(axis=0) - samples[:, :3].min(axis=0)
+        steady = steady_range == 0.0 or bool(np.all(ranges <= steady_range * abs(mean_fx)))
+        if prev is not None and abs(cd - prev) < TOL and steady:
             state = "converged"
         elif steps >= CAP:
             state = "capped"
         prev = cd
+    s.close()
     assert r["state"] == state
     assert r["steps"] == steps
     assert r["cd"] == pytest.approx(cd, rel=1e-10)
+    if steady_range == 1e-9:
+        assert state == "capped"
 
 
 def test_memory_budget_admission():

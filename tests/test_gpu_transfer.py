@@ -117,3 +117,10 @@ def test_read_back_into_earlier_arrays():
                               m.velocity_z, m.solid)
         with pytest.raises(S.LbmError):
             s.macroscopic(out=bad)
+    # fields filled by another solver of the same size carry this solver's mask
+    solid2 = np.zeros(nx * ny * nz, np.uint8)
+    solid2[::7] = 1
+    with S.make_gpu_solver(cfg, SolidMask3D(nx, ny, nz, solid2, None)) as s2:
+        m3 = s2.macroscopic(out=m)
+        assert m3 is m and np.array_equal(m.solid.reshape(-1), solid2)
+        assert np.array_equal(s2.macroscopic().solid, m.solid)
