@@ -79,15 +79,16 @@ class Server:
 
     def submit(self, w: Workload3D, window: int = 500, tolerance: float = 1e-4, max_steps: int = 0,
                initial_state: bool = True, moment_centre=(0.0, 0.0, 0.0), fixed_steps: bool = False,
-               ramp_steps: float = 0.0, steady_range: float = STEADY_RANGE) -> int:
+               ramp_steps: float = 0.0, steady_range: float = 0.0) -> int:
         """Queues the solve of workload `w`; returns its id.  Without
         `initial_state` the solve starts from the uniform inlet state.
         `fixed_steps`: run exactly `max_steps` steps and report the means over
         the last `window` steps.  `ramp_steps` > 0: start at rest with the
         reference adapter's gradual start of the inlet velocity.
-        `steady_range`: a window settles only when its force ranges are within
-        this fraction of the mean drag force as well (the reference adapter's
-        steady test, 1e-3 there); 0 leaves only the |delta Cd| rule."""
+        `steady_range` > 0: a window settles only when its force ranges are
+        within this fraction of the mean drag force as well (the reference
+        adapter's steady test; STEADY_RANGE is its bound); 0, the default,
+        leaves the |delta Cd| rule alone."""
         c = w.config.to_c()
         solid = np.ascontiguousarray(w.mask.solid, np.uint8).reshape(-1)
         dist = None if w.mask.distance is None else np.ascontiguousarray(w.mask.distance, np.float64).reshape(-1)

@@ -28,7 +28,7 @@ def small(seed, nx=64, ny=32, nz=32, reynolds=60.0, diameter=8.0):
     return W.sphere3d(seed=seed, nx=nx, ny=ny, nz=nz, diameter=diameter, reynolds=reynolds)
 
 
-def serve(workloads, storage="f32", delays=None, steady_range=STEADY_RANGE, **opts):
+def serve(workloads, storage="f32", delays=None, steady_range=0.0, **opts):
     with Server(storage=storage, chunk_steps=CHUNK, sample_every=10, **opts) as srv:
         ids = []
         for k, w in enumerate(workloads):
