@@ -301,6 +301,10 @@ def run_form(args, rank: int) -> int:
     return 0
 
 
+def _oracle_check(text: str):
+    return text if text == "converged" else int(text)
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -316,8 +320,9 @@ def main(argv=None) -> int:
     ap.add_argument("--lattices", type=int, default=64, help="batched form: lattices")
     ap.add_argument("--requests", type=int, default=48, help="serve form: requests")
     ap.add_argument("--max-steps", type=int, default=20000, help="serve form: step cap per solve")
-    ap.add_argument("--oracle-check", type=int, default=0,
-                    help="serve form: requests whose Cd is checked against the binary64 form")
+    ap.add_argument("--oracle-check", type=_oracle_check, default=0,
+                    help="serve form: the first N requests, or 'converged' (every solve that settled), "
+                         "whose Cd is checked against the binary64 and binary32 forms")
     ap.add_argument("--no-plain", action="store_true", help="batched/serve: skip the plain-form baseline")
     ap.add_argument("--serve-kernel", default="auto", choices=["auto", "rows", "staged"],
                     help="serve form: the batch schedule's kernel")

@@ -122,3 +122,38 @@ def test_backend_refuses_bad_calls():
     O = _oracle()
     n, text = O.reference_backend_refusals()
     assert n == 5, text
+
+
+def test_force_over_more_links_than_one_grid_dimension():
+    """The driver's force dispatch for more links than 65535 groups of 64
+    reach in one dimension (test_lbm3d_gpu_driver.cpp:93-156: a periodic
+    128 x 128 x 66 box, fluid where x and y are even, 16 links per fluid
+    node, 4,325,376 in all) tiles the links into rows; on the CUDA backend
+    every link must be summed once.  Here the fluid moves (seeded velocities),
+    so the force is not zero, and it must match the reference CPU solver's
+    after one step."""
+    O = _oracle()
+    nx, ny, nz = 128, 128, 66
+    cfg = periodic_box(nx, ny, nz, 0.6)
+    mask = M.fluid_mask_3d(nx, ny, nz)
+    x = np.arange(nx)[None, None, :]
+    y = np.arange(ny)[None, :, None]
+    solid = np.broadcast_to(~((x % 2 == 0) & (y % 2 == 0)), (nz, ny, nx)).astype(np.uint8).reshape(-1)
+    mask.solid = solid
+    rng = np.random.default_rng(17)
+    n = cfg.cells
+    fields = (1.0 + 1e-3 * rng.standard_normal(n), 0.02 * rng.standard_normal(n),
+              0.02 * rng.standard_normal(n), 0.02 * rng.standard_normal(n))
+    cpu = O.Reference3D(cfg, solid, None)
+    links = len(cpu.links()[0])
+    cpu.initialize(*fields)
+    cpu.step(1)
+    fc = np.asarray(cpu.force())
+    cpu.close()
+    assert links == nx * ny * nz // 4 * 16 and links > 65535 * 64
+    g = O.reference_gpu_driver_solve(cfg, solid, None, fields=fields, steps=1)
+    err = np.abs(np.asarray(g["force"]) - fc[:3]).max() / np.abs(fc[:3]).max()
+    err_m = np.abs(np.asarray(g["moment"]) - fc[3:]).max() / np.abs(fc[3:]).max()
+    print(f"measured: CUDA backend force over {links} links vs CPU: force {err:.2e}, moment {err_m:.2e} "
+          f"of the largest component")
+    assert err < 1e-4 and err_m < 1e-4
