@@ -535,6 +535,52 @@ ORR_API orr_status orr_gl3d_moments(orr_gl3d* tables, const orr_gl3d_params* par
 ORR_API orr_status orr_gl3d_link_force(orr_gl3d* tables, const orr_gl3d_params* params, const float* src,
                                        const uint32_t* links, float* link_force, const float* wall, void* stream);
 
+/* The D2Q9 twins: the three kernels the reference's GpuLbm2D dispatches
+ * (lbm_d2q9_step, lbm_d2q9_moments, lbm_d2q9_force: src/aero/lbm/
+ * lbm2d_gpu.cpp:36-44, 104-124, 220-300), on buffers in that driver's
+ * layout: binary32 populations shifted by their weights (9 * nx*ny), solid
+ * flags (uint32: 1 solid, 0 fluid), the moments (rho - 1, ux, uy planes), the
+ * convective-outlet history (3 * ny: directions 3, 6, 7, slot * ny + y) and
+ * the links (cell, direction pairs).  No slack is needed around the
+ * population buffers. */
+typedef struct orr_gl2d_params {   /* the driver's uniforms (lbm2d_gpu.cpp:104-124) */
+    uint32_t nx, ny;               /* u_nx, u_ny */
+    uint32_t x_mode;               /* u_x_mode: 1 inflow / outflow, 0 periodic */
+    uint32_t bottom_kind, top_kind; /* u_bottom_kind, u_top_kind: 0 periodic, 1 slip, 2 no-slip */
+    float bottom_ux, top_ux;       /* u_bottom_ux, u_top_ux */
+    float inlet[2];                /* u_inlet_ux, u_inlet_uy */
+    float tau;                     /* u_tau */
+    float smagorinsky_c2;          /* u_smagorinsky_c2: the closure is on when positive */
+    float force[2];                /* u_force_x, u_force_y */
+    uint32_t outlet_mode;          /* u_outlet_mode: 1 extrapolation, 0 convective */
+    float outlet_speed;            /* u_outlet_speed */
+    uint32_t link_count;           /* u_link_count */
+} orr_gl2d_params;
+
+typedef struct orr_gl2d orr_gl2d;  /* the tables derived from one solid-flag buffer */
+
+/* Tables for the lattice of `params` whose solid flags are `solid_flags`
+ * (host, nx*ny values): this library's node classes and bounce-back masks,
+ * on `device`.  The lattice is validated as the 2D make_gpu_solver
+ * validates it. */
+ORR_API orr_status orr_gl2d_create(const orr_gl2d_params* params, const uint32_t* solid_flags, int32_t device,
+                                   orr_gl2d** out);
+ORR_API void orr_gl2d_destroy(orr_gl2d* tables);
+ORR_API const char* orr_gl2d_last_error(const orr_gl2d* tables);
+/* lbm_d2q9_step: binding 0 (src) -> binding 2 (dst), binding 6 (outlet
+ * history, updated). */
+ORR_API orr_status orr_gl2d_step(orr_gl2d* tables, const orr_gl2d_params* params, const float* src, float* dst,
+                                 float* outlet, void* stream);
+/* lbm_d2q9_moments: binding 0 (src) -> binding 3 (moments). */
+ORR_API orr_status orr_gl2d_moments(orr_gl2d* tables, const orr_gl2d_params* params, const float* src,
+                                    float* moments, void* stream);
+/* lbm_d2q9_force: binding 0 (src), 4 (links) -> binding 5 (per link the two
+ * components of 2 c_o fs_o, fs_o the shifted population leaving towards the
+ * wall; a link outside the lattice gives 0).  `tables` may be NULL (the
+ * kernel needs the lattice size only; it then runs on the current device). */
+ORR_API orr_status orr_gl2d_link_force(orr_gl2d* tables, const orr_gl2d_params* params, const float* src,
+                                       const uint32_t* links, float* link_force, void* stream);
+
 /* ---- D2Q9 -------------------------------------------------------------- */
 
 /* validate (lbm2d.h:85-86; lbm2d_common.cpp:31-77) plus the binary32 checks

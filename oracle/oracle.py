@@ -735,7 +735,10 @@ def _backend_lib():
         lib = ctypes.CDLL(BACKEND_SO)
         lib.ref_backend_solve.argtypes = [ctypes.POINTER(abi.CLbm3DConfig), _u8p, _dp, _dp, _dp, _dp, _dp,
                                           ctypes.c_uint64, _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_solve2d.argtypes = [ctypes.POINTER(abi.CLbm2DConfig), _u8p, _dp, _dp, _dp,
+                                            ctypes.c_uint64, _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_refusals.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_adapter2d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
         _backend = lib
     return _backend
 
@@ -765,6 +768,43 @@ def reference_gpu_driver_solve(config, solid, distance=None, fields=None, steps:
     return {"populations": pops, "density": mom[:n], "ux": mom[n:2 * n], "uy": mom[2 * n:3 * n],
             "uz": mom[3 * n:], "force": force[:3], "moment": force[3:], "dispatches": int(meta[0]),
             "tables_built": int(meta[1]), "executes_kernels": bool(meta[2]), "steps": int(meta[3])}
+
+
+def reference_gpu_driver_solve2d(config, solid, fields=None, steps: int = 0) -> dict:
+    """One solve of the reference's own D2Q9 GPU driver (make_gpu_solver of
+    src/aero/lbm/lbm2d_gpu.cpp) on the CUDA compute backend: initial fields
+    (rho, ux, uy) or the uniform inlet state, `steps` steps; returns the
+    populations, the moments (density, ux, uy), the force (x, y, moment) and
+    the backend's dispatch count and solid-flag tables built."""
+    lib = _backend_lib()
+    c = config.to_c()
+    n = int(config.nx) * int(config.ny)
+    s = np.ascontiguousarray(solid, np.uint8).reshape(-1)
+    f = [None] * 3 if fields is None else [np.ascontiguousarray(a, np.float64).reshape(-1) for a in fields]
+    pops = np.zeros(9 * n)
+    mom = np.zeros(3 * n)
+    force = np.zeros(3)
+    meta = np.zeros(4)
+    msg = ctypes.create_string_buffer(2048)
+    rc = lib.ref_backend_solve2d(ctypes.byref(c), _ptr(s, _u8p), *[_ptr(a, _dp) for a in f], int(steps),
+                                 _ptr(pops, _dp), _ptr(mom, _dp), _ptr(force, _dp), _ptr(meta, _dp), msg, 2048)
+    if rc != 0:
+        raise ReferenceError_(msg.value.decode())
+    return {"populations": pops, "density": mom[:n], "ux": mom[n:2 * n], "uy": mom[2 * n:], "force": force,
+            "dispatches": int(meta[0]), "tables_built": int(meta[1]), "executes_kernels": bool(meta[2]),
+            "steps": int(meta[3])}
+
+
+def reference_adapter2d_on_backend() -> dict:
+    """The reference's 2D adapter (LbmAeroSolver2D) on its CPU solver and on
+    the GPU driver over the CUDA backend, the case of the reference's
+    "IAeroSolver adapter runs on the GPU backend" test."""
+    out = np.zeros(6)
+    msg = ctypes.create_string_buffer(2048)
+    if _backend_lib().ref_backend_adapter2d(_ptr(out, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return {"cd_cpu": float(out[0]), "cd_gpu": float(out[1]), "iterations_cpu": int(out[2]),
+            "iterations_gpu": int(out[3]), "cp_cpu": int(out[4]), "cp_gpu": int(out[5])}
 
 
 def reference_backend_refusals():

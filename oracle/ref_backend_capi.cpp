@@ -10,14 +10,18 @@
 // "GPU and CPU D3Q19 agree" comparisons, tests/aero/lbm3d/test_lbm3d_gpu.cpp,
 // with the CUDA backend in place of the GL one).  The product never links or
 // loads it.
+#include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <numbers>
 #include <exception>
 #include <memory>
 #include <string>
 #include <vector>
 
 #include "compute_backend_cuda.h"
+#include "orrery/aero/lbm/lbm2d.h"
+#include "orrery/aero/lbm/lbm_aero_solver.h"
 #include "orrery/aero/lbm3d/lbm3d.h"
 #include "orrery_lbm.h"
 #include "ref_convert.h"
@@ -27,7 +31,7 @@ namespace compute = orrery::aero::compute;
 
 extern "C" {
 
-// One solve of the reference's GPU driver on the CUDA backend: make_gpu_solver
+// One solve of the reference's D3Q19 GPU driver on the CUDA backend: make_gpu_solver
 // on (config, solid, distance), initialise from the four fields (or the
 // uniform inlet state when rho is null), `steps` steps, then the read-backs
 // whose outputs are not null: populations (19 cells, unshifted), moments
@@ -102,6 +106,133 @@ int ref_backend_solve(const orr_lbm3d_config* config, const uint8_t* solid, cons
             meta[3] = static_cast<double>(solver->steps());
         }
         solver.reset();
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The same for the reference's D2Q9 driver, GpuLbm2D (src/aero/lbm/
+// lbm2d_gpu.cpp, its make_gpu_solver): initial fields (rho, ux, uy) or the
+// uniform inlet state; populations (9 cells, unshifted), moments (density,
+// ux, uy planes) and force (x, y, moment about the origin).
+int ref_backend_solve2d(const orr_lbm2d_config* config, const uint8_t* solid, const double* rho,
+                        const double* ux, const double* uy, uint64_t steps, double* populations, double* moments,
+                        double* force, double* meta, char* message, size_t capacity) {
+    try {
+        compute::CudaComputeBackend backend(0);
+        const lbm::Lbm2DConfig c = ref_convert::config2d_of(*config);
+        lbm::SolidMask2D mask;
+        mask.nx = c.nx;
+        mask.ny = c.ny;
+        mask.solid.assign(solid, solid + c.nx * c.ny);
+        auto made = lbm::make_gpu_solver(backend, c, std::move(mask));
+        if (!made) {
+            ref_convert::copy_message(made.error(), message, capacity);
+            return -1;
+        }
+        std::unique_ptr<lbm::Lbm2DSolver> solver = std::move(made).value();
+        if (rho != nullptr) {
+            const std::size_t nx = c.nx;
+            const auto state = [=](std::size_t x, std::size_t y) {
+                const std::size_t k = x + nx * y;
+                return lbm::d2q9::Moments{rho[k], ux[k], uy[k]};
+            };
+            if (auto done = solver->initialize(state); !done) {
+                ref_convert::copy_message(done.error(), message, capacity);
+                return -1;
+            }
+        }
+        if (auto done = solver->step(steps); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        const std::size_t cells = c.nx * c.ny;
+        if (populations != nullptr) {
+            auto f = solver->populations();
+            if (!f) {
+                ref_convert::copy_message(f.error(), message, capacity);
+                return -1;
+            }
+            std::memcpy(populations, f.value().data(), f.value().size() * sizeof(double));
+        }
+        if (moments != nullptr) {
+            auto m = solver->macroscopic();
+            if (!m) {
+                ref_convert::copy_message(m.error(), message, capacity);
+                return -1;
+            }
+            const lbm::MacroFields2D& v = m.value();
+            std::memcpy(moments, v.density.data(), cells * sizeof(double));
+            std::memcpy(moments + cells, v.velocity_x.data(), cells * sizeof(double));
+            std::memcpy(moments + 2 * cells, v.velocity_y.data(), cells * sizeof(double));
+        }
+        if (force != nullptr) {
+            auto f = solver->force();
+            if (!f) {
+                ref_convert::copy_message(f.error(), message, capacity);
+                return -1;
+            }
+            force[0] = f.value().x;
+            force[1] = f.value().y;
+            force[2] = f.value().moment;
+        }
+        if (meta != nullptr) {
+            meta[0] = static_cast<double>(backend.dispatches());
+            meta[1] = static_cast<double>(backend.tables_built());
+            meta[2] = backend.info().executes_kernels ? 1.0 : 0.0;
+            meta[3] = static_cast<double>(solver->steps());
+        }
+        solver.reset();
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The reference's 2D adapter, LbmAeroSolver2D (src/aero/lbm/lbm_aero_solver.cpp),
+// on its CPU solver and on GpuLbm2D over the CUDA backend: the case of
+// "The IAeroSolver adapter runs on the GPU backend" (tests/aero/lbm/
+// test_lbm_gpu.cpp:278-311; a circle of 96 points, radius 0.01, speed 0.1,
+// density 1000, Re 100, 10 cells per length, u_lat 0.05, duration 10, 2000
+// steps per call).  out (6): Cd CPU, Cd GPU, iterations CPU, iterations GPU,
+// surface Cp samples CPU, GPU.  0 on success; -1 with the error's text.
+int ref_backend_adapter2d(double* out, char* message, size_t capacity) {
+    try {
+        namespace aero = orrery::aero;
+        compute::CudaComputeBackend backend(0);
+        aero::AeroGeometry geometry;
+        for (int k = 0; k < 96; ++k) {
+            const double a = 2.0 * std::numbers::pi * static_cast<double>(k) / 96.0;
+            geometry.section.push_back({0.01 * std::cos(a), 0.01 * std::sin(a)});
+        }
+        geometry.reference.length = 0.02;
+        geometry.reference.area = 0.02;
+        aero::FlowConditions conditions;
+        conditions.speed = 0.1;
+        conditions.density = 1000.0;
+        conditions.viscosity = 1000.0 * 0.1 * 0.02 / 100.0;
+        lbm::LbmSolverOptions options;
+        options.resolution = lbm::LatticeResolution{10.0, 0.05};
+        options.duration = 10.0;
+        options.steps_per_call = 2000;
+        lbm::LbmAeroSolver2D cpu(options);
+        options.backend = &backend;
+        lbm::LbmAeroSolver2D gpu(options);
+        cpu.setup(geometry, conditions);
+        gpu.setup(geometry, conditions);
+        while (!cpu.step()) {
+        }
+        while (!gpu.step()) {
+        }
+        out[0] = cpu.result().cd;
+        out[1] = gpu.result().cd;
+        out[2] = static_cast<double>(cpu.result().iterations);
+        out[3] = static_cast<double>(gpu.result().iterations);
+        out[4] = static_cast<double>(cpu.result().surface.cp.size());
+        out[5] = static_cast<double>(gpu.result().surface.cp.size());
         return 0;
     } catch (const std::exception& e) {
         ref_convert::copy_message(e.what(), message, capacity);

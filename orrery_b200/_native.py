@@ -59,6 +59,12 @@ SIGNATURES = {
     "orr_gl3d_step": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "orr_gl3d_moments": (_st, [_vp, _vp, _vp, _vp, _vp]),
     "orr_gl3d_link_force": (_st, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "orr_gl2d_create": (_st, [_vp, _u32p, ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "orr_gl2d_destroy": (None, [_vp]),
+    "orr_gl2d_last_error": (ctypes.c_char_p, [_vp]),
+    "orr_gl2d_step": (_st, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "orr_gl2d_moments": (_st, [_vp, _vp, _vp, _vp, _vp]),
+    "orr_gl2d_link_force": (_st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "orr_lbm3d_kernel_info": (_st, [_vp, ctypes.POINTER(abi.CKernelInfo)]),
     "orr_lbm3d_force_static": (_st, [ctypes.POINTER(abi.CForceLinks), _dp]),
     "orr_lbm2d_validate": (_st, [_c2, _u8p, _opt, ctypes.c_char_p, ctypes.c_size_t]),

@@ -27,6 +27,11 @@ constexpr std::uint32_t kBindWall = 7;
 constexpr std::string_view kStep = "lbm_d3q19_step";
 constexpr std::string_view kMoments = "lbm_d3q19_moments";
 constexpr std::string_view kForce = "lbm_d3q19_force";
+// The D2Q9 driver's kernels (lbm2d_gpu.cpp; binding points 0..6 as above,
+// binding 1 the solid flags).
+constexpr std::string_view kStep2 = "lbm_d2q9_step";
+constexpr std::string_view kMoments2 = "lbm_d2q9_moments";
+constexpr std::string_view kForce2 = "lbm_d2q9_force";
 
 Status failure(std::string text) {
     return core::failure(std::move(text));
@@ -103,6 +108,54 @@ std::optional<std::string> read_uniforms(std::span<const Uniform> uniforms, orr_
     return std::nullopt;
 }
 
+// The D2Q9 driver's uniforms (lbm2d_gpu.cpp:104-124), by the same rules.
+std::optional<std::string> read_uniforms2(std::span<const Uniform> uniforms, orr_gl2d_params& p) {
+    struct U32 {
+        std::string_view name;
+        std::uint32_t* at;
+    };
+    struct F32 {
+        std::string_view name;
+        float* at;
+    };
+    const std::array<U32, 7> u32{{{"u_nx", &p.nx},
+                                  {"u_ny", &p.ny},
+                                  {"u_x_mode", &p.x_mode},
+                                  {"u_bottom_kind", &p.bottom_kind},
+                                  {"u_top_kind", &p.top_kind},
+                                  {"u_link_count", &p.link_count},
+                                  {"u_outlet_mode", &p.outlet_mode}}};
+    const std::array<F32, 10> f32{{{"u_bottom_ux", &p.bottom_ux},
+                                   {"u_top_ux", &p.top_ux},
+                                   {"u_inlet_ux", &p.inlet[0]},
+                                   {"u_inlet_uy", &p.inlet[1]},
+                                   {"u_tau", &p.tau},
+                                   {"u_smagorinsky_c2", &p.smagorinsky_c2},
+                                   {"u_force_x", &p.force[0]},
+                                   {"u_force_y", &p.force[1]},
+                                   {"u_outlet_speed", &p.outlet_speed},
+                                   {"", nullptr}}};
+    for (const Uniform& u : uniforms) {
+        for (const U32& k : u32) {
+            if (k.name == u.name) {
+                if (!std::holds_alternative<std::uint32_t>(u.value)) {
+                    return "cuda backend: uniform " + std::string(u.name) + " must be an unsigned integer";
+                }
+                *k.at = std::get<std::uint32_t>(u.value);
+            }
+        }
+        for (const F32& k : f32) {
+            if (!k.name.empty() && k.name == u.name) {
+                if (!std::holds_alternative<Float32Uniform>(u.value)) {
+                    return "cuda backend: uniform " + std::string(u.name) + " must be a binary32 value";
+                }
+                *k.at = static_cast<float>(std::get<Float32Uniform>(u.value).value);
+            }
+        }
+    }
+    return std::nullopt;
+}
+
 } // namespace
 
 CudaComputeBackend::CudaComputeBackend(int device) : device_(device) {
@@ -117,7 +170,10 @@ CudaComputeBackend::CudaComputeBackend(int device) : device_(device) {
 CudaComputeBackend::~CudaComputeBackend() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(static_cast<cudaStream_t>(stream_));
-    for (auto& [id, t] : tables_) orr_gl3d_destroy(t.handle);
+    for (auto& [id, t] : tables_) {
+        orr_gl3d_destroy(t.handle);
+        orr_gl2d_destroy(t.handle2);
+    }
     for (auto& [id, b] : buffers_) cudaFree(b.base);
     if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
 }
@@ -132,7 +188,8 @@ ComputeBackendInfo CudaComputeBackend::info() const {
 }
 
 bool CudaComputeBackend::has_kernel(std::string_view name) const {
-    return name == kStep || name == kMoments || name == kForce;
+    return name == kStep || name == kMoments || name == kForce || name == kStep2 || name == kMoments2 ||
+           name == kForce2;
 }
 
 DeviceMemory CudaComputeBackend::memory() const {
@@ -174,6 +231,7 @@ void CudaComputeBackend::drop_tables(BufferId buffer) noexcept {
     auto it = tables_.find(buffer.value);
     if (it != tables_.end()) {
         orr_gl3d_destroy(it->second.handle);
+        orr_gl2d_destroy(it->second.handle2);
         tables_.erase(it);
     }
 }
@@ -243,7 +301,7 @@ Status CudaComputeBackend::tables_for(BufferId classes, const orr_gl3d_params& p
     auto it = tables_.find(classes.value);
     if (it != tables_.end()) {
         const orr_gl3d_params& l = it->second.lattice;
-        const bool same = l.nx == params.nx && l.ny == params.ny && l.nz == params.nz &&
+        const bool same = it->second.handle != nullptr && l.nx == params.nx && l.ny == params.ny && l.nz == params.nz &&
                           l.x_mode == params.x_mode && l.outlet_mode == params.outlet_mode &&
                           std::equal(std::begin(l.wall_kind), std::end(l.wall_kind), std::begin(params.wall_kind));
         if (same) {
@@ -274,12 +332,123 @@ Status CudaComputeBackend::tables_for(BufferId classes, const orr_gl3d_params& p
     return std::monostate{};
 }
 
+Status CudaComputeBackend::tables2_for(BufferId solid, const orr_gl2d_params& params, Tables*& out) {
+    auto it = tables_.find(solid.value);
+    if (it != tables_.end()) {
+        const orr_gl2d_params& l = it->second.lattice2;
+        const bool same = it->second.handle2 != nullptr && l.nx == params.nx && l.ny == params.ny &&
+                          l.x_mode == params.x_mode && l.outlet_mode == params.outlet_mode &&
+                          l.bottom_kind == params.bottom_kind && l.top_kind == params.top_kind;
+        if (same) {
+            out = &it->second;
+            return std::monostate{};
+        }
+        drop_tables(solid);
+    }
+    const std::size_t cells = static_cast<std::size_t>(params.nx) * params.ny;
+    if (buffer_size(solid) < cells * sizeof(std::uint32_t)) {
+        return failure("cuda backend: the solid-flag buffer is smaller than the lattice");
+    }
+    std::vector<std::uint32_t> flags(cells);
+    if (Status read = readback(solid, 0, std::as_writable_bytes(std::span<std::uint32_t>(flags))); !read) {
+        return read;
+    }
+    orr_gl2d* handle = nullptr;
+    if (orr_gl2d_create(&params, flags.data(), device_, &handle) != ORR_OK) {
+        return failure(std::string("cuda backend: ") + orr_last_error());
+    }
+    Tables& entry = tables_[solid.value];
+    entry = Tables{};
+    entry.handle2 = handle;
+    entry.lattice2 = params;
+    ++tables_built_;
+    out = &entry;
+    return std::monostate{};
+}
+
+// The D2Q9 driver's dispatches (GpuLbm2D::step, macroscopic, force:
+// lbm2d_gpu.cpp:218-300).
+Status CudaComputeBackend::dispatch2(const DispatchCommand& command) {
+    orr_gl2d_params p{};
+    if (auto bad = read_uniforms2(command.uniforms, p)) {
+        return failure(*bad);
+    }
+    std::array<Buffer*, 8> bound{};
+    std::array<BufferId, 8> ids{};
+    for (const BufferBinding& b : command.buffers) {
+        auto it = buffers_.find(b.buffer.value);
+        if (it == buffers_.end()) {
+            return failure("cuda backend: dispatch binds an unknown buffer");
+        }
+        if (b.binding < bound.size()) {
+            bound[b.binding] = &it->second;
+            ids[b.binding] = b.buffer;
+        }
+    }
+    const std::size_t cells = static_cast<std::size_t>(p.nx) * p.ny;
+    const auto need = [&](std::uint32_t binding, std::size_t bytes, const char* what) -> std::optional<std::string> {
+        if (bound[binding] == nullptr) {
+            return std::string("cuda backend: ") + what + " is not bound";
+        }
+        if (bound[binding]->bytes < bytes) {
+            return std::string("cuda backend: the ") + what + " buffer is too small for the lattice";
+        }
+        return std::nullopt;
+    };
+    if (auto bad = need(kBindSource, 9 * cells * sizeof(float), "population source")) return failure(*bad);
+    cudaSetDevice(device_);
+    const auto* src = reinterpret_cast<const float*>(bound[kBindSource]->data);
+    orr_status st = ORR_OK;
+    orr_gl2d* t = nullptr;
+    if (command.kernel == kForce2) {
+        // The force kernel binds no solid flags and needs no tables (the
+        // link list carries the geometry).
+        if (auto bad = need(kBindLinks, 2 * static_cast<std::size_t>(p.link_count) * sizeof(std::uint32_t), "link")) {
+            return failure(*bad);
+        }
+        if (auto bad = need(kBindLinkForce, 2 * static_cast<std::size_t>(p.link_count) * sizeof(float),
+                            "link force")) {
+            return failure(*bad);
+        }
+        st = orr_gl2d_link_force(t, &p, src, reinterpret_cast<const std::uint32_t*>(bound[kBindLinks]->data),
+                                 reinterpret_cast<float*>(bound[kBindLinkForce]->data), stream_);
+    } else {
+        if (auto bad = need(kBindClass, cells * sizeof(std::uint32_t), "solid flag")) return failure(*bad);
+        Tables* tables = nullptr;
+        if (Status ok = tables2_for(ids[kBindClass], p, tables); !ok) {
+            return ok;
+        }
+        t = tables->handle2;
+        if (command.kernel == kStep2) {
+            if (auto bad = need(kBindDestination, 9 * cells * sizeof(float), "population destination")) {
+                return failure(*bad);
+            }
+            if (auto bad = need(kBindOutlet, 3 * static_cast<std::size_t>(p.ny) * sizeof(float), "outlet")) {
+                return failure(*bad);
+            }
+            st = orr_gl2d_step(t, &p, src, reinterpret_cast<float*>(bound[kBindDestination]->data),
+                               reinterpret_cast<float*>(bound[kBindOutlet]->data), stream_);
+        } else {
+            if (auto bad = need(kBindMoments, 3 * cells * sizeof(float), "moment")) return failure(*bad);
+            st = orr_gl2d_moments(t, &p, src, reinterpret_cast<float*>(bound[kBindMoments]->data), stream_);
+        }
+    }
+    if (st != ORR_OK) {
+        return failure(std::string("cuda backend: ") + (t ? orr_gl2d_last_error(t) : orr_last_error()));
+    }
+    ++dispatches_;
+    return std::monostate{};
+}
+
 Status CudaComputeBackend::dispatch(const DispatchCommand& command) {
     if (!has_kernel(command.kernel)) {
         return failure("cuda backend: unknown kernel " + std::string(command.kernel));
     }
     if (command.global.x == 0 || command.global.y == 0 || command.global.z == 0) {
         return failure("cuda backend: empty dispatch");
+    }
+    if (command.kernel == kStep2 || command.kernel == kMoments2 || command.kernel == kForce2) {
+        return dispatch2(command);
     }
     orr_gl3d_params p{};
     if (auto bad = read_uniforms(command.uniforms, p)) {

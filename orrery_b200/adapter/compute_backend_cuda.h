@@ -10,12 +10,14 @@
 // library's step reads past a lattice's edges); upload and readback are
 // ordered after every earlier dispatch on the backend's one stream, so
 // barrier() has nothing to do.  dispatch() serves the three kernels the
-// driver binds (lbm_d3q19_step, lbm_d3q19_moments, lbm_d3q19_force) through
-// the library's orr_gl3d_* entry points, with the driver's binding points
-// and uniforms: the tables the library derives from a node-code buffer are
-// built at the first dispatch that binds it and kept until that buffer is
-// written again or released.  Like the reference's backends, one thread uses
-// a backend.
+// D3Q19 driver binds (lbm_d3q19_step, lbm_d3q19_moments, lbm_d3q19_force)
+// through the library's orr_gl3d_* entry points, and the three of the D2Q9
+// driver, GpuLbm2D (src/aero/lbm/lbm2d_gpu.cpp: lbm_d2q9_step, _moments,
+// _force), through orr_gl2d_*, with the drivers' binding points and
+// uniforms: the tables the library derives from a node-code (or solid-flag)
+// buffer are built at the first dispatch that binds it and kept until that
+// buffer is written again or released.  Like the reference's backends, one
+// thread uses a backend.
 #pragma once
 
 #include <cstdint>
@@ -58,12 +60,16 @@ private:
         std::size_t bytes = 0;
     };
     struct Tables {
-        orr_gl3d* handle = nullptr;
+        orr_gl3d* handle = nullptr;    // D3Q19: from a node-code buffer
         orr_gl3d_params lattice{};
         std::size_t wall_values = 0;   // wall fractions the node codes' slots address
+        orr_gl2d* handle2 = nullptr;   // D2Q9: from a solid-flag buffer
+        orr_gl2d_params lattice2{};
     };
 
     [[nodiscard]] Status tables_for(BufferId classes, const orr_gl3d_params& params, Tables*& out);
+    [[nodiscard]] Status tables2_for(BufferId solid, const orr_gl2d_params& params, Tables*& out);
+    [[nodiscard]] Status dispatch2(const DispatchCommand& command);
     void drop_tables(BufferId buffer) noexcept;
 
     int device_ = 0;

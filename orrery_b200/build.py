@@ -41,6 +41,7 @@ SOURCES = {
     "force_static.cu": [],
     "tiles.cu": [],
     "gl3d.cu": [],
+    "gl2d.cu": [],
     "batch3d.cu": [],
     "serve3d.cu": [],
     "voxel.cu": ["-fmad=false"],

@@ -157,3 +157,111 @@ def test_force_over_more_links_than_one_grid_dimension():
     print(f"measured: CUDA backend force over {links} links vs CPU: force {err:.2e}, moment {err_m:.2e} "
           f"of the largest component")
     assert err < 1e-4 and err_m < 1e-4
+
+
+# ---- D2Q9: the reference's GpuLbm2D on the CUDA backend -------------------
+# Cases and bars of the reference's 2D GPU-vs-CPU comparisons
+# (tests/aero/lbm/test_lbm_gpu.cpp:83-120 compare(), 204-276), with the CUDA
+# backend in place of the GL one.
+
+def _fluid2(nx, ny):
+    return np.zeros(nx * ny, np.uint8)
+
+
+def _density_deviation_error(a, b, solid):
+    """density_deviation_error of lbm_test_support.h:60-78."""
+    keep = np.asarray(solid) == 0
+    a, b = np.asarray(a)[keep], np.asarray(b)[keep]
+    peak = float(np.max(np.abs(b - 1.0))) if b.size else 0.0
+    diff = float(np.sum((a - b) ** 2))
+    if b.size == 0 or peak == 0.0:
+        return math.sqrt(diff)
+    return math.sqrt(diff / b.size) / peak
+
+
+def compare2(O, config, solid, steps, fields=None):
+    """compare() of test_lbm_gpu.cpp:83-120 with the CUDA backend."""
+    cpu = O.Reference2D(config, solid)
+    if fields is not None:
+        cpu.initialize(*fields)
+    cpu.step(steps)
+    crho, cux, cuy = cpu.macroscopic()
+    fc = cpu.force()
+    pc = cpu.populations()
+    cpu.close()
+    g = O.reference_gpu_driver_solve2d(config, solid, fields=fields, steps=steps)
+    assert g["executes_kernels"] and g["steps"] == steps
+    assert g["tables_built"] == 1          # one solid-flag buffer, tables kept over every dispatch
+    out = {
+        "velocity": velocity_l2([g["ux"], g["uy"]], [cux, cuy], solid),
+        "density": _density_deviation_error(g["density"], crho, solid),
+        "populations": l2_relative(g["populations"], pc),
+        "force_x": abs(g["force"][0] - fc[0]) / abs(fc[0]) if fc[0] != 0 else abs(g["force"][0]),
+    }
+    print(f"measured: CUDA backend D2Q9 vs CPU after {steps} steps: {out}")
+    return out
+
+
+def test_d2q9_analytic_flows():
+    O = _oracle()
+    from orrery_b200.lbm3d import Lbm2DConfig, XBoundary
+    pois = Lbm2DConfig(nx=8, ny=64, tau=0.8, x_boundary=XBoundary.periodic, bottom=wall(WallKind.no_slip),
+                       top=wall(WallKind.no_slip), body_force_x=1e-6)
+    assert compare2(O, pois, _fluid2(8, 64), 4000)["velocity"] < 1e-4
+    cou = Lbm2DConfig(nx=8, ny=32, tau=0.9, x_boundary=XBoundary.periodic, bottom=wall(WallKind.no_slip),
+                      top=wall(WallKind.no_slip, 0.03))
+    assert compare2(O, cou, _fluid2(8, 32), 4000)["velocity"] < 1e-4
+    # Taylor-Green vortex on a periodic 64 x 64 box (taylor_green, :106-116)
+    n, u0 = 64, 0.03
+    box = Lbm2DConfig(nx=n, ny=n, tau=0.6, x_boundary=XBoundary.periodic, bottom=wall(WallKind.periodic),
+                      top=wall(WallKind.periodic))
+    k = 2.0 * math.pi / n
+    y, x = np.meshgrid(np.arange(n, dtype=np.float64), np.arange(n, dtype=np.float64), indexing="ij")
+    rho = 1.0 - 0.75 * u0 * u0 * (np.cos(2.0 * k * x) + np.cos(2.0 * k * y))
+    ux = -u0 * np.cos(k * x) * np.sin(k * y)
+    uy = u0 * np.sin(k * x) * np.cos(k * y)
+    r = compare2(O, box, _fluid2(n, n), 2000, fields=(rho.reshape(-1), ux.reshape(-1), uy.reshape(-1)))
+    assert r["velocity"] < 1e-4 and r["density"] < 1e-3, r
+
+
+@pytest.mark.parametrize("rho", [1.0, 2.0, 0.7])
+def test_d2q9_uniform_stream_between_co_moving_walls(rho):
+    O = _oracle()
+    from orrery_b200.lbm3d import Lbm2DConfig, XBoundary
+    u = 0.02
+    cfg = Lbm2DConfig(nx=4, ny=12, tau=0.8, x_boundary=XBoundary.periodic, bottom=wall(WallKind.no_slip, u),
+                      top=wall(WallKind.no_slip, u))
+    n = 4 * 12
+    g = O.reference_gpu_driver_solve2d(cfg, _fluid2(4, 12), fields=(np.full(n, rho), np.full(n, u), np.zeros(n)),
+                                       steps=200)
+    worst = max(float(np.max(np.abs(g["density"] - rho) / rho)), float(np.max(np.abs(g["ux"] - u) / u)),
+                float(np.max(np.abs(g["uy"]) / u)))
+    print(f"measured: CUDA backend D2Q9 co-moving walls at density {rho}: {worst}")
+    assert worst < 1e-4
+
+
+@pytest.mark.parametrize("les", [False, True])
+def test_d2q9_cylinder_channel(les):
+    """Re 100, D 10 at (50, 50.5) of 200 x 100: Zou-He inlet, extrapolation
+    outlet, slip sides, bounce-back and momentum exchange, with and without
+    the LES closure (C 0.17), 4000 steps (test_lbm_gpu.cpp:259-276)."""
+    O = _oracle()
+    from helpers import cylinder_setup
+    from orrery_b200.lbm3d import Smagorinsky
+    cfg, mask = cylinder_setup(200, 100, 10.0, 50.0, 50.5, 0.05, 100.0)
+    if les:
+        cfg.smagorinsky = Smagorinsky(True, 0.17)
+    r = compare2(O, cfg, mask.solid, 4000)
+    assert r["velocity"] < 1e-4 and r["force_x"] < 1e-4, r
+
+
+def test_d2q9_adapter_on_the_cuda_backend():
+    """The reference's 2D adapter with its backend option set to the CUDA
+    backend (test_lbm_gpu.cpp:278-311): Cd within 1e-4 of the CPU solver's,
+    the same iterations and surface samples."""
+    O = _oracle()
+    r = O.reference_adapter2d_on_backend()
+    print(f"measured: 2D adapter Cd CPU {r['cd_cpu']!r}, CUDA backend {r['cd_gpu']!r}")
+    assert r["cd_gpu"] == pytest.approx(r["cd_cpu"], rel=1e-4)
+    assert r["iterations_gpu"] == r["iterations_cpu"]
+    assert r["cp_gpu"] == r["cp_cpu"] > 0
