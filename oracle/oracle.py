@@ -739,6 +739,7 @@ def _backend_lib():
                                             ctypes.c_uint64, _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_refusals.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_adapter2d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_adapter3d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
         _backend = lib
     return _backend
 
@@ -805,6 +806,18 @@ def reference_adapter2d_on_backend() -> dict:
         raise ReferenceError_(msg.value.decode())
     return {"cd_cpu": float(out[0]), "cd_gpu": float(out[1]), "iterations_cpu": int(out[2]),
             "iterations_gpu": int(out[3]), "cp_cpu": int(out[4]), "cp_gpu": int(out[5])}
+
+
+def reference_adapter3d_on_backend() -> dict:
+    """The reference's 3D adapter (LbmAeroSolver3D) on its CPU solver and on
+    its own GPU driver over the CUDA backend, the case of the reference's
+    "3D IAeroSolver adapter runs on the GPU backend" test."""
+    out = np.zeros(4)
+    msg = ctypes.create_string_buffer(2048)
+    if _backend_lib().ref_backend_adapter3d(_ptr(out, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return {"cd_cpu": float(out[0]), "cd_gpu": float(out[1]), "iterations_cpu": int(out[2]),
+            "iterations_gpu": int(out[3])}
 
 
 def reference_backend_refusals():

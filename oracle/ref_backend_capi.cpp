@@ -23,6 +23,8 @@
 #include "orrery/aero/lbm/lbm2d.h"
 #include "orrery/aero/lbm/lbm_aero_solver.h"
 #include "orrery/aero/lbm3d/lbm3d.h"
+#include "orrery/aero/lbm3d/lbm_aero_solver3d.h"
+#include "orrery/geom/primitives.h"
 #include "orrery_lbm.h"
 #include "ref_convert.h"
 
@@ -233,6 +235,55 @@ int ref_backend_adapter2d(double* out, char* message, size_t capacity) {
         out[3] = static_cast<double>(gpu.result().iterations);
         out[4] = static_cast<double>(cpu.result().surface.cp.size());
         out[5] = static_cast<double>(gpu.result().surface.cp.size());
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The reference's 3D adapter, LbmAeroSolver3D (src/aero/lbm3d/
+// lbm_aero_solver3d.cpp), unmodified, on its CPU solver and on the reference's
+// GPU driver over the CUDA backend (LbmSolver3DOptions::backend): the case of
+// "The 3D IAeroSolver adapter runs on the GPU backend" (tests/aero/lbm3d/
+// test_lbm3d_gpu.cpp:291-324; a 2 cm sphere of 32 segments, speed 0.1,
+// density 1000, Re 50, 10 cells per length, u_lat 0.05, upstream 2,
+// downstream 4, width 4, duration 5, window 2, 1000 steps per call).  out
+// (4): Cd CPU, Cd GPU, iterations CPU, iterations GPU.
+int ref_backend_adapter3d(double* out, char* message, size_t capacity) {
+    try {
+        namespace aero = orrery::aero;
+        namespace geom = orrery::geom;
+        compute::CudaComputeBackend backend(0);
+        aero::AeroGeometry geometry;
+        geometry.mesh = geom::sphere_profile(0.01).mesh({32, 0.1});
+        geometry.reference.length = 0.02;
+        geometry.reference.area = 0.25 * std::numbers::pi * 0.02 * 0.02;
+        aero::FlowConditions conditions;
+        conditions.speed = 0.1;
+        conditions.density = 1000.0;
+        conditions.viscosity = 1000.0 * 0.1 * 0.02 / 50.0;
+        lbm::LbmSolver3DOptions options;
+        options.resolution = lbm::LatticeResolution{10.0, 0.05};
+        options.upstream = 2.0;
+        options.downstream = 4.0;
+        options.width = 4.0;
+        options.duration = 5.0;
+        options.average_window = 2.0;
+        options.steps_per_call = 1000;
+        lbm::LbmAeroSolver3D cpu(options);
+        cpu.setup(geometry, conditions);
+        while (!cpu.step()) {
+        }
+        options.backend = &backend;
+        lbm::LbmAeroSolver3D gpu(options);
+        gpu.setup(geometry, conditions);
+        while (!gpu.step()) {
+        }
+        out[0] = cpu.result().cd;
+        out[1] = gpu.result().cd;
+        out[2] = static_cast<double>(cpu.result().iterations);
+        out[3] = static_cast<double>(gpu.result().iterations);
         return 0;
     } catch (const std::exception& e) {
         ref_convert::copy_message(e.what(), message, capacity);

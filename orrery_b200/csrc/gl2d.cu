@@ -156,7 +156,10 @@ orr_status orr_gl2d_create(const orr_gl2d_params* params, const uint32_t* solid_
         for (std::size_t c = 0; c < cells; ++c) {
             solid[c] = solid_flags[c] != 0u ? 1u : 0u;
         }
-        const orr_lbm2d_config c = config_of2(p);
+        orr_lbm2d_config c = config_of2(p);
+        // Validated with the configured inlet speed (u_outlet_speed), not the
+        // instantaneous one of the dispatch.
+        c.inlet_ux = p.outlet_speed;
         if (std::string problem = problem2d(c, solid.data(), ORR_STORAGE_F32, true); !problem.empty()) {
             throw Refusal{ORR_ERR_INVALID, problem};
         }

@@ -213,6 +213,10 @@ orr_status orr_gl3d_create(const orr_gl3d_params* params, const uint32_t* class_
         // Node classes and bounce-back masks from the solid nodes (the
         // halfway plan: both depend on the mask and the sides only).
         orr_lbm3d_config c = config_of(p, false);
+        // The dispatch's inlet velocity is the instantaneous one (the adapter
+        // ramps it up from rest); the lattice is validated with the
+        // configured speed, which the driver passes as u_outlet_speed.
+        c.inlet_ux = p.outlet_speed;
         if (std::string problem = problem3d(c, solid.data(), nullptr, ORR_STORAGE_F32, true); !problem.empty()) {
             throw Refusal{ORR_ERR_INVALID, problem};
         }

@@ -265,3 +265,51 @@ def test_d2q9_adapter_on_the_cuda_backend():
     assert r["cd_gpu"] == pytest.approx(r["cd_cpu"], rel=1e-4)
     assert r["iterations_gpu"] == r["iterations_cpu"]
     assert r["cp_gpu"] == r["cp_cpu"] > 0
+
+
+def test_d3q19_adapter_on_the_cuda_backend():
+    """The reference's 3D adapter, unmodified, with its backend option set to
+    the CUDA backend, so its own GPU driver runs the lattice
+    (test_lbm3d_gpu.cpp:291-324): Cd within 1e-4 of the CPU solver's and the
+    same iterations."""
+    O = _oracle()
+    r = O.reference_adapter3d_on_backend()
+    print(f"measured: 3D adapter Cd CPU {r['cd_cpu']!r}, GPU driver on the CUDA backend {r['cd_gpu']!r}")
+    assert abs(r["cd_gpu"] - r["cd_cpu"]) / r["cd_cpu"] < 1e-4
+    assert r["iterations_gpu"] == r["iterations_cpu"]
+
+
+def test_smagorinsky_closure_through_the_driver():
+    """The closure relaxes a manufactured shear at the predicted rate on the
+    driver's binary32 populations (test_lbm3d_gpu.cpp:168-195: tau 0.52,
+    C 0.4, shear 0.01 along every pair of axes): the effective relaxation
+    time of one collision within 2% of tau_eff - tau."""
+    O = _oracle()
+    from helpers import closure_probe
+    tau, gamma, cconst = 0.52, 0.01, 0.4
+    n = 8
+    coords = [np.tile(np.arange(n), n * n), np.tile(np.repeat(np.arange(n), n), n), np.repeat(np.arange(n), n * n)]
+    worst = 0.0
+    for a in range(3):
+        for b in range(3):
+            if a == b:
+                continue
+            cfg = periodic_box(n, n, n, tau)
+            cfg.smagorinsky = Smagorinsky(True, cconst)
+            cells = cfg.cells
+            u = [np.zeros(cells), np.zeros(cells), np.zeros(cells)]
+            u[a] = gamma * (coords[b] - 3.5)
+            fields = (np.ones(cells), *u)
+            solid = np.zeros(cells, np.uint8)
+            before = O.reference_gpu_driver_solve(cfg, solid, fields=fields, steps=0)["populations"]
+            after = O.reference_gpu_driver_solve(cfg, solid, fields=fields, steps=1)["populations"]
+            for k in (1, 3, 6):
+                node = [2, 5, 4]
+                node[b] = k
+                measured, predicted = closure_probe(before.reshape(19, cells), after.reshape(19, cells), node,
+                                                    a, b, tau, cconst)
+                rel = abs(measured - predicted) / (predicted - tau)
+                worst = max(worst, rel)
+                assert rel < 0.02, (a, b, k, measured, predicted)
+    print(f"measured: closure through the driver on the CUDA backend, worst |tau_eff - closure| / "
+          f"(closure - tau) {worst:.2e}")
