@@ -217,7 +217,12 @@ core::Result<BufferId, std::string> CudaComputeBackend::create_buffer(std::size_
         cudaGetLastError();
         return core::failure(cuda_text("buffer allocation", e));
     }
-    if (cudaError_t e = cudaMemset(b.base, 0, total); e != cudaSuccess) {
+    // Cleared on the backend's stream, which every later upload, dispatch
+    // and read-back of the buffer follows (a clear on the legacy stream would
+    // not be ordered before them: the backend's stream does not synchronise
+    // with it).
+    auto s = static_cast<cudaStream_t>(stream_);
+    if (cudaError_t e = cudaMemsetAsync(b.base, 0, total, s); e != cudaSuccess) {
         cudaFree(b.base);
         return core::failure(cuda_text("buffer clear", e));
     }

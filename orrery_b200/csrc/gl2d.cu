@@ -182,6 +182,9 @@ orr_status orr_gl2d_create(const orr_gl2d_params* params, const uint32_t* solid_
         check(cudaMalloc(reinterpret_cast<void**>(&t->nmask), cells * 4), "gl2d mask table");
         check(cudaMemcpy(t->cls, plan.cls.data(), cells, cudaMemcpyHostToDevice), "gl2d class upload");
         check(cudaMemcpy(t->nmask, plan.nmask.data(), cells * 4, cudaMemcpyHostToDevice), "gl2d mask upload");
+        // Landed before any kernel on the caller's stream reads them (copies
+        // from pageable memory may return before their data lands).
+        check(cudaStreamSynchronize(nullptr), "gl2d table upload");
         *out = t.release();
         return ORR_OK;
     });

@@ -251,7 +251,7 @@ orr_status orr_gl3d_create(const orr_gl3d_params* params, const uint32_t* class_
         g.flat = open_side(c.y_low) && open_side(c.y_high) && open_side(c.z_low) && open_side(c.z_high) &&
                  !interpolated;
         check(cudaMalloc(reinterpret_cast<void**>(&t->cls), cells + kClassPad), "gl3d class table");
-        check(cudaMemset(t->cls, 0, cells + kClassPad), "gl3d class table");
+        check(cudaMemsetAsync(t->cls, 0, cells + kClassPad, nullptr), "gl3d class table");
         check(cudaMalloc(reinterpret_cast<void**>(&t->nmask), cells * 4), "gl3d mask table");
         check(cudaMalloc(reinterpret_cast<void**>(&t->inlet), 4 * sizeof(float)), "gl3d inlet");
         check(cudaMemcpy(t->cls, plan.cls.data(), cells, cudaMemcpyHostToDevice), "gl3d class upload");
@@ -260,6 +260,11 @@ orr_status orr_gl3d_create(const orr_gl3d_params* params, const uint32_t* class_
             check(cudaMalloc(reinterpret_cast<void**>(&t->nslot), cells * 4), "gl3d slot table");
             check(cudaMemcpy(t->nslot, slot.data(), cells * 4, cudaMemcpyHostToDevice), "gl3d slot upload");
         }
+        // The clear and the uploads ran on the legacy stream, and a copy from
+        // pageable memory may return before its data lands: wait for them
+        // here, since the kernels run on the caller's stream, which need not
+        // synchronise with the legacy one.
+        check(cudaStreamSynchronize(nullptr), "gl3d table upload");
         *out = t.release();
         return ORR_OK;
     });

@@ -111,12 +111,26 @@ void stripe(std::size_t len, int t, int n, std::size_t& a, std::size_t& b) {
     b = std::min(len, a + part);
 }
 
-// Chunk j of a copy: `len` bytes at `host` and at `device`.
+// Chunk j of a copy: `len` bytes at `device` and at `host` (2 * len there
+// for a widening chunk).
 struct Chunk {
     unsigned char* host;
     unsigned char* device;
     std::size_t len;
+    bool widen = false;
+    double add = 0.0;
 };
+
+// Binary32 values [a, b) (byte offsets) of a staged chunk to the host as
+// binary64 plus `add`.
+void widen_stripe(const Chunk& c, const unsigned char* from, std::size_t a, std::size_t b) {
+    const auto* src = reinterpret_cast<const float*>(from + a);
+    auto* dst = reinterpret_cast<double*>(c.host + 2 * a);
+    const std::size_t n = (b - a) / sizeof(float);
+    for (std::size_t k = 0; k < n; ++k) {
+        dst[k] = static_cast<double>(src[k]) + c.add;
+    }
+}
 
 void staged(bool upload, const std::vector<Chunk>& chunks, cudaStream_t stream, int device) {
     std::lock_guard<std::mutex> hold(g_ring_lock);
@@ -159,7 +173,11 @@ void staged(bool upload, const std::vector<Chunk>& chunks, cudaStream_t stream, 
                     pr.fail(s, "staged read-back");
                     return;
                 }
-                std::memcpy(chunks[j].host + a, slot(j) + a, b - a);
+                if (chunks[j].widen) {
+                    widen_stripe(chunks[j], slot(j), a, b);
+                } else {
+                    std::memcpy(chunks[j].host + a, slot(j) + a, b - a);
+                }
             }
             pr.mark_filled(j);
         }
@@ -215,10 +233,18 @@ void staged(bool upload, const std::vector<Chunk>& chunks, cudaStream_t stream, 
 
 void copy(bool upload, const HostSpan* spans, int count, cudaStream_t stream, int device) {
     std::size_t total = 0;
+    bool widen = false;
     for (int k = 0; k < count; ++k) {
         total += spans[k].bytes;
+        if (spans[k].widen) {
+            if (upload || spans[k].bytes % sizeof(float) != 0) {
+                throw CudaError{cudaErrorInvalidValue, "widening copy (read-backs of binary32 values only)"};
+            }
+            widen = true;
+        }
     }
-    if (total < kStagedCopyBytes) {
+    // Widening spans always take the ring: the host threads do the widening.
+    if (total < kStagedCopyBytes && !widen) {
         const char* what = upload ? "upload" : "read-back";
         for (int k = 0; k < count; ++k) {
             const HostSpan& s = spans[k];
@@ -236,8 +262,10 @@ void copy(bool upload, const HostSpan* spans, int count, cudaStream_t stream, in
     for (int k = 0; k < count; ++k) {
         auto* h = static_cast<unsigned char*>(spans[k].host);
         auto* d = static_cast<unsigned char*>(spans[k].device);
+        const std::size_t scale = spans[k].widen ? 2 : 1;
         for (std::size_t off = 0; off < spans[k].bytes; off += kChunk) {
-            chunks.push_back(Chunk{h + off, d + off, std::min(kChunk, spans[k].bytes - off)});
+            chunks.push_back(Chunk{h + scale * off, d + off, std::min(kChunk, spans[k].bytes - off), spans[k].widen,
+                                   spans[k].add});
         }
     }
     staged(upload, chunks, stream, device);

@@ -18,11 +18,17 @@ namespace orr {
 
 inline constexpr std::size_t kStagedCopyBytes = std::size_t(8) << 20;
 
-// One contiguous range of a copy: `bytes` at `host` and at `device`.
+// One contiguous range of a copy: `bytes` at `host` and at `device`.  A
+// widening span (read-backs only) holds binary32 values on the device
+// (`bytes` of them) and receives them on the host as binary64 values plus
+// `add` (2 * bytes at `host`): the host threads widen while they copy, so
+// the bus moves half the bytes.
 struct HostSpan {
     void* host;
     void* device;
     std::size_t bytes;
+    bool widen = false;
+    double add = 0.0;
 };
 
 // Copies every span (host to device, or device to host) as one pipeline and

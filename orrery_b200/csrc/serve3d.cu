@@ -152,6 +152,14 @@ struct orr_server {
         if (worker.joinable()) {
             worker.join();
         }
+        // The worker has stopped and its last launch has completed; the loop
+        // graph goes before the memory its nodes name, then the solvers,
+        // then the batch.
+        cudaSetDevice(opt.device);
+        if (batch && batch->stream) {
+            cudaStreamSynchronize(batch->stream);
+        }
+        release_loop();
         for (auto* list : {&active, &joining}) {
             for (Active& a : *list) {
                 if (a.solver) orr_lbm3d_destroy(a.solver);
@@ -159,7 +167,6 @@ struct orr_server {
             }
             list->clear();
         }
-        release_loop();
         if (batch) {
             orr_batch3d_destroy(batch);
             batch = nullptr;
@@ -247,7 +254,11 @@ struct orr_server {
                     }
                 }
                 check(cudaMalloc(&ramp, table.size()), "serve: ramp table");
-                check(cudaMemcpy(ramp, table.data(), table.size(), cudaMemcpyHostToDevice), "serve: ramp table");
+                // On the solver's stream, which the batch's stream waits for
+                // before the loop reads the table.
+                check(cudaMemcpyAsync(ramp, table.data(), table.size(), cudaMemcpyHostToDevice, s->stream),
+                      "serve: ramp table");
+                check(cudaStreamSynchronize(s->stream), "serve: ramp table");
             } catch (const Refusal& r) {
                 st = r.status;
                 why = r.text;

@@ -579,20 +579,6 @@ orr_status orr_lbm3d_force(orr_lbm3d* solver, double force_moment[6]) {
     });
 }
 
-namespace {
-
-// Binary64 moment planes from the binary32 ones of the shifted forms (rho is
-// stored as rho - 1), written where the host copies them from.
-__global__ void widen_moments_kernel(const float* __restrict__ m, double* __restrict__ out, uint64_t cells) {
-    const uint64_t n = 4 * cells;
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        out[i] = static_cast<double>(m[i]) + (i < cells ? 1.0 : 0.0);
-    }
-}
-
-} // namespace
-
 orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, double* uy,
                                  double* uz) {
     orr::Zone zone("lbm_macroscopic");
@@ -604,24 +590,23 @@ orr_status orr_lbm3d_macroscopic(orr_lbm3d* solver, double* rho, double* ux, dou
               "moments kernel");
         ++h->launches;
         double* outs[4] = {rho, ux, uy, uz};
-        // The binary32 planes are widened on the device into the idle
-        // population buffer (19 values of at least 2 bytes per node hold 4
-        // doubles; the next step overwrites it whole), then copied straight
-        // into the caller's arrays.
-        const double* planes = static_cast<const double*>(h->moments);
-        if (h->storage != ORR_STORAGE_F64) {
-            double* wide = static_cast<double*>(h->f[1 - h->cur]);
-            widen_moments_kernel<<<std::min<uint64_t>((4 * cells + 255) / 256, 4 * 1184), 256, 0, h->stream>>>(
-                static_cast<const float*>(h->moments), wide, cells);
-            check(cudaGetLastError(), "moment widening");
-            ++h->launches;
-            planes = wide;
-        }
+        // The binary32 planes of the shifted forms (rho - 1, ux, uy, uz) cross
+        // the bus as binary32 and are widened to binary64 by the host threads
+        // of the staged copy, rho with 1 added back (exact: rho - 1 has 24
+        // significant bits and 1 + (rho - 1) fits in 53); binary64 planes are
+        // copied as they are.
+        const bool narrow = h->storage != ORR_STORAGE_F64;
         orr::HostSpan spans[4];
         int count = 0;
         for (int k = 0; k < 4; ++k) {
-            if (outs[k] != nullptr) {
-                spans[count++] = {outs[k], const_cast<double*>(planes + k * cells), cells * 8};
+            if (outs[k] == nullptr) {
+                continue;
+            }
+            if (narrow) {
+                spans[count++] = {outs[k], static_cast<float*>(h->moments) + k * cells, cells * 4, true,
+                                  k == 0 ? 1.0 : 0.0};
+            } else {
+                spans[count++] = {outs[k], static_cast<double*>(h->moments) + k * cells, cells * 8};
             }
         }
         orr::copy_to_host(spans, count, h->stream, h->device);

@@ -91,12 +91,57 @@ int failures(fake::Stream& s) {
     return 0;
 }
 
+// Widening read-backs: binary32 values on the "device" come back as binary64
+// plus the span's offset, exactly, for spans on both sides of the staging
+// threshold and ragged chunk tails; a widening upload is refused.
+int widening(std::mt19937_64& g, fake::Stream& s) {
+    std::uniform_real_distribution<float> value(-2.0f, 2.0f);
+    for (int trial = 0; trial < 12; ++trial) {
+        const int n = 1 + static_cast<int>(g() % 4);
+        std::vector<std::vector<float>> dev(n);
+        std::vector<std::vector<double>> back(n);
+        std::vector<orr::HostSpan> down(n);
+        for (int k = 0; k < n; ++k) {
+            std::size_t count = 0;
+            switch (g() % 3) {
+            case 0: count = g() % 3000; break;
+            case 1: count = (std::size_t(1) << 20) * (1 + g() % 3) + g() % 5; break;
+            default: count = g() % (std::size_t(6) << 20); break;
+            }
+            dev[k].resize(count);
+            for (auto& v : dev[k]) v = value(g);
+            back[k].assign(count, -7.0);
+            const double add = k % 2 == 0 ? 1.0 : 0.0;
+            down[k] = {back[k].data(), dev[k].data(), count * sizeof(float), true, add};
+        }
+        orr::copy_to_host(down.data(), n, &s, 0);
+        for (int k = 0; k < n; ++k) {
+            for (std::size_t i = 0; i < dev[k].size(); ++i) {
+                if (back[k][i] != static_cast<double>(dev[k][i]) + down[k].add) {
+                    std::printf("widening differs: trial %d span %d value %zu\n", trial, k, i);
+                    return 1;
+                }
+            }
+        }
+    }
+    std::vector<float> d(16, 1.0f);
+    std::vector<double> h(16, 0.0);
+    orr::HostSpan up{h.data(), d.data(), d.size() * sizeof(float), true, 0.0};
+    try {
+        orr::copy_to_device(&up, 1, &s, 0);
+        std::printf("a widening upload was accepted\n");
+        return 1;
+    } catch (const orr::CudaError&) {
+    }
+    return 0;
+}
+
 } // namespace
 
 int main() {
     std::mt19937_64 g(12345);
     fake::Stream s;
-    if (round_trips(g, s, 24) != 0 || failures(s) != 0) {
+    if (round_trips(g, s, 24) != 0 || failures(s) != 0 || widening(g, s) != 0) {
         return 1;
     }
     std::printf("ok\n");

@@ -141,3 +141,39 @@ def test_server_refuses_bfloat16_before_touching_a_device():
         Server(storage="bf16")
     assert e.value.status == abi.ORR_ERR_INVALID
     assert "bfloat16" in str(e.value) and "0.5%" in str(e.value)
+
+
+@pytest.mark.skipif(__import__("shutil").which("gcc") is None, reason="needs gcc")
+def test_ctypes_records_match_the_header(tmp_path):
+    """Every ctypes record of the Python binding has the size and field
+    offsets of its C struct in include/orrery_lbm.h (a smaller record would
+    let the library write past a Python buffer)."""
+    import os
+    import subprocess
+    pairs = {"orr_wall": abi.CWall, "orr_lbm3d_config": abi.CLbm3DConfig, "orr_lbm2d_config": abi.CLbm2DConfig,
+             "orr_force_links": abi.CForceLinks, "orr_kernel_info": abi.CKernelInfo,
+             "orr_solver_options": abi.CSolverOptions, "orr_batch_schedule": abi.CBatchSchedule,
+             "orr_serve_options": abi.CServeOptions, "orr_solve_request": abi.CSolveRequest,
+             "orr_solve_result": abi.CSolveResult, "orr_serve_statistics": abi.CServeStatistics,
+             "orr_grid_spec": abi.CGridSpec, "orr_mesh": abi.CMesh}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "orrery_lbm.h"', "int main(void) {"]
+    for name, rec in pairs.items():
+        lines.append(f'    printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in rec._fields_:
+            lines.append(f'    printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "records.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "records"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    seen = {}
+    for line in out:
+        if line:
+            name, field, value = line.split()
+            seen[(name, field)] = int(value)
+    for name, rec in pairs.items():
+        assert seen[(name, "size")] == ctypes.sizeof(rec), name
+        for field, _ in rec._fields_:
+            assert seen[(name, field)] == getattr(rec, field).offset, (name, field)
