@@ -109,7 +109,7 @@ typedef struct orr_solver_options {
     int32_t allow_high_mach;  /* 1: skip the lattice Mach guard (opt-in; off by default) */
     int32_t device;           /* CUDA device ordinal */
     int32_t block_x;          /* threads per block of the step kernel; 0 = tuned default */
-    int32_t kernel;           /* ORR_KERNEL_*: the D3Q19 step kernel (0 = automatic) */
+    int32_t kernel;           /* ORR_KERNEL_*: the D3Q19 step kernel (0 = automatic: the row kernel) */
     int32_t stages;           /* pipeline stages of ORR_KERNEL_STAGED; 0 = tuned default */
     int32_t nodes_per_thread; /* STAGED: 1 or 2 nodes per thread of a span; ROWS: 1, or 2
                                  neighbouring nodes per thread (2-byte storage, periodic or

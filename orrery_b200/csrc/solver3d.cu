@@ -386,10 +386,8 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             check(cudaMemcpyAsync(h->ldir, p.link_dir.data(), n * 4, cudaMemcpyHostToDevice, s), "link upload");
             check(cudaMemcpyAsync(h->lq, p.link_q.data(), n * 8, cudaMemcpyHostToDevice, s), "link upload");
         }
-        // Step kernel: the persistent staged step when asked for, or
-        // automatically for the 2-byte storage forms when the lattice's rows
-        // can be staged (there it is the faster one; for binary32 and
-        // binary64 the row-tile step is).
+        // Step kernel: the row-tile step, or the persistent staged or tiled
+        // step when asked for.
         if (o.kernel == ORR_KERNEL_STAGED && !g.flat) {
             throw Refusal{ORR_ERR_INVALID, "lbm3d gpu: the staged step needs periodic or free-slip sides "
                                            "and halfway walls"};
@@ -425,10 +423,11 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             const uint64_t most = std::max<uint64_t>({h->tgrid.tiles, h->tgrid.direct, 1});
             h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
         }
-        const bool want = !h->tiled &&
-                          (o.kernel == ORR_KERNEL_STAGED ||
-                           (o.kernel == ORR_KERNEL_AUTO && h->sbytes == 2 && g.flat && stageable(g) &&
-                            (o.block_x == 0 || o.block_x == 128 || o.block_x == 256)));
+        // The automatic choice is the row kernel for every storage: at 48
+        // registers it runs the 2-byte forms as fast as the staged kernel
+        // (45.5 against 45.0 GLUPS for binary16 on the 256 x 128 x 128 sphere)
+        // with no pipeline to wait on.
+        const bool want = !h->tiled && o.kernel == ORR_KERNEL_STAGED;
         if (want) {
             const uint32_t sblock = o.block_x == 128 ? 128u : 256u;
             const uint32_t npt = o.nodes_per_thread > 0 ? static_cast<uint32_t>(o.nodes_per_thread)
