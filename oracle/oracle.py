@@ -739,6 +739,8 @@ def _backend_lib():
                                             ctypes.c_uint64, _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_refusals.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_adapter2d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_cuda2d_solve.argtypes = [ctypes.POINTER(abi.CLbm2DConfig), _u8p, _dp, _dp, _dp, ctypes.c_uint64,
+                                         _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_adapter3d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
         _backend = lib
     return _backend
@@ -794,6 +796,29 @@ def reference_gpu_driver_solve2d(config, solid, fields=None, steps: int = 0) -> 
     return {"populations": pops, "density": mom[:n], "ux": mom[n:2 * n], "uy": mom[2 * n:], "force": force,
             "dispatches": int(meta[0]), "tables_built": int(meta[1]), "executes_kernels": bool(meta[2]),
             "steps": int(meta[3])}
+
+
+def reference_cuda2d_solve(config, solid, fields=None, steps: int = 0) -> dict:
+    """One solve through the Lbm2DSolver seam: make_cuda_solver of
+    orrery_b200/adapter/lbm2d_cuda.cpp (the C++ adapter over the C ABI),
+    compiled against the reference's headers; outputs as
+    reference_gpu_driver_solve2d."""
+    lib = _backend_lib()
+    c = config.to_c()
+    n = int(config.nx) * int(config.ny)
+    s = np.ascontiguousarray(solid, np.uint8).reshape(-1)
+    f = [None] * 3 if fields is None else [np.ascontiguousarray(a, np.float64).reshape(-1) for a in fields]
+    pops = np.zeros(9 * n)
+    mom = np.zeros(3 * n)
+    force = np.zeros(3)
+    meta = np.zeros(1)
+    msg = ctypes.create_string_buffer(2048)
+    rc = lib.ref_cuda2d_solve(ctypes.byref(c), _ptr(s, _u8p), *[_ptr(a, _dp) for a in f], int(steps),
+                              _ptr(pops, _dp), _ptr(mom, _dp), _ptr(force, _dp), _ptr(meta, _dp), msg, 2048)
+    if rc != 0:
+        raise ReferenceError_(msg.value.decode())
+    return {"populations": pops, "density": mom[:n], "ux": mom[n:2 * n], "uy": mom[2 * n:], "force": force,
+            "steps": int(meta[0])}
 
 
 def reference_adapter2d_on_backend() -> dict:

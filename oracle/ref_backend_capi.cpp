@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "compute_backend_cuda.h"
+#include "lbm2d_cuda.h"
 #include "orrery/aero/lbm/lbm2d.h"
 #include "orrery/aero/lbm/lbm_aero_solver.h"
 #include "orrery/aero/lbm3d/lbm3d.h"
@@ -115,70 +116,90 @@ int ref_backend_solve(const orr_lbm3d_config* config, const uint8_t* solid, cons
     }
 }
 
+namespace {
+
+// Initial fields (or none), `steps` steps and the read-backs of one D2Q9
+// solver: populations (9 cells, unshifted), moments (density, ux, uy planes)
+// and force (x, y, moment about the origin), whichever outputs are not null.
+int run2d(lbm::Lbm2DSolver& solver, const lbm::Lbm2DConfig& c, const double* rho, const double* ux,
+          const double* uy, uint64_t steps, double* populations, double* moments, double* force, char* message,
+          size_t capacity) {
+    if (rho != nullptr) {
+        const std::size_t nx = c.nx;
+        const auto state = [=](std::size_t x, std::size_t y) {
+            const std::size_t k = x + nx * y;
+            return lbm::d2q9::Moments{rho[k], ux[k], uy[k]};
+        };
+        if (auto done = solver.initialize(state); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+    }
+    if (auto done = solver.step(steps); !done) {
+        ref_convert::copy_message(done.error(), message, capacity);
+        return -1;
+    }
+    const std::size_t cells = c.nx * c.ny;
+    if (populations != nullptr) {
+        auto f = solver.populations();
+        if (!f) {
+            ref_convert::copy_message(f.error(), message, capacity);
+            return -1;
+        }
+        std::memcpy(populations, f.value().data(), f.value().size() * sizeof(double));
+    }
+    if (moments != nullptr) {
+        auto m = solver.macroscopic();
+        if (!m) {
+            ref_convert::copy_message(m.error(), message, capacity);
+            return -1;
+        }
+        const lbm::MacroFields2D& v = m.value();
+        std::memcpy(moments, v.density.data(), cells * sizeof(double));
+        std::memcpy(moments + cells, v.velocity_x.data(), cells * sizeof(double));
+        std::memcpy(moments + 2 * cells, v.velocity_y.data(), cells * sizeof(double));
+    }
+    if (force != nullptr) {
+        auto f = solver.force();
+        if (!f) {
+            ref_convert::copy_message(f.error(), message, capacity);
+            return -1;
+        }
+        force[0] = f.value().x;
+        force[1] = f.value().y;
+        force[2] = f.value().moment;
+    }
+    return 0;
+}
+
+lbm::SolidMask2D mask2d_of(const lbm::Lbm2DConfig& c, const uint8_t* solid) {
+    lbm::SolidMask2D mask;
+    mask.nx = c.nx;
+    mask.ny = c.ny;
+    mask.solid.assign(solid, solid + c.nx * c.ny);
+    return mask;
+}
+
+} // namespace
+
 // The same for the reference's D2Q9 driver, GpuLbm2D (src/aero/lbm/
-// lbm2d_gpu.cpp, its make_gpu_solver): initial fields (rho, ux, uy) or the
-// uniform inlet state; populations (9 cells, unshifted), moments (density,
-// ux, uy planes) and force (x, y, moment about the origin).
+// lbm2d_gpu.cpp, its make_gpu_solver), on the CUDA backend: initial fields
+// (rho, ux, uy) or the uniform inlet state; the outputs of run2d.  meta (4):
+// dispatches, solid-flag tables built, executes kernels, steps.
 int ref_backend_solve2d(const orr_lbm2d_config* config, const uint8_t* solid, const double* rho,
                         const double* ux, const double* uy, uint64_t steps, double* populations, double* moments,
                         double* force, double* meta, char* message, size_t capacity) {
     try {
         compute::CudaComputeBackend backend(0);
         const lbm::Lbm2DConfig c = ref_convert::config2d_of(*config);
-        lbm::SolidMask2D mask;
-        mask.nx = c.nx;
-        mask.ny = c.ny;
-        mask.solid.assign(solid, solid + c.nx * c.ny);
-        auto made = lbm::make_gpu_solver(backend, c, std::move(mask));
+        auto made = lbm::make_gpu_solver(backend, c, mask2d_of(c, solid));
         if (!made) {
             ref_convert::copy_message(made.error(), message, capacity);
             return -1;
         }
         std::unique_ptr<lbm::Lbm2DSolver> solver = std::move(made).value();
-        if (rho != nullptr) {
-            const std::size_t nx = c.nx;
-            const auto state = [=](std::size_t x, std::size_t y) {
-                const std::size_t k = x + nx * y;
-                return lbm::d2q9::Moments{rho[k], ux[k], uy[k]};
-            };
-            if (auto done = solver->initialize(state); !done) {
-                ref_convert::copy_message(done.error(), message, capacity);
-                return -1;
-            }
-        }
-        if (auto done = solver->step(steps); !done) {
-            ref_convert::copy_message(done.error(), message, capacity);
+        if (run2d(*solver, c, rho, ux, uy, steps, populations, moments, force, message, capacity) != 0) {
             return -1;
-        }
-        const std::size_t cells = c.nx * c.ny;
-        if (populations != nullptr) {
-            auto f = solver->populations();
-            if (!f) {
-                ref_convert::copy_message(f.error(), message, capacity);
-                return -1;
-            }
-            std::memcpy(populations, f.value().data(), f.value().size() * sizeof(double));
-        }
-        if (moments != nullptr) {
-            auto m = solver->macroscopic();
-            if (!m) {
-                ref_convert::copy_message(m.error(), message, capacity);
-                return -1;
-            }
-            const lbm::MacroFields2D& v = m.value();
-            std::memcpy(moments, v.density.data(), cells * sizeof(double));
-            std::memcpy(moments + cells, v.velocity_x.data(), cells * sizeof(double));
-            std::memcpy(moments + 2 * cells, v.velocity_y.data(), cells * sizeof(double));
-        }
-        if (force != nullptr) {
-            auto f = solver->force();
-            if (!f) {
-                ref_convert::copy_message(f.error(), message, capacity);
-                return -1;
-            }
-            force[0] = f.value().x;
-            force[1] = f.value().y;
-            force[2] = f.value().moment;
         }
         if (meta != nullptr) {
             meta[0] = static_cast<double>(backend.dispatches());
@@ -187,6 +208,32 @@ int ref_backend_solve2d(const orr_lbm2d_config* config, const uint8_t* solid, co
             meta[3] = static_cast<double>(solver->steps());
         }
         solver.reset();
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The same through the Lbm2DSolver seam: make_cuda_solver of
+// orrery_b200/adapter/lbm2d_cuda.cpp (binary32 storage).  meta (1): steps.
+int ref_cuda2d_solve(const orr_lbm2d_config* config, const uint8_t* solid, const double* rho, const double* ux,
+                     const double* uy, uint64_t steps, double* populations, double* moments, double* force,
+                     double* meta, char* message, size_t capacity) {
+    try {
+        const lbm::Lbm2DConfig c = ref_convert::config2d_of(*config);
+        auto made = lbm::make_cuda_solver(c, mask2d_of(c, solid));
+        if (!made) {
+            ref_convert::copy_message(made.error(), message, capacity);
+            return -1;
+        }
+        std::unique_ptr<lbm::Lbm2DSolver> solver = std::move(made).value();
+        if (run2d(*solver, c, rho, ux, uy, steps, populations, moments, force, message, capacity) != 0) {
+            return -1;
+        }
+        if (meta != nullptr) {
+            meta[0] = static_cast<double>(solver->steps());
+        }
         return 0;
     } catch (const std::exception& e) {
         ref_convert::copy_message(e.what(), message, capacity);

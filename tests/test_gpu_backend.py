@@ -179,8 +179,10 @@ def _density_deviation_error(a, b, solid):
     return math.sqrt(diff / b.size) / peak
 
 
-def compare2(O, config, solid, steps, fields=None):
-    """compare() of test_lbm_gpu.cpp:83-120 with the CUDA backend."""
+def compare2(O, config, solid, steps, fields=None, via="backend"):
+    """compare() of test_lbm_gpu.cpp:83-120 with the CUDA backend under the
+    reference's GpuLbm2D (via "backend"), or with the C++ Lbm2DSolver adapter
+    of orrery_b200/adapter/lbm2d_cuda.cpp (via "solver")."""
     cpu = O.Reference2D(config, solid)
     if fields is not None:
         cpu.initialize(*fields)
@@ -189,28 +191,33 @@ def compare2(O, config, solid, steps, fields=None):
     fc = cpu.force()
     pc = cpu.populations()
     cpu.close()
-    g = O.reference_gpu_driver_solve2d(config, solid, fields=fields, steps=steps)
-    assert g["executes_kernels"] and g["steps"] == steps
-    assert g["tables_built"] == 1          # one solid-flag buffer, tables kept over every dispatch
+    if via == "backend":
+        g = O.reference_gpu_driver_solve2d(config, solid, fields=fields, steps=steps)
+        assert g["executes_kernels"] and g["steps"] == steps
+        assert g["tables_built"] == 1      # one solid-flag buffer, tables kept over every dispatch
+    else:
+        g = O.reference_cuda2d_solve(config, solid, fields=fields, steps=steps)
+        assert g["steps"] == steps
     out = {
         "velocity": velocity_l2([g["ux"], g["uy"]], [cux, cuy], solid),
         "density": _density_deviation_error(g["density"], crho, solid),
         "populations": l2_relative(g["populations"], pc),
         "force_x": abs(g["force"][0] - fc[0]) / abs(fc[0]) if fc[0] != 0 else abs(g["force"][0]),
     }
-    print(f"measured: CUDA backend D2Q9 vs CPU after {steps} steps: {out}")
+    print(f"measured: CUDA D2Q9 ({via}) vs CPU after {steps} steps: {out}")
     return out
 
 
-def test_d2q9_analytic_flows():
+@pytest.mark.parametrize("via", ["backend", "solver"])
+def test_d2q9_analytic_flows(via):
     O = _oracle()
     from orrery_b200.lbm3d import Lbm2DConfig, XBoundary
     pois = Lbm2DConfig(nx=8, ny=64, tau=0.8, x_boundary=XBoundary.periodic, bottom=wall(WallKind.no_slip),
                        top=wall(WallKind.no_slip), body_force_x=1e-6)
-    assert compare2(O, pois, _fluid2(8, 64), 4000)["velocity"] < 1e-4
+    assert compare2(O, pois, _fluid2(8, 64), 4000, via=via)["velocity"] < 1e-4
     cou = Lbm2DConfig(nx=8, ny=32, tau=0.9, x_boundary=XBoundary.periodic, bottom=wall(WallKind.no_slip),
                       top=wall(WallKind.no_slip, 0.03))
-    assert compare2(O, cou, _fluid2(8, 32), 4000)["velocity"] < 1e-4
+    assert compare2(O, cou, _fluid2(8, 32), 4000, via=via)["velocity"] < 1e-4
     # Taylor-Green vortex on a periodic 64 x 64 box (taylor_green, :106-116)
     n, u0 = 64, 0.03
     box = Lbm2DConfig(nx=n, ny=n, tau=0.6, x_boundary=XBoundary.periodic, bottom=wall(WallKind.periodic),
@@ -220,7 +227,7 @@ def test_d2q9_analytic_flows():
     rho = 1.0 - 0.75 * u0 * u0 * (np.cos(2.0 * k * x) + np.cos(2.0 * k * y))
     ux = -u0 * np.cos(k * x) * np.sin(k * y)
     uy = u0 * np.sin(k * x) * np.cos(k * y)
-    r = compare2(O, box, _fluid2(n, n), 2000, fields=(rho.reshape(-1), ux.reshape(-1), uy.reshape(-1)))
+    r = compare2(O, box, _fluid2(n, n), 2000, fields=(rho.reshape(-1), ux.reshape(-1), uy.reshape(-1)), via=via)
     assert r["velocity"] < 1e-4 and r["density"] < 1e-3, r
 
 
@@ -240,8 +247,9 @@ def test_d2q9_uniform_stream_between_co_moving_walls(rho):
     assert worst < 1e-4
 
 
+@pytest.mark.parametrize("via", ["backend", "solver"])
 @pytest.mark.parametrize("les", [False, True])
-def test_d2q9_cylinder_channel(les):
+def test_d2q9_cylinder_channel(les, via):
     """Re 100, D 10 at (50, 50.5) of 200 x 100: Zou-He inlet, extrapolation
     outlet, slip sides, bounce-back and momentum exchange, with and without
     the LES closure (C 0.17), 4000 steps (test_lbm_gpu.cpp:259-276)."""
@@ -251,7 +259,7 @@ def test_d2q9_cylinder_channel(les):
     cfg, mask = cylinder_setup(200, 100, 10.0, 50.0, 50.5, 0.05, 100.0)
     if les:
         cfg.smagorinsky = Smagorinsky(True, 0.17)
-    r = compare2(O, cfg, mask.solid, 4000)
+    r = compare2(O, cfg, mask.solid, 4000, via=via)
     assert r["velocity"] < 1e-4 and r["force_x"] < 1e-4, r
 
 
