@@ -255,6 +255,44 @@ def default_forms(args) -> dict:
     return out
 
 
+def reference_benchmarks(local_rank: int) -> list:
+    """The reference's own GPU benchmark cases (tests/bench/aero/
+    bench_lbm_gpu.cpp: D3Q19 128^3 sphere, D2Q9 2048 x 1024 cylinder, BGK and
+    Smagorinsky) on the CUDA solver, binary32 as the reference: 50 warm-up
+    steps, then 1000 steps timed like the reference (host clock around
+    step(1000) and a drain) and on the device (CUDA events on the solver's
+    stream).  Beside each, the reference's published rate on its OpenGL
+    backend (RX 9060 XT), for context: other hardware."""
+    import numpy as np
+    import torch
+
+    from orrery_b200 import solver as S
+    from orrery_b200 import workloads as W
+    out = []
+    for case in W.reference_benchmarks():
+        s = S.make_gpu_solver(case.config, case.mask)
+        stream = torch.cuda.ExternalStream(s.stream(), device=torch.device("cuda", local_rank))
+        s.step(50)
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        start.record(stream)
+        s.step(1000)
+        stop.record(stream)
+        stop.synchronize()
+        wall = time.perf_counter() - t0
+        device_s = start.elapsed_time(stop) * 1e-3
+        finite = bool(np.isfinite(s.mass()))
+        s.close()
+        out.append({"case": case.name, "nodes": case.cells, "steps_per_s": 1000.0 / wall,
+                    "mlups": case.cells * 1000.0 / wall / 1e6, "device_steps_per_s": 1000.0 / device_s,
+                    "device_mlups": case.cells * 1000.0 / device_s / 1e6, "finite": finite,
+                    "reference_gl_steps_per_s": case.published_steps_per_s,
+                    "vs_reference_gl": 1000.0 / wall / case.published_steps_per_s})
+    return out
+
+
 def run_form(args, rank: int) -> int:
     """The batched and served forms (one GPU; other ranks idle)."""
     if rank != 0:
@@ -460,7 +498,9 @@ def main(argv=None) -> int:
                "cpu_model": cpu_model(), "nproc": os.cpu_count()}
 
     forms_out = None
+    ref_cases = None
     if rank == 0 and world == 1 and not args.no_forms:
+        ref_cases = reference_benchmarks(local_rank)
         forms_out = default_forms(args)
 
     if rank == 0:
@@ -486,6 +526,8 @@ def main(argv=None) -> int:
         }
         if forms_out is not None:
             line["forms"] = forms_out
+        if ref_cases is not None:
+            line["reference_benchmarks"] = ref_cases
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -742,6 +742,10 @@ def _backend_lib():
         lib.ref_cuda2d_solve.argtypes = [ctypes.POINTER(abi.CLbm2DConfig), _u8p, _dp, _dp, _dp, ctypes.c_uint64,
                                          _dp, _dp, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
         lib.ref_backend_adapter3d.argtypes = [_dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_rate3d.argtypes = [ctypes.POINTER(abi.CLbm3DConfig), _u8p, ctypes.c_uint64,
+                                           ctypes.c_uint64, _dp, ctypes.c_char_p, ctypes.c_size_t]
+        lib.ref_backend_rate2d.argtypes = [ctypes.POINTER(abi.CLbm2DConfig), _u8p, ctypes.c_uint64,
+                                           ctypes.c_uint64, _dp, ctypes.c_char_p, ctypes.c_size_t]
         _backend = lib
     return _backend
 
@@ -843,6 +847,20 @@ def reference_adapter3d_on_backend() -> dict:
         raise ReferenceError_(msg.value.decode())
     return {"cd_cpu": float(out[0]), "cd_gpu": float(out[1]), "iterations_cpu": int(out[2]),
             "iterations_gpu": int(out[3])}
+
+
+def reference_driver_rate(config, solid, warmup: int = 50, count: int = 1000) -> float:
+    """Steps per second of the reference's own GPU benchmark loop with its GPU
+    driver (3D or 2D, by the configuration) on the CUDA backend."""
+    lib = _backend_lib()
+    c = config.to_c()
+    s = np.ascontiguousarray(solid, np.uint8).reshape(-1)
+    seconds = np.zeros(1)
+    msg = ctypes.create_string_buffer(2048)
+    fn = lib.ref_backend_rate3d if isinstance(c, abi.CLbm3DConfig) else lib.ref_backend_rate2d
+    if fn(ctypes.byref(c), _ptr(s, _u8p), int(warmup), int(count), _ptr(seconds, _dp), msg, 2048) != 0:
+        raise ReferenceError_(msg.value.decode())
+    return count / float(seconds[0])
 
 
 def reference_backend_refusals():

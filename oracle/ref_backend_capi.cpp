@@ -10,6 +10,7 @@
 // "GPU and CPU D3Q19 agree" comparisons, tests/aero/lbm3d/test_lbm3d_gpu.cpp,
 // with the CUDA backend in place of the GL one).  The product never links or
 // loads it.
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -331,6 +332,71 @@ int ref_backend_adapter3d(double* out, char* message, size_t capacity) {
         out[1] = gpu.result().cd;
         out[2] = static_cast<double>(cpu.result().iterations);
         out[3] = static_cast<double>(gpu.result().iterations);
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+// The rate of the reference's own benchmark (tests/bench/aero/
+// bench_lbm_gpu.cpp: gpu_steps_per_second) with its GPU driver on the CUDA
+// backend: make_gpu_solver, `warmup` steps, a drain, then `count` steps
+// timed by the host clock up to the drain after them.  seconds: the timed
+// span.  The 3D and 2D drivers.
+int ref_backend_rate3d(const orr_lbm3d_config* config, const uint8_t* solid, uint64_t warmup, uint64_t count,
+                       double* seconds, char* message, size_t capacity) {
+    try {
+        compute::CudaComputeBackend backend(0);
+        const lbm::Lbm3DConfig c = ref_convert::config3d_of(*config);
+        auto made = lbm::make_gpu_solver(backend, c, ref_convert::mask3d_of(*config, solid, nullptr));
+        if (!made) {
+            ref_convert::copy_message(made.error(), message, capacity);
+            return -1;
+        }
+        auto solver = std::move(made).value();
+        if (auto done = solver->step(warmup); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        backend.finish();
+        const auto t0 = std::chrono::steady_clock::now();
+        if (auto done = solver->step(count); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        backend.finish();
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return 0;
+    } catch (const std::exception& e) {
+        ref_convert::copy_message(e.what(), message, capacity);
+        return -1;
+    }
+}
+
+int ref_backend_rate2d(const orr_lbm2d_config* config, const uint8_t* solid, uint64_t warmup, uint64_t count,
+                       double* seconds, char* message, size_t capacity) {
+    try {
+        compute::CudaComputeBackend backend(0);
+        const lbm::Lbm2DConfig c = ref_convert::config2d_of(*config);
+        auto made = lbm::make_gpu_solver(backend, c, mask2d_of(c, solid));
+        if (!made) {
+            ref_convert::copy_message(made.error(), message, capacity);
+            return -1;
+        }
+        auto solver = std::move(made).value();
+        if (auto done = solver->step(warmup); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        backend.finish();
+        const auto t0 = std::chrono::steady_clock::now();
+        if (auto done = solver->step(count); !done) {
+            ref_convert::copy_message(done.error(), message, capacity);
+            return -1;
+        }
+        backend.finish();
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return 0;
     } catch (const std::exception& e) {
         ref_convert::copy_message(e.what(), message, capacity);

@@ -187,6 +187,13 @@ ComputeBackendInfo CudaComputeBackend::info() const {
     return ComputeBackendInfo{"cuda", name, stream_ != nullptr};
 }
 
+void CudaComputeBackend::finish() {
+    if (stream_ != nullptr) {
+        cudaSetDevice(device_);
+        cudaStreamSynchronize(static_cast<cudaStream_t>(stream_));
+    }
+}
+
 bool CudaComputeBackend::has_kernel(std::string_view name) const {
     return name == kStep || name == kMoments || name == kForce || name == kStep2 || name == kMoments2 ||
            name == kForce2;

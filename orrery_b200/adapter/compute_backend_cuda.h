@@ -47,6 +47,10 @@ public:
     [[nodiscard]] Status readback(BufferId buffer, std::size_t offset, std::span<std::byte> bytes) override;
     [[nodiscard]] Status dispatch(const DispatchCommand& command) override;
     void barrier() override {}
+    // Waits until every upload, dispatch and read-back so far has completed
+    // (the GL backend's finish(), which the reference's benchmarks call
+    // around their timed steps).
+    void finish();
 
     // Dispatches served so far (by all three kernels), and node-code tables
     // built: for tests of the caching.

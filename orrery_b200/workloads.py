@@ -24,6 +24,15 @@ Workloads (sizes in lattice nodes):
                   degrees, u = 0.05, Re uniform in 200..1000 on the chord,
                   Smagorinsky C = 0.1, free-slip lateral walls, zero-gradient
                   outflow.
+  reference_benchmarks
+                  the reference's own GPU benchmark cases
+                  (tests/bench/aero/bench_lbm_gpu.cpp:91-140): the D3Q19 128^3
+                  sphere channel (D 24 a quarter node off the axis, 2.5 D from
+                  the inlet, u = 0.05, Re 300, free-slip sides) and the D2Q9
+                  2048 x 1024 cylinder (D 64 at (400, 512.5), u = 0.05,
+                  Re 1000, free-slip top and bottom), each without and with
+                  the Smagorinsky closure (C = 0.1), from the uniform inlet
+                  state.
   sphere_cone_requests
                   the serving form's request stream: Poisson arrivals (rate
                   20/s), sphere-cone capsules (half-angle 20..35 degrees, nose
@@ -154,6 +163,43 @@ def cylinder2d(seed: int = 1, nx: int = 400, ny: int = 160, diameter: float = 32
     ux = np.where(fluid, u + uniform_noise(seed, n, 0, noise), 0.0)
     uy = np.where(fluid, uniform_noise(seed, n, 1, noise), 0.0)
     return Workload2D(f"cylinder2d_{nx}x{ny}", cfg, mask, rho, ux, uy, diameter)
+
+
+@dataclass
+class BenchmarkCase:
+    """One of the reference's GPU benchmark cases and its published rate on
+    its OpenGL backend (AMD Radeon RX 9060 XT, binary32;
+    docs/performance.md:140-141, 164)."""
+    name: str
+    config: object
+    mask: object
+    cells: int
+    published_steps_per_s: float
+
+
+def reference_benchmarks() -> list[BenchmarkCase]:
+    """The four cases of tests/bench/aero/bench_lbm_gpu.cpp (sphere_channel,
+    lbm3d_test_support.h:249-270; cylinder_setup, lbm_test_support.h:
+    154-167)."""
+    cases = []
+    published = {(3, False): 681.86, (3, True): 676.67, (2, False): 1521.0, (2, True): 1475.0}
+    for les in (False, True):
+        n, d, u = 128, 24.0, 0.05
+        c = Lbm3DConfig(nx=n, ny=n, nz=n, tau=tau_of_viscosity(u * d / 300.0),
+                        x_boundary=XBoundary.inflow_outflow, y_low=wall(WallKind.slip),
+                        y_high=wall(WallKind.slip), z_low=wall(WallKind.slip), z_high=wall(WallKind.slip),
+                        inlet_ux=u, smagorinsky=Smagorinsky(les, 0.1))
+        centre = (2.5 * d, 0.5 * (n - 1) + 0.25, 0.5 * (n - 1) + 0.25)
+        cases.append(BenchmarkCase(f"sphere3d_128^3_{'les' if les else 'bgk'}", c,
+                                   M.sphere_mask(n, n, n, centre, 0.5 * d), n ** 3, published[(3, les)]))
+    for les in (False, True):
+        nx, ny, d, u = 2048, 1024, 64.0, 0.05
+        c = Lbm2DConfig(nx=nx, ny=ny, tau=tau_of_viscosity(u * d / 1000.0),
+                        x_boundary=XBoundary.inflow_outflow, bottom=wall(WallKind.slip),
+                        top=wall(WallKind.slip), inlet_ux=u, smagorinsky=Smagorinsky(les, 0.1))
+        cases.append(BenchmarkCase(f"cylinder2d_2048x1024_{'les' if les else 'bgk'}", c,
+                                   M.circle_mask(nx, ny, 400.0, 512.5, 0.5 * d), nx * ny, published[(2, les)]))
+    return cases
 
 
 def coefficients3d(force, moment, u: float, area: float, length: float, rho: float = 1.0,
