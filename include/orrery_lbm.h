@@ -122,9 +122,9 @@ typedef struct orr_solver_options {
  * row spans receive their 19 source segments through a shared-memory
  * pipeline of bulk asynchronous copies (rows of lattices whose nx is a
  * multiple of 16; other rows take the per-node path); it serves lattices with
- * periodic or free-slip sides and halfway walls (and refuses others).  AUTO picks STAGED for the binary16
- * and bfloat16 forms when the lattice qualifies, ROWS otherwise.  Both give
- * the same result bit for bit. */
+ * periodic or free-slip sides and halfway walls (and refuses others).  TILED:
+ * a persistent kernel fed by tensor-map tile copies, for the same lattices.
+ * AUTO picks ROWS for every storage.  All give the same result bit for bit. */
 enum { ORR_KERNEL_AUTO = 0, ORR_KERNEL_ROWS = 1, ORR_KERNEL_STAGED = 2, ORR_KERNEL_TILED = 3 };
 
 typedef struct orr_lbm3d orr_lbm3d;

@@ -1040,13 +1040,20 @@ __device__ __forceinline__ void step_node3(const Geom3D& g, const Phys3D<typenam
 }
 
 // Resident 256-thread blocks per SM the row step is compiled for: 48
-// registers for the binary32-arithmetic flat step, 64 for the general one,
-// 128 for binary64.  The flat step fits 48 without spills, and the extra
-// resident warps hide more of the memory latency: 45.5 against 42.8 GLUPS for
-// binary16 storage in 128-thread blocks, 41.4 against 39.9 for binary32 in
-// 256-thread blocks (256 x 128 x 128 sphere channel).
+// registers for the binary32 flat step, 40 for the flat step of the 2-byte
+// storages, 64 for the general one, 128 for binary64.  The flat step fits 48
+// without spills, and the extra resident warps hide more of the memory
+// latency: 45.5 against 42.8 GLUPS for binary16 storage in 128-thread blocks,
+// 41.4 against 39.9 for binary32 in 256-thread blocks (256 x 128 x 128 sphere
+// channel).  The 2-byte forms, which issue more instructions per byte moved,
+// gain again from 48 warps at 40 registers despite a few spilled values
+// (binary16 88.1 against 92.1 us per step, bfloat16 89.8 against 93.1);
+// binary32 loses there (105.2 against 101.1 us), so it keeps 48 registers.
 template <class S, bool kFlat>
-constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2 : (kFlat ? 5 : 4);
+constexpr int kStepMinBlocks = sizeof(typename Storage<S>::A) == 8 ? 2
+                               : !kFlat                        ? 4
+                               : sizeof(S) == 2                ? 6
+                                                               : 5;
 
 // Grid (tiles along x, ny, nz): block (t, y, z) covers x in [t B, (t + 1) B)
 // of row (y, z).

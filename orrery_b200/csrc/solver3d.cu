@@ -423,9 +423,9 @@ orr_status orr_lbm3d_create(const orr_lbm3d_config* config, const uint8_t* solid
             const uint64_t most = std::max<uint64_t>({h->tgrid.tiles, h->tgrid.direct, 1});
             h->shape.grid = static_cast<uint32_t>(std::min<uint64_t>(h->shape.grid, most));
         }
-        // The automatic choice is the row kernel for every storage: at 48
-        // registers it runs the 2-byte forms as fast as the staged kernel
-        // (45.5 against 45.0 GLUPS for binary16 on the 256 x 128 x 128 sphere)
+        // The automatic choice is the row kernel for every storage: at 40
+        // registers it runs the 2-byte forms faster than the staged kernel
+        // (47.4 against 45.0 GLUPS for binary16 on the 256 x 128 x 128 sphere)
         // with no pipeline to wait on.
         const bool want = !h->tiled && o.kernel == ORR_KERNEL_STAGED;
         if (want) {
